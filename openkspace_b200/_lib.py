@@ -1,0 +1,96 @@
+"""ctypes binding of ``libokscuda.so`` (the C-ABI of ``include/okscuda.h``).
+
+The library is required: importing the compute entry points without it, or
+calling them on a machine without a CUDA device, raises -- there is no CPU
+fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libokscuda.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "okscuda.h")
+
+OKS_OK = 0
+OKS_EINVAL = -1
+OKS_ESHAPE = -2
+OKS_EODD = -3
+OKS_ENOTPD = -4
+OKS_ECUDA = -5
+OKS_ENOMEM = -6
+OKS_EAGAIN = -7
+OKS_ETIMEDOUT = -8
+OKS_ENOTSUP = -9
+OKS_ESKIP = -10
+
+_c = ctypes
+_vp = _c.c_void_p
+_i = _c.c_int
+_f = _c.c_float
+_sz = _c.c_size_t
+
+# name -> (restype, argtypes); every symbol include/okscuda.h declares
+SIGNATURES = {
+    "okscuda_create": (_i, [_i, _c.POINTER(_vp)]),
+    "okscuda_destroy": (None, [_vp]),
+    "okscuda_last_error": (_i, [_vp, _c.c_char_p, _sz]),
+    "okscuda_set_stream": (_i, [_vp, _vp]),
+    "okscuda_get_stream": (_vp, [_vp]),
+    "okscuda_synchronize": (_i, [_vp]),
+    "okscuda_version": (_c.c_char_p, []),
+    "okscuda_malloc": (_i, [_vp, _sz, _c.POINTER(_vp)]),
+    "okscuda_free": (_i, [_vp, _vp]),
+    "okscuda_upload": (_i, [_vp, _vp, _vp, _sz]),
+    "okscuda_download": (_i, [_vp, _vp, _vp, _sz]),
+    "okscuda_host_alloc": (_i, [_vp, _sz, _c.POINTER(_vp)]),
+    "okscuda_host_free": (_i, [_vp, _vp]),
+    "okscuda_centred_fft2": (_i, [_vp, _vp, _i, _i, _i, _i]),
+    "okscuda_haar_forward": (_i, [_vp, _vp, _vp, _i, _i, _i]),
+    "okscuda_haar_inverse": (_i, [_vp, _vp, _vp, _i, _i, _i]),
+    "okscuda_soft_threshold_details": (_i, [_vp, _vp, _i, _i, _i, _f]),
+    "okscuda_rss_crop": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _vp]),
+    "okscuda_fista_cs": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp]),
+    "okscuda_cs_slice": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp, _vp]),
+}
+
+_lib = None
+
+
+class OksError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def header_symbols() -> list[str]:
+    """Function names declared in include/okscuda.h."""
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(okscuda_[a-z0-9_]+)\s*\(", txt)))
+
+
+def load(build_if_missing: bool = True):
+    """Load the library (building it in-tree when sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing:
+        from . import build as _b
+        if _b.needs_build():
+            try:
+                _b.build()
+            except Exception:  # noqa: BLE001 - a prebuilt library may still be loadable
+                if not os.path.exists(LIB_PATH):
+                    raise
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} is missing: build it with `python -m openkspace_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L

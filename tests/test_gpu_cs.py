@@ -1,0 +1,161 @@
+"""Parity of the sm_100a FISTA-CS path with the oracle, through the C-ABI.
+
+Tolerances (stated by the spec of this path): relative L2 <= 1e-4 against the
+FP32 restatement of the reference (``csref``) after the stated iteration
+count, and NRMSE <= 1e-4 against the FP64 oracle.  Primitives (single FFTs,
+Haar) are held to 1e-5 / 1e-6.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import cs_fp64 as o64
+from oracle import csref
+from openkspace_b200 import OksError, _lib, synth
+from tests.conftest import crandn, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_CS = 1e-4
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "cs_golden.npz")
+
+
+def row_mask(rng, ny, nx, frac=0.4):
+    rows = rng.random(ny) < frac
+    rows[ny // 2 - min(2, ny // 2):ny // 2 + min(2, ny // 2)] = True
+    return np.repeat(rows[:, None], nx, axis=1)
+
+
+# ------------------------------------------------------------- primitives
+@pytest.mark.parametrize("ny,nx", [(8, 8), (16, 12), (5, 7), (23, 46), (256, 256), (368, 320),
+                                   (384, 640), (192, 22), (1, 4), (2, 1)])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_centred_fft2(ctx, rng, ny, nx, inverse):
+    x = crandn(rng, (2, ny, nx))
+    got = ctx.centred_fft2(x, inverse)
+    want = o64.centred_ifft2(x) if inverse else o64.centred_fft2(x)
+    assert rel_l2(got, want) < 1e-5
+
+
+def test_centred_fft2_unitary_reference_case(ctx):
+    """cs.rs:224-256 on the device: energy 1e-3, round trip 1e-4."""
+    i, j = np.meshgrid(np.arange(8), np.arange(8), indexing="ij")
+    x = ((i + j) + 1j * (i - j) * 0.3).astype(np.complex64)
+    y = ctx.centred_fft2(x)
+    assert abs(np.sum(np.abs(x) ** 2) - np.sum(np.abs(y) ** 2)) < 1e-3
+    assert np.max(np.abs(ctx.centred_fft2(y, True) - x)) < 1e-4
+
+
+@pytest.mark.parametrize("ny,nx", [(8, 8), (4, 6), (64, 32)])
+def test_haar_and_threshold(ctx, rng, ny, nx):
+    x = crandn(rng, (3, ny, nx))
+    f = ctx.haar_forward(x)
+    assert rel_l2(f, o64.haar_forward(x)) < 1e-6
+    assert rel_l2(ctx.haar_inverse(f), x) < 1e-6
+    s = ctx.soft_threshold_details(x, 0.7)
+    assert rel_l2(s, o64.soft_threshold_details(x, 0.7)) < 1e-6
+
+
+def test_rss_crop(ctx, rng):
+    c = crandn(rng, (5, 20, 16))
+    assert rel_l2(ctx.rss_crop(c), o64.rss_combine(c)) < 1e-6
+    got = ctx.rss_crop(c, (12, 8))
+    want = o64.center_crop_3d(o64.rss_combine(c)[None], (1, 12, 8))[0]
+    assert rel_l2(got, want) < 1e-6
+    a = np.array([3, 4, 5], np.complex64).reshape(3, 1, 1)
+    assert abs(ctx.rss_crop(np.repeat(np.repeat(a, 2, 1), 2, 2))[0, 0] - np.sqrt(50.0)) < 1e-5
+
+
+# ------------------------------------------------------------------- FISTA
+@pytest.mark.parametrize("ny,nx,iters", [(16, 16, 30), (24, 20, 40), (46, 16, 25), (2, 2, 10),
+                                         (256, 256, 20), (320, 64, 15), (368, 32, 15),
+                                         (384, 32, 12), (250, 12, 10), (2 * 7 * 11, 8, 10)])
+def test_fista_matches_oracles(ctx, rng, ny, nx, iters):
+    k = crandn(rng, (2, ny, nx))
+    m = row_mask(rng, ny, nx)
+    k = np.where(m[None], k, 0).astype(np.complex64)
+    got = ctx.fista_cs(k, m, iters, 0.05)
+    want64 = o64.fista_cs_single_coil(k, m, iters, 0.05)
+    assert rel_l2(got, want64) < TOL_CS
+    want32 = np.stack([csref.fista_cs_single_coil(k[c], m, iters, 0.05) for c in range(2)])
+    assert rel_l2(got, want32) < TOL_CS
+
+
+def test_fista_golden_vectors(ctx):
+    g = np.load(GOLDEN)
+    names = sorted({key.split("__")[0] for key in g.files})
+    ran = 0
+    for name in names:
+        k, m = g[f"{name}__kspace"], g[f"{name}__mask"].astype(bool)
+        iters, lam = g[f"{name}__params"]
+        rows_ok = np.all(m == m[:, :1])
+        if not rows_ok:
+            continue   # general 2-D masks: covered once that path exists
+        got = ctx.fista_cs(k, m, int(iters), float(lam))
+        assert rel_l2(got, g[f"{name}__x"]) < TOL_CS, name
+        ran += 1
+    assert ran >= 4
+
+
+def test_sparse_phantom_reference_case(ctx):
+    """cs.rs:258-321 on the device: cs_err < 0.8 zf_err."""
+    from tests.test_oracle_pins import sparse_phantom_case
+    truth, kzf, mask = sparse_phantom_case()
+    zf = o64.centred_ifft2(kzf)
+    rec = ctx.fista_cs_single_coil(kzf, mask, 200, 0.02)
+    assert np.linalg.norm((rec - truth).ravel()) < 0.8 * np.linalg.norm((zf - truth).ravel())
+    assert rel_l2(rec, o64.fista_cs_single_coil(kzf, mask, 200, 0.02)) < TOL_CS
+
+
+def test_fista_edge_cases(ctx, rng):
+    ny, nx = 16, 8
+    k = crandn(rng, (ny, nx))
+    # iters = 0: zero-filled reconstruction (atb)
+    m = row_mask(rng, ny, nx)
+    kz = np.where(m, k, 0)
+    assert rel_l2(ctx.fista_cs(kz, m, 0, 0.01), o64.centred_ifft2(kz)) < 1e-5
+    # empty mask -> zeros; full mask -> reference result
+    zero = ctx.fista_cs(k, np.zeros((ny, nx), bool), 5, 0.01)
+    assert np.all(zero == 0)
+    full = np.ones((ny, nx), bool)
+    assert rel_l2(ctx.fista_cs(k, full, 7, 0.01), o64.fista_cs_single_coil(k, full, 7, 0.01)) < TOL_CS
+    # values outside the mask are ignored, as cs.rs:84-111 does
+    junk = np.where(m, k, 1e3 + 1e3j).astype(np.complex64)
+    assert rel_l2(ctx.fista_cs(junk, m, 9, 0.01), ctx.fista_cs(kz, m, 9, 0.01)) < 1e-6
+    # batch 0 is a no-op
+    d = ctx.empty((0, ny, nx))
+    assert ctx.fista_cs(np.zeros((0, ny, nx), np.complex64), m, 3, 0.01).shape == (0, ny, nx)
+    del d
+
+
+def test_fista_errors(ctx):
+    with pytest.raises(OksError) as e:
+        ctx.fista_cs(np.zeros((7, 8), np.complex64), np.ones((7, 8), bool), 1, 0.01)
+    assert e.value.code == _lib.OKS_EODD
+    with pytest.raises(OksError) as e:
+        ctx.fista_cs(np.zeros((8, 8), np.complex64), np.ones((8, 6), bool), 1, 0.01)
+    assert e.value.code == _lib.OKS_ESHAPE
+
+
+def test_fista_in_place(ctx, rng):
+    ny, nx = 32, 16
+    m = row_mask(rng, ny, nx)
+    k = np.where(m[None], crandn(rng, (3, ny, nx)), 0).astype(np.complex64)
+    d = ctx.to_device(k)
+    ctx.fista_cs(d, m, 12, 0.02, out=d)
+    assert rel_l2(d.to_host(), o64.fista_cs_single_coil(k, m, 12, 0.02)) < TOL_CS
+
+
+# ---------------------------------------------------------- per-slice RSS
+def test_cs_slice_plain_workload(ctx):
+    """8 coils, 256 x 256, R = 4 + 24 centre lines, lambda 0.01, 50 iterations."""
+    s = synth.plain_slice(0)
+    m = s.mask2d
+    rss, coils = ctx.cs_slice(s.kspace, m, 50, 0.01, return_coils=True)
+    x64 = o64.fista_cs_single_coil(s.kspace, m, 50, 0.01)
+    rss64 = o64.rss_combine(x64)
+    assert o64.nrmse(rss, rss64) < TOL_CS
+    assert o64.nrmse(coils, x64) < TOL_CS
+    rss32 = csref.csrss(s.kspace[:, None], m[None], 50, 0.01, nthreads=os.cpu_count() or 1)[0]
+    assert rel_l2(rss, rss32) < TOL_CS
