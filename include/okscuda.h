@@ -98,6 +98,105 @@ int okscuda_fista_cs(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_
 int okscuda_cs_slice(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nc,
                      int ny, int nx, int iters, float lambda, float* d_rss, okscuda_c64* d_coils);
 
+/* strategy.rs:849-885 for a whole volume in one batched launch: placed
+ * k-space d_kspace[nc, nz, ny, nx], per-slice host masks h_mask[nz, ny, nx],
+ * per-coil FISTA, f32 RSS in coil order, centre crop to [ty, tx] per slice
+ * (crop.rs:13-27 centring) into d_rss[nz, ty, tx].  d_coils[nc, nz, ny, nx]
+ * receives the coil images when not NULL. */
+int okscuda_cs_volume(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nc,
+                      int nz, int ny, int nx, int iters, float lambda, int ty, int tx, float* d_rss,
+                      okscuda_c64* d_coils);
+
+/* ------------------------------------------------------- feeding stages */
+/* prewhiten.rs:48-111 + 148-210 in FP64 on the device.  d_noise[nc, ns] holds
+ * the samples of every noise scan with nc channels (concatenated along
+ * samples); total_samples counts the samples of ALL noise scans, including
+ * scans with another channel count, as prewhiten.rs:58 does (<= 0: use ns).
+ * Writes W = L^-1 (complex64 [nc, nc], lower triangular) to d_W.  Synchronous.
+ * OKS_ESKIP: total_samples < nc (prewhiten.rs:59-66); OKS_ENOTPD: Cholesky
+ * pivot not finite or <= 0 (prewhiten.rs:161-164) -- the reference then
+ * skips prewhitening. */
+int okscuda_prewhiten_fit(okscuda_ctx* ctx, const okscuda_c64* d_noise, int nc, long long ns,
+                          long long total_samples, okscuda_c64* d_W);
+/* prewhiten.rs:118-142: every sample column of d_data[nacq, nc, ns] -> W s. */
+int okscuda_prewhiten_apply(okscuda_ctx* ctx, const okscuda_c64* d_W, okscuda_c64* d_data, long long nacq,
+                            int nc, int ns);
+/* oversampling.rs:50-71 and 103-155: d_in[nlines, enc] -> d_out[nlines, rec]
+ * (centred IFFT / enc, crop, centred FFT).  OKS_ESKIP when (enc, rec) is not
+ * an integer ratio in 2..8 (the reference builds no remover). */
+int okscuda_os_remove(okscuda_ctx* ctx, const okscuda_c64* d_in, okscuda_c64* d_out, long long nlines, int enc,
+                      int rec);
+/* fft.rs:52-56 ifft1_inplace(axis = 1): centred 1-D IFFT (1/nz) along kz of
+ * d_data[nc, nz, ny, nx], in place (3-D decoupling, strategy.rs:824-827). */
+int okscuda_ifft1_kz(okscuda_ctx* ctx, okscuda_c64* d_data, int nc, int nz, int ny, int nx);
+/* fft.rs:19-29 ifft2_inplace on the last two axes of d_data[batch, ny, nx]
+ * (1/ny and 1/nx), in place -- the odd-size fallback of strategy.rs:829-842. */
+int okscuda_ifft2(okscuda_ctx* ctx, okscuda_c64* d_data, long long batch, int ny, int nx);
+
+/* ------------------------------------------------ CsRss (strategy.rs:736-892) */
+/* One acquisition (ISMRMRD AcquisitionHeader fields the cs path reads,
+ * acquisition.rs:33-95).  Its samples are [active_channels, number_of_samples]
+ * at data + data_offset. */
+typedef struct {
+    uint64_t flags;                 /* ISMRMRD flag bits (1 << (pos - 1))           */
+    uint16_t number_of_samples;
+    uint16_t active_channels;
+    uint16_t discard_pre;
+    uint16_t discard_post;
+    uint16_t center_sample;
+    uint16_t kspace_encode_step_1;
+    uint16_t kspace_encode_step_2;
+    uint16_t slice;
+    long long data_offset;          /* in complex samples                          */
+} okscuda_acq_header;
+
+/* The reference's IsmrmrdFile as the cs path sees it. */
+typedef struct {
+    long long n_acq;
+    const okscuda_acq_header* headers;   /* host [n_acq]                          */
+    const okscuda_c64* data;             /* all samples (host, or device if flagged) */
+    long long data_len;                  /* complex samples in data               */
+    int data_on_device;                  /* 1: data is a device pointer           */
+    int enc_x, enc_y, enc_z;             /* encoding.encoded_matrix               */
+    int rec_x, rec_y, rec_z;             /* encoding.recon_matrix                 */
+    int ky_center, kz_center;            /* encoding limits centre (reader.rs:343-347) */
+} okscuda_acq_set;
+
+/* CsRss public fields (strategy.rs:753-761). */
+typedef struct {
+    int remove_oversampling;
+    int prewhiten;
+    int phase_correct;
+    int iters;
+    float lambda;
+    int fft_mode;                        /* 0 Auto, 1 TwoD, 2 ThreeD (strategy.rs:72-79) */
+    int crop_to_recon_matrix;
+} okscuda_csrss_cfg;
+
+/* strategy.rs:763-775 defaults: iters 60, lambda 0.01, everything on. */
+void okscuda_csrss_default(okscuda_csrss_cfg* cfg);
+/* "cs" (strategy.rs:778-780) */
+const char* okscuda_csrss_name(void);
+/* CsRss::reconstruct (strategy.rs:782-891): calibration, prewhitening,
+ * oversampling removal, placement (reader.rs:225-468), kz decoupling,
+ * odd-size fallback, per-slice per-coil FISTA, RSS, crop.  Writes the
+ * magnitude volume [nz, ny, nx] (after crop) to h_out (host, capacity
+ * out_cap floats) and its shape to out_dims[3].  OKS_EINVAL mirrors
+ * IoError::MissingField (no image acquisitions / zero channels);
+ * OKS_ENOTSUP when phase_correct is set and navigator scans are present
+ * (navigator phase correction is not part of this library). */
+int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, const okscuda_acq_set* acqs,
+                              float* h_out, long long out_cap, int* out_dims);
+
+/* ------------------------------------------------------------- profiling */
+/* No reference counterpart (the reference has no timing hooks).  When
+ * enabled, every kernel launch of this context is bracketed by CUDA events
+ * on the context stream; okscuda_profile_read aggregates per kernel name the
+ * summed device time (ms) and the launch count.  Enabling clears the log. */
+int okscuda_profile_enable(okscuda_ctx* ctx, int on);
+int okscuda_profile_read(okscuda_ctx* ctx, char* names, int name_len, double* total_ms,
+                         long long* launches, int nslots, int* nfound);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,18 @@ SIGNATURES = {
     "okscuda_rss_crop": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _vp]),
     "okscuda_fista_cs": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp]),
     "okscuda_cs_slice": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp, _vp]),
+    "okscuda_cs_volume": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _i, _i, _vp, _vp]),
+    "okscuda_prewhiten_fit": (_i, [_vp, _vp, _i, _c.c_longlong, _c.c_longlong, _vp]),
+    "okscuda_prewhiten_apply": (_i, [_vp, _vp, _vp, _c.c_longlong, _i, _i]),
+    "okscuda_os_remove": (_i, [_vp, _vp, _vp, _c.c_longlong, _i, _i]),
+    "okscuda_ifft1_kz": (_i, [_vp, _vp, _i, _i, _i, _i]),
+    "okscuda_ifft2": (_i, [_vp, _vp, _c.c_longlong, _i, _i]),
+    "okscuda_csrss_default": (None, [_vp]),
+    "okscuda_csrss_name": (_c.c_char_p, []),
+    "okscuda_csrss_reconstruct": (_i, [_vp, _vp, _vp, _vp, _c.c_longlong, _c.POINTER(_i)]),
+    "okscuda_profile_enable": (_i, [_vp, _i]),
+    "okscuda_profile_read": (_i, [_vp, _c.c_char_p, _i, _c.POINTER(_c.c_double),
+                                  _c.POINTER(_c.c_longlong), _i, _c.POINTER(_i)]),
 }
 
 _lib = None

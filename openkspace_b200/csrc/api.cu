@@ -1,119 +1,6 @@
 // C-ABI of the FISTA-CS path (include/okscuda.h): contexts, device memory,
 // FFT plans and the dispatch of the sm_100a kernels.
-#include <cuda_runtime.h>
-
-#include <cmath>
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
-#include <map>
-#include <memory>
-#include <string>
-#include <vector>
-
-#include "../../include/okscuda.h"
-#include "kernels.h"
-#include "plan.h"
-
-using oks::DevPlan;
-
-struct okscuda_ctx {
-    int device = 0;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    oks::PlanCache plans;
-    std::map<int, float*> alpha;          // iters -> device alpha table
-    // scratch (grow-only)
-    void* scratch = nullptr;
-    size_t scratch_bytes = 0;
-};
-
-namespace {
-
-int set_err(okscuda_ctx* c, int code, const char* fmt, ...) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    if (c) c->err = buf;
-    return code;
-}
-
-int cuda_err(okscuda_ctx* c, cudaError_t e, const char* where) {
-    return set_err(c, e == cudaErrorMemoryAllocation ? OKS_ENOMEM : OKS_ECUDA, "%s: %s (%s)", where,
-                   cudaGetErrorString(e), cudaGetErrorName(e));
-}
-
-#define OKS_CUDA(call)                                   \
-    do {                                                 \
-        cudaError_t e_ = (call);                         \
-        if (e_ != cudaSuccess) return cuda_err(ctx, e_, #call); \
-    } while (0)
-
-#define OKS_CHECK_CTX()                                                  \
-    do {                                                                 \
-        if (!ctx) return OKS_EINVAL;                                     \
-        cudaError_t e0_ = cudaSetDevice(ctx->device);                    \
-        if (e0_ != cudaSuccess) return cuda_err(ctx, e0_, "cudaSetDevice"); \
-    } while (0)
-
-int ensure_scratch(okscuda_ctx* ctx, size_t bytes) {
-    if (bytes <= ctx->scratch_bytes) return OKS_OK;
-    if (ctx->scratch) {
-        cudaStreamSynchronize(ctx->stream);
-        cudaFree(ctx->scratch);
-        ctx->scratch = nullptr;
-        ctx->scratch_bytes = 0;
-    }
-    cudaError_t e = cudaMalloc(&ctx->scratch, bytes);
-    if (e != cudaSuccess) return cuda_err(ctx, e, "cudaMalloc(scratch)");
-    ctx->scratch_bytes = bytes;
-    return OKS_OK;
-}
-
-// cs.rs:125-126 in f32, as the reference computes it.
-int get_alpha(okscuda_ctx* ctx, int iters, const float** out) {
-    auto it = ctx->alpha.find(iters);
-    if (it != ctx->alpha.end()) { *out = it->second; return OKS_OK; }
-    std::vector<float> h(iters > 0 ? iters : 1, 0.f);
-    float t = 1.0f;
-    for (int i = 0; i < iters; ++i) {
-        float t_new = 0.5f * (1.0f + std::sqrt(1.0f + 4.0f * t * t));
-        h[i] = (t - 1.0f) / t_new;
-        t = t_new;
-    }
-    float* d = nullptr;
-    OKS_CUDA(cudaMalloc(&d, sizeof(float) * h.size()));
-    OKS_CUDA(cudaMemcpy(d, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
-    ctx->alpha[iters] = d;
-    *out = d;
-    return OKS_OK;
-}
-
-int get_plan(okscuda_ctx* ctx, int n, const DevPlan** out) {
-    std::string msg;
-    const DevPlan* p = ctx->plans.get(n, &msg);
-    if (!p) return set_err(ctx, OKS_ECUDA, "FFT plan for n=%d: %s", n, msg.c_str());
-    *out = p;
-    return OKS_OK;
-}
-
-// Row mask of a 2-D mask when every row is all-0 or all-1.
-bool separable_rows(const uint8_t* mask, int ny, int nx, std::vector<uint8_t>* rows) {
-    rows->assign(ny, 0);
-    for (int r = 0; r < ny; ++r) {
-        const uint8_t* m = mask + (size_t)r * nx;
-        const bool on = m[0] != 0;
-        for (int x = 1; x < nx; ++x)
-            if ((m[x] != 0) != on) return false;
-        (*rows)[r] = on ? 1 : 0;
-    }
-    return true;
-}
-
-}  // namespace
+#include "ctx.h"
 
 // ====================================================================== C-ABI
 extern "C" {
@@ -144,6 +31,9 @@ void okscuda_destroy(okscuda_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (auto& kv : ctx->alpha) cudaFree(kv.second);
     if (ctx->scratch) cudaFree(ctx->scratch);
+    ctx->staging.release();
+    for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : ctx->ev_pool) cudaEventDestroy(e);
     ctx->plans.clear();
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -231,11 +121,15 @@ int okscuda_centred_fft2(okscuda_ctx* ctx, okscuda_c64* d_data, int batch, int n
     oks::RowXformArgs ra{};
     ra.in = d; ra.out = d; ra.nrows = (long long)batch * ny; ra.ld_in = nx; ra.ld_out = nx;
     ra.sign = inverse ? +1 : -1; ra.centred = 1; ra.scale = 1.0f; ra.rows_per_prob = ny;
-    OKS_CUDA(oks::launch_row_xform(ra, oks::RowBits{}, *px, ctx->stream));
+    {
+        ProfScope ps(ctx, "k_row_xform");
+        OKS_CUDA(oks::launch_row_xform(ra, *px, ctx->stream));
+    }
     oks::ColXformArgs ca{};
     ca.data = d; ca.nprob = batch; ca.ny = ny; ca.nx = nx; ca.prob_stride = (long long)ny * nx;
     ca.sign = inverse ? +1 : -1; ca.centred = 1;
     ca.scale = 1.0f / std::sqrt((float)ny * (float)nx);
+    ProfScope ps(ctx, "k_col_xform");
     OKS_CUDA(oks::launch_col_xform(ca, *py, ctx->stream));
     return OKS_OK;
 }
@@ -247,6 +141,7 @@ static int haar_common(okscuda_ctx* ctx, const okscuda_c64* in, okscuda_c64* out
         return set_err(ctx, OKS_EINVAL, "haar: bad arguments");
     if (ny % 2 || nx % 2) return set_err(ctx, OKS_EODD, "Haar: dims must be even");
     if (in == out) return set_err(ctx, OKS_EINVAL, "haar: in and out must differ");
+    ProfScope ps(ctx, "k_haar");
     OKS_CUDA(oks::launch_haar(reinterpret_cast<const float2*>(in), reinterpret_cast<float2*>(out), batch,
                               ny, nx, inverse, ctx->stream));
     return OKS_OK;
@@ -267,6 +162,7 @@ int okscuda_soft_threshold_details(okscuda_ctx* ctx, okscuda_c64* d_data, int ba
     OKS_CHECK_CTX();
     if (!d_data || batch < 0 || ny <= 0 || nx <= 0)
         return set_err(ctx, OKS_EINVAL, "soft_threshold: bad arguments");
+    ProfScope ps(ctx, "k_soft_threshold");
     OKS_CUDA(oks::launch_soft_threshold(reinterpret_cast<float2*>(d_data), batch, ny, nx, lambda,
                                         ctx->stream));
     return OKS_OK;
@@ -281,23 +177,37 @@ int okscuda_rss_crop(okscuda_ctx* ctx, const okscuda_c64* d_coils, int nc, int n
     a.coils = reinterpret_cast<const float2*>(d_coils);
     a.coil_stride = (long long)ny * nx;
     a.nc = nc; a.ny = ny; a.nx = nx;
+    a.nslice = 1; a.slice_stride = 0;
     a.ty = ty; a.tx = tx; a.y0 = (ny - ty) / 2; a.x0 = (nx - tx) / 2;
     a.out = d_out;
+    ProfScope ps(ctx, "k_rss");
     OKS_CUDA(oks::launch_rss(a, ctx->stream));
     return OKS_OK;
 }
 
 // ---------------------------------------------------------------- FISTA-CS
-static int fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int batch,
-                      int ny, int nx, int iters, float lambda, okscuda_c64* d_out) {
-    if (!d_kspace || !h_mask || !d_out || batch < 0 || ny <= 0 || nx <= 0 || iters < 0)
-        return set_err(ctx, OKS_EINVAL, "fista_cs: bad arguments");
-    if (ny % 2 || nx % 2)
-        return set_err(ctx, OKS_EODD, "CS: Ny (%d) and Nx (%d) must both be even for Haar wavelet", ny, nx);
-    if (batch == 0) return OKS_OK;
-    std::vector<uint8_t> rows;
-    if (!separable_rows(h_mask, ny, nx, &rows))
-        return set_err(ctx, OKS_ENOTSUP, "fista_cs: mask varies along kx (general 2-D mask path not built)");
+// Row masks of `nmask` 2-D masks [nmask][ny][nx] when every row of every mask
+// is all-0 or all-1 (a ky-only mask), packed 32 rows per word.
+static bool pack_row_masks(const uint8_t* h_mask, int nmask, int ny, int nx, std::vector<uint32_t>* words,
+                           int* wstride) {
+    *wstride = (ny + 31) / 32;
+    words->assign((size_t)nmask * *wstride, 0u);
+    for (int k = 0; k < nmask; ++k)
+        for (int r = 0; r < ny; ++r) {
+            const uint8_t* m = h_mask + ((size_t)k * ny + r) * nx;
+            const bool on = m[0] != 0;
+            for (int x = 1; x < nx; ++x)
+                if ((m[x] != 0) != on) return false;
+            if (on) (*words)[(size_t)k * *wstride + (r >> 5)] |= 1u << (r & 31);
+        }
+    return true;
+}
+
+// FISTA with an arbitrary 2-D mask (not constant along kx): two passes per
+// iteration over state kept in device memory, problems processed in chunks
+// sized so the chunk's state stays resident in L2.
+static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nmask,
+                        long long nprob, int ny, int nx, int iters, float lambda, okscuda_c64* d_out) {
     const DevPlan *px, *py;
     int rc = get_plan(ctx, nx, &px);
     if (rc) return rc;
@@ -306,55 +216,199 @@ static int fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8
     const float* alpha = nullptr;
     rc = get_alpha(ctx, iters, &alpha);
     if (rc) return rc;
-    if (ny > oks::kMaxMaskRows)
-        return set_err(ctx, OKS_ENOTSUP, "fista_cs: ny=%d above %d", ny, oks::kMaxMaskRows);
-    oks::RowBits bits{};
-    for (int r = 0; r < ny; ++r)
-        if (rows[r]) bits.w[r >> 5] |= 1u << (r & 31);
+    const long long N = (long long)ny * nx;
+    oks::Staging::Slot* slot = nullptr;
+    rc = stage_upload(ctx, h_mask, (size_t)nmask * N, &slot);
+    if (rc) return rc;
+    long long chunk = ctx->fista2d_chunk > 0 ? ctx->fista2d_chunk
+                                             : std::max<long long>(1, (64ll << 20) / (4 * N * 8));
+    if (chunk > nprob) chunk = nprob;
+    void* scratch = nullptr;
+    cudaError_t e = cudaMallocAsync(&scratch, sizeof(float2) * 3 * chunk * N, ctx->stream);
+    if (e != cudaSuccess) { stage_release(ctx, slot); return cuda_err(ctx, e, "cudaMallocAsync(fista2d)"); }
+    const int hs = ((ny / 2) + (nx / 2)) & 1;
+    for (long long p0 = 0; p0 < nprob && e == cudaSuccess; p0 += chunk) {
+        oks::Fista2dArgs a{};
+        a.nprob = std::min(chunk, nprob - p0);
+        a.y = reinterpret_cast<const float2*>(d_kspace) + p0 * N;
+        a.y_stride = N;
+        // problem p0 + i uses mask (p0 + i) % nmask (mask_offset = p0 % nmask)
+        a.mask_mod = nmask;
+        a.mask_stride = N;
+        a.mask = static_cast<const uint8_t*>(slot->dev);
+        a.X = static_cast<float2*>(scratch) + 2 * chunk * N;
+        a.Z = static_cast<float2*>(scratch);
+        a.S = a.Z + chunk * N;
+        a.st_stride = N;
+        a.ny = ny; a.nx = nx;
+        a.ysc = std::sqrt((float)ny * (float)nx) * (hs ? -1.f : 1.f);
+        a.minv = 1.0f / ((float)ny * (float)nx);
+        a.lambda = lambda;
+        a.alpha = alpha;
+        a.mask_offset = p0 % nmask;
+        {
+            ProfScope ps(ctx, "k2d_col");
+            e = oks::launch_fista2d_col(a, *py, 0, ctx->stream);
+        }
+        if (e == cudaSuccess) {
+            ProfScope ps(ctx, "k2d_row");
+            e = oks::launch_fista2d_row(a, *px, 0, 0, ctx->stream);
+        }
+        for (int it = 0; it < iters && e == cudaSuccess; ++it) {
+            {
+                ProfScope ps(ctx, "k2d_col");
+                e = oks::launch_fista2d_col(a, *py, 1, ctx->stream);
+            }
+            if (e == cudaSuccess) {
+                ProfScope ps(ctx, "k2d_row");
+                e = oks::launch_fista2d_row(a, *px, 1, it, ctx->stream);
+            }
+        }
+        if (e == cudaSuccess) {
+            ProfScope ps(ctx, "k2d_demod");
+            e = oks::launch_fista2d_demod(a.X, reinterpret_cast<float2*>(d_out) + p0 * N, a.nprob, ny, nx, N, N, ctx->stream);
+        }
+    }
+    cudaFreeAsync(scratch, ctx->stream);
+    stage_release(ctx, slot);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "fista2d launch");
+    return OKS_OK;
+}
+
+// FISTA on `nprob` problems [nprob][ny][nx]; problem b uses mask b % nmask.
+int oks_fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nmask,
+                      long long nprob, int ny, int nx, int iters, float lambda, okscuda_c64* d_out) {
+    if (!h_mask || nmask <= 0 || nprob < 0 || ny <= 0 || nx <= 0 || iters < 0)
+        return set_err(ctx, OKS_EINVAL, "fista_cs: bad arguments");
+    if (ny % 2 || nx % 2)
+        return set_err(ctx, OKS_EODD, "CS: Ny (%d) and Nx (%d) must both be even for Haar wavelet", ny, nx);
+    if (nprob == 0) return OKS_OK;
+    if (!d_kspace || !d_out) return set_err(ctx, OKS_EINVAL, "fista_cs: null data pointer");
+    std::vector<uint32_t> words;
+    int wstride = 0;
+    if (!pack_row_masks(h_mask, nmask, ny, nx, &words, &wstride))
+        return fista2d_core(ctx, d_kspace, h_mask, nmask, nprob, ny, nx, iters, lambda, d_out);
+    const DevPlan *px, *py;
+    int rc = get_plan(ctx, nx, &px);
+    if (rc) return rc;
+    rc = get_plan(ctx, ny, &py);
+    if (rc) return rc;
+    const float* alpha = nullptr;
+    rc = get_alpha(ctx, iters, &alpha);
+    if (rc) return rc;
+    oks::Staging::Slot* slot = nullptr;
+    rc = stage_upload(ctx, words.data(), words.size() * sizeof(uint32_t), &slot);
+    if (rc) return rc;
+    oks::RowMasks rm{static_cast<const uint32_t*>(slot->dev), wstride, nmask};
 
     // y' = sqrt(ny) (-1)^{ny/2} (-1)^r * centred unitary row-IDFT of y
     float2* out = reinterpret_cast<float2*>(d_out);
     oks::RowXformArgs ra{};
     ra.in = reinterpret_cast<const float2*>(d_kspace);
     ra.out = out;
-    ra.nrows = (long long)batch * ny;
+    ra.nrows = nprob * ny;
     ra.ld_in = nx; ra.ld_out = nx;
     ra.sign = +1; ra.centred = 1;
     ra.scale = std::sqrt((float)ny) / std::sqrt((float)nx) * (((ny / 2) & 1) ? -1.0f : 1.0f);
     ra.rows_per_prob = ny; ra.rowsign = 1;
-    ra.use_keep = 1;
-    OKS_CUDA(oks::launch_row_xform(ra, bits, *px, ctx->stream));
-
-    oks::FistaColArgs fa{};
-    fa.ytil = out; fa.prob_stride = (long long)ny * nx;
-    fa.minv = 1.0f / (float)ny;
-    fa.xout = out; fa.out_stride = (long long)ny * nx;
-    fa.ny = ny; fa.nx = nx; fa.iters = iters; fa.lambda = lambda; fa.alpha = alpha;
-    fa.nprob = batch;
-    OKS_CUDA(oks::launch_fista_col(fa, bits, *py, ctx->stream));
+    ra.use_keep = 1; ra.keep = rm;
+    cudaError_t e;
+    {
+        ProfScope ps(ctx, "k_row_xform");
+        e = oks::launch_row_xform(ra, *px, ctx->stream);
+    }
+    if (e == cudaSuccess) {
+        oks::FistaColArgs fa{};
+        fa.ytil = out; fa.prob_stride = (long long)ny * nx;
+        fa.minv = 1.0f / (float)ny;
+        fa.mask = rm;
+        fa.xout = out; fa.out_stride = (long long)ny * nx;
+        fa.ny = ny; fa.nx = nx; fa.iters = iters; fa.lambda = lambda; fa.alpha = alpha;
+        fa.nprob = nprob;
+        ProfScope ps(ctx, "k_fista_col");
+        e = oks::launch_fista_col(fa, *py, ctx->stream);
+    }
+    stage_release(ctx, slot);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "fista_cs launch");
     return OKS_OK;
 }
 
 int okscuda_fista_cs(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int batch, int ny,
                      int nx, int iters, float lambda, okscuda_c64* d_out) {
     OKS_CHECK_CTX();
-    return fista_core(ctx, d_kspace, h_mask, batch, ny, nx, iters, lambda, d_out);
+    return oks_fista_core(ctx, d_kspace, h_mask, 1, batch, ny, nx, iters, lambda, d_out);
+}
+
+int okscuda_cs_volume(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nc, int nz,
+                      int ny, int nx, int iters, float lambda, int ty, int tx, float* d_rss,
+                      okscuda_c64* d_coils) {
+    OKS_CHECK_CTX();
+    if (!d_rss || nc < 0 || nz <= 0 || ty <= 0 || tx <= 0 || ty > ny || tx > nx)
+        return set_err(ctx, OKS_EINVAL, "cs_volume: bad arguments");
+    okscuda_c64* coils = d_coils;
+    void* own = nullptr;
+    const size_t bytes = sizeof(okscuda_c64) * (size_t)nc * nz * ny * nx;
+    if (!coils && bytes) {
+        OKS_CUDA(cudaMallocAsync(&own, bytes, ctx->stream));
+        coils = static_cast<okscuda_c64*>(own);
+    }
+    int rc = oks_fista_core(ctx, d_kspace, h_mask, nz, (long long)nc * nz, ny, nx, iters, lambda, coils);
+    if (rc == OKS_OK) {
+        oks::RssArgs a{};
+        a.coils = reinterpret_cast<const float2*>(coils);
+        a.coil_stride = (long long)nz * ny * nx;
+        a.nc = nc; a.ny = ny; a.nx = nx;
+        a.nslice = nz; a.slice_stride = (long long)ny * nx;
+        a.ty = ty; a.tx = tx; a.y0 = (ny - ty) / 2; a.x0 = (nx - tx) / 2;
+        a.out = d_rss;
+        ProfScope ps(ctx, "k_rss");
+        cudaError_t e = oks::launch_rss(a, ctx->stream);
+        if (e != cudaSuccess) rc = cuda_err(ctx, e, "rss");
+    }
+    if (own) cudaFreeAsync(own, ctx->stream);
+    return rc;
 }
 
 int okscuda_cs_slice(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nc, int ny,
                      int nx, int iters, float lambda, float* d_rss, okscuda_c64* d_coils) {
+    return okscuda_cs_volume(ctx, d_kspace, h_mask, nc, 1, ny, nx, iters, lambda, ny, nx, d_rss, d_coils);
+}
+
+// ---------------------------------------------------------------- profiling
+int okscuda_profile_enable(okscuda_ctx* ctx, int on) {
     OKS_CHECK_CTX();
-    if (!d_rss) return set_err(ctx, OKS_EINVAL, "cs_slice: null output");
-    okscuda_c64* coils = d_coils;
-    void* own = nullptr;
-    if (!coils) {
-        OKS_CUDA(cudaMallocAsync(&own, sizeof(okscuda_c64) * (size_t)nc * ny * nx, ctx->stream));
-        coils = static_cast<okscuda_c64*>(own);
+    OKS_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (auto& r : ctx->prof) { ctx->ev_pool.push_back(r.a); ctx->ev_pool.push_back(r.b); }
+    ctx->prof.clear();
+    ctx->prof_on = on != 0;
+    return OKS_OK;
+}
+
+int okscuda_profile_read(okscuda_ctx* ctx, char* names, int name_len, double* total_ms, long long* launches,
+                         int nslots, int* nfound) {
+    OKS_CHECK_CTX();
+    if (!nfound) return set_err(ctx, OKS_EINVAL, "profile_read: null count");
+    OKS_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<std::string> keys;
+    std::vector<double> ms;
+    std::vector<long long> cnt;
+    for (auto& r : ctx->prof) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        size_t k = 0;
+        for (; k < keys.size(); ++k)
+            if (keys[k] == r.name) break;
+        if (k == keys.size()) { keys.push_back(r.name); ms.push_back(0.0); cnt.push_back(0); }
+        ms[k] += t;
+        cnt[k] += 1;
     }
-    int rc = fista_core(ctx, d_kspace, h_mask, nc, ny, nx, iters, lambda, coils);
-    if (rc == OKS_OK) rc = okscuda_rss_crop(ctx, coils, nc, ny, nx, ny, nx, d_rss);
-    if (own) cudaFreeAsync(own, ctx->stream);
-    return rc;
+    *nfound = (int)keys.size();
+    for (int k = 0; k < (int)keys.size() && k < nslots; ++k) {
+        if (names && name_len > 0) std::snprintf(names + (size_t)k * name_len, name_len, "%s", keys[k].c_str());
+        if (total_ms) total_ms[k] = ms[k];
+        if (launches) launches[k] = cnt[k];
+    }
+    return OKS_OK;
 }
 
 }  // extern "C"

@@ -1,0 +1,173 @@
+// Private: the okscuda_ctx definition and helpers shared by the C-ABI
+// translation units (api.cu, strategy.cu).  Not part of the public header.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/okscuda.h"
+#include "kernels.h"
+#include "plan.h"
+
+using oks::DevPlan;
+
+struct okscuda_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    oks::PlanCache plans;
+    std::map<int, float*> alpha;          // iters -> device alpha table
+    // scratch (grow-only)
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    oks::Staging staging;
+    long long fista2d_chunk = 0;          // problems per 2-D-mask chunk (0 = auto)
+    // per-launch CUDA-event profiling (okscuda_profile_*)
+    bool prof_on = false;
+    struct ProfRec { const char* name; cudaEvent_t a, b; };
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> ev_pool;
+};
+
+namespace oks_internal {
+
+inline int set_err(okscuda_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+inline int cuda_err(okscuda_ctx* c, cudaError_t e, const char* where) {
+    return set_err(c, e == cudaErrorMemoryAllocation ? OKS_ENOMEM : OKS_ECUDA, "%s: %s (%s)", where,
+                   cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+#define OKS_CUDA(call)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_err(ctx, e_, #call); \
+    } while (0)
+
+#define OKS_CHECK_CTX()                                                  \
+    do {                                                                 \
+        if (!ctx) return OKS_EINVAL;                                     \
+        cudaError_t e0_ = cudaSetDevice(ctx->device);                    \
+        if (e0_ != cudaSuccess) return cuda_err(ctx, e0_, "cudaSetDevice"); \
+    } while (0)
+
+inline int ensure_scratch(okscuda_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->scratch_bytes) return OKS_OK;
+    if (ctx->scratch) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&ctx->scratch, bytes);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "cudaMalloc(scratch)");
+    ctx->scratch_bytes = bytes;
+    return OKS_OK;
+}
+
+// cs.rs:125-126 in f32, as the reference computes it.
+inline int get_alpha(okscuda_ctx* ctx, int iters, const float** out) {
+    auto it = ctx->alpha.find(iters);
+    if (it != ctx->alpha.end()) { *out = it->second; return OKS_OK; }
+    std::vector<float> h(iters > 0 ? iters : 1, 0.f);
+    float t = 1.0f;
+    for (int i = 0; i < iters; ++i) {
+        float t_new = 0.5f * (1.0f + std::sqrt(1.0f + 4.0f * t * t));
+        h[i] = (t - 1.0f) / t_new;
+        t = t_new;
+    }
+    float* d = nullptr;
+    OKS_CUDA(cudaMalloc(&d, sizeof(float) * h.size()));
+    OKS_CUDA(cudaMemcpy(d, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+    ctx->alpha[iters] = d;
+    *out = d;
+    return OKS_OK;
+}
+
+inline int get_plan(okscuda_ctx* ctx, int n, const DevPlan** out) {
+    std::string msg;
+    const DevPlan* p = ctx->plans.get(n, &msg);
+    if (!p) return set_err(ctx, OKS_ECUDA, "FFT plan for n=%d: %s", n, msg.c_str());
+    *out = p;
+    return OKS_OK;
+}
+
+// Small host->device uploads (masks, tables) through a ring of pinned slots:
+// the copy is enqueued on the context stream, and a slot is reused only after
+// the event recorded behind the kernels that read it has completed.
+inline int stage_upload(okscuda_ctx* ctx, const void* src, size_t bytes, oks::Staging::Slot** out) {
+    oks::Staging::Slot* s = &ctx->staging.slots[ctx->staging.next];
+    ctx->staging.next = (ctx->staging.next + 1) % oks::Staging::kSlots;
+    if (s->ev) OKS_CUDA(cudaEventSynchronize(s->ev));
+    else OKS_CUDA(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming));
+    if (bytes > s->cap) {
+        if (s->host) cudaFreeHost(s->host);
+        if (s->dev) cudaFree(s->dev);
+        s->host = s->dev = nullptr;
+        s->cap = 0;
+        size_t cap = bytes < 4096 ? 4096 : bytes;
+        OKS_CUDA(cudaMallocHost(&s->host, cap));
+        OKS_CUDA(cudaMalloc(&s->dev, cap));
+        s->cap = cap;
+    }
+    std::memcpy(s->host, src, bytes);
+    OKS_CUDA(cudaMemcpyAsync(s->dev, s->host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    *out = s;
+    return OKS_OK;
+}
+
+inline void stage_release(okscuda_ctx* ctx, oks::Staging::Slot* s) { cudaEventRecord(s->ev, ctx->stream); }
+
+inline cudaEvent_t prof_event(okscuda_ctx* ctx) {
+    if (!ctx->ev_pool.empty()) {
+        cudaEvent_t e = ctx->ev_pool.back();
+        ctx->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Records CUDA events around one kernel launch when profiling is on.
+struct ProfScope {
+    okscuda_ctx* ctx;
+    okscuda_ctx::ProfRec rec{};
+    ProfScope(okscuda_ctx* c, const char* name) : ctx(c) {
+        if (!ctx->prof_on) return;
+        rec.name = name;
+        rec.a = prof_event(ctx);
+        rec.b = prof_event(ctx);
+        cudaEventRecord(rec.a, ctx->stream);
+    }
+    ~ProfScope() {
+        if (!ctx->prof_on || !rec.a) return;
+        cudaEventRecord(rec.b, ctx->stream);
+        ctx->prof.push_back(rec);
+    }
+};
+
+}  // namespace oks_internal
+
+using namespace oks_internal;
+
+// FISTA on nprob problems [nprob][ny][nx] (problem b uses host mask b % nmask),
+// dispatching to the fused column engine (ky-only masks) or the 2-D engine.
+extern "C" int oks_fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nmask,
+                              long long nprob, int ny, int nx, int iters, float lambda, okscuda_c64* d_out);

@@ -1,0 +1,29 @@
+// Host-side launch interface of the feeding kernels (k_feed.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels.h"
+
+namespace oks {
+
+// One placed acquisition (geometry decided on the host from the headers,
+// reader.rs:332-457): samples [src_off, src_off + len) of acquisition `acq`
+// go to row (kz, ky), columns [dst_off, dst_off + len), reversed if `reverse`.
+struct PlaceEntry {
+    long long acq;
+    int kz, ky;
+    int dst_off, src_off, len;
+    int reverse;
+    int nc_fit;
+};
+
+cudaError_t launch_noise_fit(const float2* noise, int nc, long long ns, double denom, double2* partial_scratch,
+                             int max_parts, float2* W, double2* W64, int* status, cudaStream_t st);
+cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st);
+cudaError_t launch_os_remove(const float2* in, float2* out, long long nlines, const DevPlan& pe, const DevPlan& pr,
+                             cudaStream_t st);
+cudaError_t launch_place(const float2* src, int nc_src, int ns, const PlaceEntry* tab, long long nent, float2* kspace,
+                         int nz, int ny, int nx, cudaStream_t st);
+
+}  // namespace oks

@@ -24,7 +24,7 @@
 namespace oks {
 
 // ------------------------------------------------------------------ rows
-__global__ void k_row_xform(RowXformArgs a, RowBits keepb, FftPlan pl, const float2* __restrict__ gtw,
+__global__ void k_row_xform(RowXformArgs a, FftPlan pl, const float2* __restrict__ gtw,
                             const float2* __restrict__ groots, int roots_total, int rpc) {
     extern __shared__ float2 sm[];
     const int n = pl.n;
@@ -43,7 +43,7 @@ __global__ void k_row_xform(RowXformArgs a, RowBits keepb, FftPlan pl, const flo
         const long long row = row0 + lr;
         float2 v = make_float2(0.f, 0.f);
         if (row < a.nrows) {
-            if (!a.use_keep || row_on(keepb, (int)(row % a.rows_per_prob))) {
+            if (!a.use_keep || row_on(a.keep, row / a.rows_per_prob, (int)(row % a.rows_per_prob))) {
                 int src = m + c1;
                 if (src >= n) src -= n;
                 v = a.in[row * a.ld_in + src];
@@ -68,8 +68,7 @@ __global__ void k_row_xform(RowXformArgs a, RowBits keepb, FftPlan pl, const flo
 
 static int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-cudaError_t launch_row_xform(const RowXformArgs& a, const RowBits& keep, const DevPlan& pl,
-                             cudaStream_t st) {
+cudaError_t launch_row_xform(const RowXformArgs& a, const DevPlan& pl, cudaStream_t st) {
     const int n = pl.plan.n;
     if (a.nrows <= 0) return cudaSuccess;
     int rpc = 16384 / (2 * n);       // two ping-pong buffers within ~128 KB
@@ -83,7 +82,7 @@ cudaError_t launch_row_xform(const RowXformArgs& a, const RowBits& keep, const D
     if (nthr > 256) nthr = 256;
     if (nthr < 32) nthr = 32;
     long long grid = (a.nrows + rpc - 1) / rpc;
-    k_row_xform<<<(unsigned)grid, nthr, smem, st>>>(a, keep, pl.plan, pl.tw, pl.roots, pl.roots_total, rpc);
+    k_row_xform<<<(unsigned)grid, nthr, smem, st>>>(a, pl.plan, pl.tw, pl.roots, pl.roots_total, rpc);
     return cudaGetLastError();
 }
 
@@ -142,7 +141,7 @@ __device__ __forceinline__ float2 shrink(float2 c, float lam) {
     return c * ((m - lam) / m);
 }
 
-__global__ void k_fista_col(FistaColArgs a, RowBits mb, FftPlan pl, const float2* __restrict__ gtw,
+__global__ void k_fista_col(FistaColArgs a, FftPlan pl, const float2* __restrict__ gtw,
                             const float2* __restrict__ groots, int roots_total) {
     extern __shared__ float2 sm[];
     const int n = a.ny, n2 = 2 * n, nx = a.nx;
@@ -161,7 +160,7 @@ __global__ void k_fista_col(FistaColArgs a, RowBits mb, FftPlan pl, const float2
     const float2* yin = a.ytil + b * a.prob_stride + 2 * j;
     for (int q = tid; q < pl.tw_total; q += nthr) TW[q] = gtw[q];
     for (int q = tid; q < roots_total; q += nthr) RT[q] = groots[q];
-    for (int r = tid; r < n; r += nthr) M[r] = row_on(mb, r) ? a.minv : 0.f;
+    for (int r = tid; r < n; r += nthr) M[r] = row_on(a.mask, b, r) ? a.minv : 0.f;
     for (int q = tid; q < n2; q += nthr) Y[q] = yin[(long long)(q >> 1) * nx + (q & 1)];
     __syncthreads();
 
@@ -219,8 +218,7 @@ __global__ void k_fista_col(FistaColArgs a, RowBits mb, FftPlan pl, const float2
     }
 }
 
-cudaError_t launch_fista_col(const FistaColArgs& a, const RowBits& mask, const DevPlan& pl,
-                             cudaStream_t st) {
+cudaError_t launch_fista_col(const FistaColArgs& a, const DevPlan& pl, cudaStream_t st) {
     if (a.nprob <= 0 || a.nx <= 0) return cudaSuccess;
     const int n = a.ny;
     size_t smem = sizeof(float2) * ((size_t)10 * n + pl.plan.tw_total + pl.roots_total) +
@@ -232,17 +230,20 @@ cudaError_t launch_fista_col(const FistaColArgs& a, const RowBits& mask, const D
     if (nthr < 64) nthr = 64;
     if (nthr > 256) nthr = 256;
     dim3 grid(a.nx / 2, (unsigned)a.nprob);
-    k_fista_col<<<grid, nthr, smem, st>>>(a, mask, pl.plan, pl.tw, pl.roots, pl.roots_total);
+    k_fista_col<<<grid, nthr, smem, st>>>(a, pl.plan, pl.tw, pl.roots, pl.roots_total);
     return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ RSS
 __global__ void k_rss(RssArgs a) {
-    const long long npix = (long long)a.ty * a.tx;
+    const long long per = (long long)a.ty * a.tx;
+    const long long npix = per * a.nslice;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npix;
          q += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(q / a.tx), x = (int)(q - (long long)y * a.tx);
-        const long long src = (long long)(a.y0 + y) * a.nx + (a.x0 + x);
+        const long long sl = q / per;
+        const long long rem = q - sl * per;
+        const int y = (int)(rem / a.tx), x = (int)(rem - (long long)y * a.tx);
+        const long long src = sl * a.slice_stride + (long long)(a.y0 + y) * a.nx + (a.x0 + x);
         float s = 0.f;
         for (int c = 0; c < a.nc; ++c) {
             const float2 v = a.coils[c * a.coil_stride + src];
@@ -253,7 +254,7 @@ __global__ void k_rss(RssArgs a) {
 }
 
 cudaError_t launch_rss(const RssArgs& a, cudaStream_t st) {
-    const long long npix = (long long)a.ty * a.tx;
+    const long long npix = (long long)a.ty * a.tx * a.nslice;
     if (npix <= 0) return cudaSuccess;
     long long blocks = (npix + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;

@@ -1,0 +1,304 @@
+// sm_100a kernels that feed the FISTA-CS loop (the reference's read closure,
+// strategy.rs:807-815, and its calibration, strategy.rs:783-798):
+//   prewhiten.rs:48-111   noise covariance Psi           -> k_noise_cov (FP64, chunked, ordered sum)
+//   prewhiten.rs:148-210  Cholesky L, W = L^-1            -> k_chol_inv (FP64, one CTA)
+//   prewhiten.rs:118-142  s <- W s per sample column       -> k_prewhiten_apply
+//   oversampling.rs:103-155 centred IFFT/crop/FFT          -> k_os_remove
+//   reader.rs:332-457     line placement (first-wins, reverse, centring decided on the host)
+//                                                          -> k_place
+#include <cuda_runtime.h>
+#include <float.h>
+
+#include "fft_dev.cuh"
+#include "feed.h"
+
+namespace oks {
+
+// -------------------------------------------------------- noise covariance
+// Lower triangle (incl. diagonal) of sum_n s(n) s(n)^H over samples
+// [n0, n0 + chunk) of noise[nc][ns]; partial sums in FP64, one per CTA.
+__global__ void k_noise_cov(const float2* __restrict__ noise, int nc, long long ns, long long chunk,
+                            double2* __restrict__ partial) {
+    const long long n0 = blockIdx.x * chunk;
+    const long long n1 = min(ns, n0 + chunk);
+    const int npair = nc * (nc + 1) / 2;
+    double2* out = partial + (size_t)blockIdx.x * npair;
+    for (int q = threadIdx.x; q < npair; q += blockDim.x) {
+        // q -> (j, i) with j >= i : row-major lower triangle
+        int j = (int)((sqrt(8.0 * q + 1.0) - 1.0) / 2.0);
+        while ((j + 1) * (j + 2) / 2 <= q) ++j;
+        while (j * (j + 1) / 2 > q) --j;
+        const int i = q - j * (j + 1) / 2;
+        double re = 0.0, im = 0.0;
+        const float2* sj = noise + (long long)j * ns;
+        const float2* si = noise + (long long)i * ns;
+        for (long long n = n0; n < n1; ++n) {
+            const float2 a = sj[n], b = si[n];
+            // psi[j][i] += s_j * conj(s_i)      (prewhiten.rs:89-93)
+            re += (double)a.x * b.x + (double)a.y * b.y;
+            im += (double)a.y * b.x - (double)a.x * b.y;
+        }
+        out[q] = make_double2(re, im);
+    }
+}
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 zmulc(double2 a, double2 b) {   // a * conj(b)
+    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// Sums the partials in chunk order, scales by 1/max(total-1, 1), then
+// Cholesky (prewhiten.rs:148-179) and the triangular inverse
+// (prewhiten.rs:183-210), all in FP64.  status: 0 ok, 1 not positive
+// definite, 2 singular diagonal.  W (complex64, [nc][nc], upper zero) and
+// W64 (FP64) are written only when status == 0.
+__global__ void k_chol_inv(const double2* __restrict__ partial, int nparts, int nc, double denom,
+                           float2* __restrict__ W, double2* __restrict__ W64, int* __restrict__ status) {
+    extern __shared__ double2 zs[];
+    double2* A = zs;              // Psi   [nc][nc]
+    double2* L = A + nc * nc;     // L     [nc][nc]
+    double2* V = L + nc * nc;     // L^-1  [nc][nc]
+    __shared__ int bad;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int npair = nc * (nc + 1) / 2;
+    if (tid == 0) bad = 0;
+    for (int q = tid; q < nc * nc; q += nthr) {
+        A[q] = make_double2(0.0, 0.0);
+        L[q] = make_double2(0.0, 0.0);
+        V[q] = make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int q = tid; q < npair; q += nthr) {
+        int j = 0;
+        while ((j + 1) * (j + 2) / 2 <= q) ++j;
+        const int i = q - j * (j + 1) / 2;
+        double re = 0.0, im = 0.0;
+        for (int b = 0; b < nparts; ++b) {
+            re += partial[(size_t)b * npair + q].x;
+            im += partial[(size_t)b * npair + q].y;
+        }
+        A[j * nc + i] = make_double2(re / denom, im / denom);
+    }
+    __syncthreads();
+    for (int i = 0; i < nc; ++i) {
+        if (tid == 0) {
+            double2 d = A[i * nc + i];
+            for (int k = 0; k < i; ++k) {
+                const double2 t = zmulc(L[i * nc + k], L[i * nc + k]);
+                d.x -= t.x;
+                d.y -= t.y;
+            }
+            if (!(isfinite(d.x)) || d.x <= 0.0) bad = 1;
+            else L[i * nc + i] = make_double2(sqrt(d.x), 0.0);
+        }
+        __syncthreads();
+        if (bad) break;
+        const double inv = 1.0 / L[i * nc + i].x;
+        for (int j = i + 1 + tid; j < nc; j += nthr) {
+            double2 s = A[j * nc + i];
+            for (int k = 0; k < i; ++k) {
+                const double2 t = zmulc(L[j * nc + k], L[i * nc + k]);
+                s.x -= t.x;
+                s.y -= t.y;
+            }
+            L[j * nc + i] = make_double2(s.x * inv, s.y * inv);
+        }
+        __syncthreads();
+    }
+    if (bad) {
+        if (tid == 0) *status = 1;
+        return;
+    }
+    // forward substitution per unit column, one column per thread
+    for (int col = tid; col < nc; col += nthr) {
+        for (int i = 0; i < nc; ++i) {
+            double2 s = make_double2(i == col ? 1.0 : 0.0, 0.0);
+            for (int j = 0; j < i; ++j) {
+                const double2 t = zmul(L[i * nc + j], V[j * nc + col]);
+                s.x -= t.x;
+                s.y -= t.y;
+            }
+            const double2 d = L[i * nc + i];
+            if (fabs(d.x) < (double)FLT_EPSILON && fabs(d.y) < (double)FLT_EPSILON) {
+                atomicExch(&bad, 2);
+                break;
+            }
+            const double den = d.x * d.x + d.y * d.y;
+            V[i * nc + col] = make_double2((s.x * d.x + s.y * d.y) / den, (s.y * d.x - s.x * d.y) / den);
+        }
+    }
+    __syncthreads();
+    if (bad) {
+        if (tid == 0) *status = 2;
+        return;
+    }
+    for (int q = tid; q < nc * nc; q += nthr) {
+        const int i = q / nc, j = q - i * nc;
+        const double2 v = (j <= i) ? V[q] : make_double2(0.0, 0.0);
+        W[q] = make_float2((float)v.x, (float)v.y);
+        if (W64) W64[q] = v;
+    }
+    if (tid == 0) *status = 0;
+}
+
+// ------------------------------------------------------- prewhiten apply
+// data [nacq][nc][ns]: every sample column s -> W s (lower triangular).
+template <int NCMAX>
+__global__ void k_prewhiten_apply(float2* __restrict__ data, const float2* __restrict__ Wg, long long nacq, int nc,
+                                  int ns) {
+    __shared__ float2 W[NCMAX * NCMAX];
+    for (int q = threadIdx.x; q < nc * nc; q += blockDim.x) W[(q / nc) * NCMAX + q % nc] = Wg[q];
+    __syncthreads();
+    const long long total = nacq * ns;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long a = t / ns;
+        const int n = (int)(t - a * ns);
+        float2* col = data + a * nc * (long long)ns + n;
+        float2 s[NCMAX];
+#pragma unroll
+        for (int j = 0; j < NCMAX; ++j) s[j] = (j < nc) ? col[(long long)j * ns] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < NCMAX; ++i) {
+            if (i >= nc) break;
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j <= i; ++j) acc = acc + cmul(W[i * NCMAX + j], s[j]);
+            col[(long long)i * ns] = acc;
+        }
+    }
+}
+
+cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st) {
+    const long long total = nacq * ns;
+    if (total <= 0 || nc <= 0) return cudaSuccess;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (nc <= 8) k_prewhiten_apply<8><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns);
+    else if (nc <= 16) k_prewhiten_apply<16><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns);
+    else if (nc <= 32) k_prewhiten_apply<32><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns);
+    else if (nc <= 64) k_prewhiten_apply<64><<<(unsigned)blocks, 128, 0, st>>>(data, W, nacq, nc, ns);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_noise_fit(const float2* noise, int nc, long long ns, double denom, double2* partial_scratch,
+                             int max_parts, float2* W, double2* W64, int* status, cudaStream_t st) {
+    if (nc <= 0 || nc > 128) return cudaErrorInvalidValue;
+    long long chunk = 4096;
+    long long parts = (ns + chunk - 1) / chunk;
+    if (parts > max_parts) {
+        chunk = (ns + max_parts - 1) / max_parts;
+        parts = (ns + chunk - 1) / chunk;
+    }
+    if (parts < 1) parts = 1;
+    k_noise_cov<<<(unsigned)parts, 256, 0, st>>>(noise, nc, ns, chunk, partial_scratch);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t smem = sizeof(double2) * 3 * (size_t)nc * nc;
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k_chol_inv<<<1, 128, smem, st>>>(partial_scratch, (int)parts, nc, denom, W, W64, status);
+    return cudaGetLastError();
+}
+
+// -------------------------------------------------- oversampling removal
+// in [nlines][enc] -> out [nlines][rec]: ifftshift, IDFT, *1/enc, fftshift,
+// crop [(enc-rec)/2, +rec), ifftshift, DFT, fftshift (oversampling.rs:122-145).
+__global__ void k_os_remove(const float2* __restrict__ in, float2* __restrict__ out, long long nlines, int enc,
+                            int rec, FftPlan pe, const float2* __restrict__ twe, const float2* __restrict__ rte,
+                            int rte_n, FftPlan pr, const float2* __restrict__ twr, const float2* __restrict__ rtr,
+                            int rtr_n, int lpc) {
+    extern __shared__ float2 sm[];
+    float2* A = sm;
+    float2* B = A + (size_t)lpc * enc;
+    float2* TWE = B + (size_t)lpc * enc;
+    float2* RTE = TWE + pe.tw_total;
+    float2* TWR = RTE + rte_n;
+    float2* RTR = TWR + pr.tw_total;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    for (int q = tid; q < pe.tw_total; q += nthr) TWE[q] = twe[q];
+    for (int q = tid; q < rte_n; q += nthr) RTE[q] = rte[q];
+    for (int q = tid; q < pr.tw_total; q += nthr) TWR[q] = twr[q];
+    for (int q = tid; q < rtr_n; q += nthr) RTR[q] = rtr[q];
+    const long long l0 = (long long)blockIdx.x * lpc;
+    const int c1 = (enc + 1) / 2;
+    for (int q = tid; q < lpc * enc; q += nthr) {
+        const int l = q / enc, m = q - l * enc;
+        int src = m + c1;
+        if (src >= enc) src -= enc;
+        A[q] = (l0 + l < nlines) ? in[(l0 + l) * enc + src] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* X = fft_smem<+1, false>(A, A, B, pe, TWE, RTE, lpc, enc, 1, tid, nthr);
+    float2* C = (X == A) ? B : A;
+    // cropped[i] = fftshift(X)[start + i] = X[(start + i + enc/2) % enc];
+    // then the rec-point ifftshift: buf[m] = cropped[(m + ceil(rec/2)) % rec]
+    const int start = (enc - rec) / 2, h = enc / 2, cr = (rec + 1) / 2;
+    const float sc = 1.0f / (float)enc;
+    for (int q = tid; q < lpc * rec; q += nthr) {
+        const int l = q / rec, m = q - l * rec;
+        int i = m + cr;
+        if (i >= rec) i -= rec;
+        int k = start + i + h;
+        if (k >= enc) k -= enc;
+        C[l * rec + m] = X[l * enc + k] * sc;
+    }
+    __syncthreads();
+    float2* Y = fft_smem<-1, false>(C, C, X, pr, TWR, RTR, lpc, rec, 1, tid, nthr);
+    const int h2 = rec / 2;
+    for (int q = tid; q < lpc * rec; q += nthr) {
+        const int l = q / rec, k = q - l * rec;
+        if (l0 + l >= nlines) continue;
+        int src = k + h2;
+        if (src >= rec) src -= rec;
+        out[(l0 + l) * rec + k] = Y[l * rec + src];
+    }
+}
+
+cudaError_t launch_os_remove(const float2* in, float2* out, long long nlines, const DevPlan& pe, const DevPlan& pr,
+                             cudaStream_t st) {
+    const int enc = pe.plan.n, rec = pr.plan.n;
+    if (nlines <= 0) return cudaSuccess;
+    int lpc = 8192 / enc;
+    if (lpc < 1) lpc = 1;
+    if (lpc > 16) lpc = 16;
+    size_t smem = sizeof(float2) * ((size_t)2 * lpc * enc + pe.plan.tw_total + pe.roots_total + pr.plan.tw_total +
+                                    pr.roots_total);
+    cudaError_t e = cudaFuncSetAttribute(k_os_remove, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    long long grid = (nlines + lpc - 1) / lpc;
+    k_os_remove<<<(unsigned)grid, 256, smem, st>>>(in, out, nlines, enc, rec, pe.plan, pe.tw, pe.roots, pe.roots_total,
+                                                   pr.plan, pr.tw, pr.roots, pr.roots_total, lpc);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- placement
+// One placed acquisition per CTA row: kspace[c][kz][ky][dst + i] =
+// src[a][c][src_off + (reverse ? len-1-i : i)] for c < nc_fit, i < len.
+__global__ void k_place(const float2* __restrict__ src, int nc_src, int ns, const PlaceEntry* __restrict__ tab,
+                        long long nent, float2* __restrict__ kspace, int nz, int ny, int nx) {
+    for (long long e = blockIdx.x; e < nent; e += gridDim.x) {
+        const PlaceEntry t = tab[e];
+        const float2* s = src + t.acq * (long long)nc_src * ns;
+        for (int q = threadIdx.x; q < t.nc_fit * t.len; q += blockDim.x) {
+            const int c = q / t.len, i = q - c * t.len;
+            const int si = t.src_off + (t.reverse ? t.len - 1 - i : i);
+            kspace[(((long long)c * nz + t.kz) * ny + t.ky) * nx + t.dst_off + i] = s[(long long)c * ns + si];
+        }
+    }
+}
+
+cudaError_t launch_place(const float2* src, int nc_src, int ns, const PlaceEntry* tab, long long nent, float2* kspace,
+                         int nz, int ny, int nx, cudaStream_t st) {
+    if (nent <= 0) return cudaSuccess;
+    long long blocks = nent < 148 * 16 ? nent : 148 * 16;
+    k_place<<<(unsigned)blocks, 256, 0, st>>>(src, nc_src, ns, tab, nent, kspace, nz, ny, nx);
+    return cudaGetLastError();
+}
+
+}  // namespace oks

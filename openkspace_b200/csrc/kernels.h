@@ -16,12 +16,17 @@ struct DevPlan {
     int roots_total = 0;
 };
 
-// ky row mask passed by value as a kernel parameter (no per-call upload).
-constexpr int kMaxMaskRows = 4096;
-struct RowBits {
-    uint32_t w[kMaxMaskRows / 32];
+// ky row masks on the device: mask m is `wstride` 32-bit words at
+// words + m * wstride; row r is bit (r & 31) of word r >> 5.  Problem b uses
+// mask (b % mod) -- e.g. b = c * nz + kz with mod = nz gives one mask per slice.
+struct RowMasks {
+    const uint32_t* words;
+    int wstride;
+    int mod;
 };
-__host__ __device__ inline bool row_on(const RowBits& b, int r) { return (b.w[r >> 5] >> (r & 31)) & 1u; }
+__device__ __forceinline__ bool row_on(const RowMasks& m, long long prob, int r) {
+    return (__ldg(m.words + (prob % m.mod) * m.wstride + (r >> 5)) >> (r & 31)) & 1u;
+}
 
 // Batched transform of contiguous rows: out[row][k] for nrows rows of length n.
 struct RowXformArgs {
@@ -34,10 +39,10 @@ struct RowXformArgs {
     float scale;
     int rows_per_prob;   // row index r within a problem is row % rows_per_prob
     int rowsign;         // multiply row r by (-1)^r
-    int use_keep;        // rows r with row_on(keep, r) == false are zero
+    int use_keep;        // rows outside the problem's row mask are zero
+    RowMasks keep;
 };
-cudaError_t launch_row_xform(const RowXformArgs& a, const RowBits& keep, const DevPlan& pl,
-                             cudaStream_t st);
+cudaError_t launch_row_xform(const RowXformArgs& a, const DevPlan& pl, cudaStream_t st);
 
 // Batched transform along y of [nprob][ny][nx] in place.
 struct ColXformArgs {
@@ -54,7 +59,8 @@ cudaError_t launch_col_xform(const ColXformArgs& a, const DevPlan& pl, cudaStrea
 struct FistaColArgs {
     const float2* ytil;       // prepared hybrid data y' ([ny][nx] per problem)
     long long prob_stride;
-    float minv;               // m' = 1/ny on sampled rows (RowBits), 0 elsewhere
+    float minv;               // m' = 1/ny on sampled rows, 0 elsewhere
+    RowMasks mask;
     float2* xout;             // coil images x ([ny][nx] per problem); may alias ytil
     long long out_stride;
     int ny, nx, iters;
@@ -62,16 +68,42 @@ struct FistaColArgs {
     const float* alpha;       // [iters] FISTA momentum weights
     long long nprob;
 };
-cudaError_t launch_fista_col(const FistaColArgs& a, const RowBits& mask, const DevPlan& pl,
-                             cudaStream_t st);
+cudaError_t launch_fista_col(const FistaColArgs& a, const DevPlan& pl, cudaStream_t st);
 
-// RSS over coils with centre crop: out[(y)][(x)] = sqrt(sum_c |in_c[y0+y][x0+x]|^2)
+// FISTA for arbitrary 2-D masks (k_fista2d.cu): state X~, Z~, S per problem.
+struct Fista2dArgs {
+    const float2* y;          // k-space [ny][nx] per problem
+    long long y_stride;
+    const uint8_t* mask;      // byte masks [ny][nx]; problem p uses mask p % mask_mod
+    long long mask_stride;
+    int mask_mod;
+    long long mask_offset;    // problem p uses mask (p + mask_offset) % mask_mod
+    float2* X;
+    float2* Z;
+    float2* S;
+    long long st_stride;      // per-problem stride of X, Z, S
+    int ny, nx;
+    float ysc;                // (-1)^{ny/2 + nx/2} sqrt(ny nx)
+    float minv;               // 1 / (ny nx)
+    float lambda;
+    const float* alpha;
+    long long nprob;
+};
+cudaError_t launch_fista2d_col(const Fista2dArgs& a, const DevPlan& py, int mode, cudaStream_t st);
+cudaError_t launch_fista2d_row(const Fista2dArgs& a, const DevPlan& px, int mode, int it, cudaStream_t st);
+cudaError_t launch_fista2d_demod(const float2* X, float2* out, long long nprob, int ny, int nx, long long in_stride,
+                                 long long out_stride, cudaStream_t st);
+
+// RSS over coils with centre crop, per slice s:
+//   out[s][y][x] = sqrt(sum_c |coils[c * coil_stride + s * slice_stride + (y0+y) nx + x0+x]|^2)
 struct RssArgs {
-    const float2* coils;     // coil c at coils + c * coil_stride, [ny][nx]
+    const float2* coils;
     long long coil_stride;
     int nc, ny, nx;
+    int nslice;
+    long long slice_stride;
     int y0, x0, ty, tx;      // crop window
-    float* out;              // [ty][tx]
+    float* out;              // [nslice][ty][tx]
 };
 cudaError_t launch_rss(const RssArgs& a, cudaStream_t st);
 
@@ -80,5 +112,26 @@ cudaError_t launch_haar(const float2* in, float2* out, long long nprob, int ny, 
                         cudaStream_t st);
 cudaError_t launch_soft_threshold(float2* data, long long nprob, int ny, int nx, float lambda,
                                   cudaStream_t st);
+
+// Pinned host + device slots for small per-call uploads (see api.cu).
+struct Staging {
+    struct Slot {
+        void* host = nullptr;
+        void* dev = nullptr;
+        size_t cap = 0;
+        cudaEvent_t ev = nullptr;
+    };
+    static constexpr int kSlots = 8;
+    Slot slots[kSlots];
+    int next = 0;
+    void release() {
+        for (auto& s : slots) {
+            if (s.ev) cudaEventSynchronize(s.ev), cudaEventDestroy(s.ev);
+            if (s.host) cudaFreeHost(s.host);
+            if (s.dev) cudaFree(s.dev);
+            s = Slot{};
+        }
+    }
+};
 
 }  // namespace oks

@@ -186,6 +186,40 @@ class Context:
         """Same signature and meaning as the reference (cs.rs:59)."""
         return self.fista_cs(kspace_zf, mask, iters, lam)
 
+    def cs_volume(self, kspace, mask, iters: int, lam: float, crop=None, out: DeviceArray | None = None,
+                  coils: DeviceArray | None = None):
+        """strategy.rs:849-885 for placed k-space [nc, nz, ny, nx] with masks
+        [nz, ny, nx]; one batched launch for every (coil, slice).  Returns the
+        RSS volume [nz, ty, tx] (host) unless ``out`` is given."""
+        d, _ = self._dev(kspace)
+        nc, nz, ny, nx = d.shape
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        if m.shape != (nz, ny, nx):
+            raise OksError(_lib.OKS_ESHAPE, f"mask shape {m.shape} != {(nz, ny, nx)}")
+        ty, tx = crop if crop is not None else (ny, nx)
+        o = out if out is not None else self.empty((nz, ty, tx), np.float32)
+        self.check(self.lib.okscuda_cs_volume(self.handle, d.ptr, m.ctypes.data, nc, nz, ny, nx, int(iters),
+                                              float(lam), ty, tx, o.ptr, coils.ptr if coils else None))
+        return o if out is not None else o.to_host()
+
+    # -- profiling ----------------------------------------------------------
+    def profile(self, on: bool = True):
+        self.check(self.lib.okscuda_profile_enable(self.handle, int(on)))
+
+    def profile_read(self) -> dict:
+        """{kernel name: (total device ms, launches)} since profile(True)."""
+        n = 64
+        names = ctypes.create_string_buffer(64 * n)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_longlong * n)()
+        found = ctypes.c_int()
+        self.check(self.lib.okscuda_profile_read(self.handle, names, 64, ms, cnt, n, ctypes.byref(found)))
+        out = {}
+        for k in range(min(found.value, n)):
+            nm = names.raw[64 * k:64 * (k + 1)].split(b"\0", 1)[0].decode()
+            out[nm] = (ms[k], cnt[k])
+        return out
+
     def cs_slice(self, kspace, mask, iters: int, lam: float, return_coils: bool = False):
         """strategy.rs:850-880 for one slice: kspace [nc, ny, nx], mask [ny, nx]."""
         d, _ = self._dev(kspace)

@@ -159,3 +159,30 @@ def test_cs_slice_plain_workload(ctx):
     assert o64.nrmse(coils, x64) < TOL_CS
     rss32 = csref.csrss(s.kspace[:, None], m[None], 50, 0.01, nthreads=os.cpu_count() or 1)[0]
     assert rel_l2(rss, rss32) < TOL_CS
+
+
+def test_cs_volume_per_slice_masks(ctx, rng):
+    """strategy.rs:849-885: every slice has its own mask; RSS in coil order; crop."""
+    nc, nz, ny, nx = 3, 4, 32, 24
+    m = np.stack([row_mask(rng, ny, nx, 0.3 + 0.1 * z) for z in range(nz)])
+    k = np.where(m[None], crandn(rng, (nc, nz, ny, nx)), 0).astype(np.complex64)
+    rss = ctx.cs_volume(k, m, 15, 0.02)
+    want = o64.csrss_from_kspace(k, m, 15, 0.02)
+    assert o64.nrmse(rss, want) < TOL_CS
+    cropped = ctx.cs_volume(k, m, 15, 0.02, crop=(20, 10))
+    assert o64.nrmse(cropped, o64.maybe_crop(want, (10, 20, 1))) < TOL_CS
+    want32 = csref.csrss(k, m, 15, 0.02, nthreads=4)
+    assert rel_l2(rss, want32) < TOL_CS
+
+
+def test_profile_counts_launches(ctx, rng):
+    ny, nx = 16, 16
+    m = row_mask(rng, ny, nx)
+    k = np.where(m[None], crandn(rng, (2, ny, nx)), 0).astype(np.complex64)
+    d = ctx.to_device(k)
+    ctx.profile(True)
+    ctx.fista_cs(d, m, 5, 0.01, out=d)
+    p = ctx.profile_read()
+    ctx.profile(False)
+    assert p["k_fista_col"][1] == 1 and p["k_row_xform"][1] == 1
+    assert p["k_fista_col"][0] > 0

@@ -1,0 +1,76 @@
+"""Parity of the arbitrary-2-D-mask FISTA engine (masks not constant along kx,
+e.g. the partial rows the reference's reader produces after readout
+oversampling removal, reader.rs:394-457) against the oracle.  Tolerance:
+relative L2 <= 1e-4 vs the FP32 restatement and NRMSE <= 1e-4 vs FP64."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import cs_fp64 as o64
+from oracle import csref
+from tests.conftest import crandn, rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL_CS = 1e-4
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "cs_golden.npz")
+
+
+def partial_row_mask(rng, ny, nx, frac=0.35):
+    """ky rows sampled only over the central half of kx (the placement of a
+    readout shortened 2x by oversampling removal)."""
+    rows = rng.random(ny) < frac
+    rows[ny // 2 - 2:ny // 2 + 2] = True
+    m = np.zeros((ny, nx), bool)
+    m[rows, nx // 4:nx // 4 + nx // 2] = True
+    return m
+
+
+@pytest.mark.parametrize("ny,nx,iters", [(16, 16, 20), (24, 40, 25), (46, 20, 15), (64, 128, 10),
+                                         (368, 64, 8), (48, 640, 6), (2, 4, 5)])
+def test_partial_row_masks(ctx, rng, ny, nx, iters):
+    m = partial_row_mask(rng, ny, nx)
+    k = np.where(m[None], crandn(rng, (2, ny, nx)), 0).astype(np.complex64)
+    got = ctx.fista_cs(k, m, iters, 0.03)
+    assert rel_l2(got, o64.fista_cs_single_coil(k, m, iters, 0.03)) < TOL_CS
+    want32 = np.stack([csref.fista_cs_single_coil(k[c], m, iters, 0.03) for c in range(2)])
+    assert rel_l2(got, want32) < TOL_CS
+
+
+@pytest.mark.parametrize("ny,nx", [(20, 28), (32, 32), (10, 6)])
+def test_random_2d_masks(ctx, rng, ny, nx):
+    m = rng.random((ny, nx)) < 0.45
+    k = np.where(m[None], crandn(rng, (3, ny, nx)), 0).astype(np.complex64)
+    got = ctx.fista_cs(k, m, 20, 0.02)
+    assert rel_l2(got, o64.fista_cs_single_coil(k, m, 20, 0.02)) < TOL_CS
+
+
+def test_golden_2d_mask(ctx):
+    g = np.load(GOLDEN)
+    name = "rect20x28_2d"
+    k, m = g[f"{name}__kspace"], g[f"{name}__mask"].astype(bool)
+    iters, lam = g[f"{name}__params"]
+    assert not np.all(m == m[:, :1])
+    got = ctx.fista_cs(k, m, int(iters), float(lam))
+    assert rel_l2(got, g[f"{name}__x"]) < TOL_CS
+
+
+def test_2d_iters0_and_empty(ctx, rng):
+    ny, nx = 12, 16
+    m = partial_row_mask(rng, ny, nx)
+    k = np.where(m, crandn(rng, (ny, nx)), 0).astype(np.complex64)
+    assert rel_l2(ctx.fista_cs(k, m, 0, 0.01), o64.centred_ifft2(k)) < 1e-5
+    m0 = np.zeros((ny, nx), bool)
+    m0[3, 2] = True   # not constant along kx, one sample
+    z = ctx.fista_cs(k, m0, 4, 0.01)
+    assert rel_l2(z, o64.fista_cs_single_coil(k, m0, 4, 0.01)) < TOL_CS
+
+
+def test_volume_with_partial_rows_matches_oracle(ctx, rng):
+    """strategy.rs:849-885 with per-slice partial-row masks."""
+    nc, nz, ny, nx = 2, 3, 24, 32
+    m = np.stack([partial_row_mask(rng, ny, nx) for _ in range(nz)])
+    k = np.where(m[None], crandn(rng, (nc, nz, ny, nx)), 0).astype(np.complex64)
+    rss = ctx.cs_volume(k, m, 12, 0.02, crop=(24, 16))
+    want = o64.maybe_crop(o64.csrss_from_kspace(k, m, 12, 0.02), (16, 24, 1))
+    assert o64.nrmse(rss, want) < TOL_CS
