@@ -181,7 +181,9 @@ const char* okscuda_csrss_name(void);
  * oversampling removal, placement (reader.rs:225-468), kz decoupling,
  * odd-size fallback, per-slice per-coil FISTA, RSS, crop.  Writes the
  * magnitude volume [nz, ny, nx] (after crop) to h_out (host, capacity
- * out_cap floats) and its shape to out_dims[3].  OKS_EINVAL mirrors
+ * out_cap floats) and its shape to out_dims[3]; h_out == NULL queries the
+ * shape only.  When acqs->data_on_device is set, h_out is a device buffer
+ * too and the call returns without waiting for the GPU.  OKS_EINVAL mirrors
  * IoError::MissingField (no image acquisitions / zero channels);
  * OKS_ENOTSUP when phase_correct is set and navigator scans are present
  * (navigator phase correction is not part of this library). */

@@ -76,8 +76,8 @@ cudaError_t launch_row_xform(const RowXformArgs& a, const DevPlan& pl, cudaStrea
     if (rpc > 32) rpc = 32;
     if (rpc > a.nrows) rpc = (int)a.nrows;
     size_t smem = sizeof(float2) * ((size_t)2 * rpc * n + pl.plan.tw_total + pl.roots_total);
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_row_xform, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_row_xform, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     int nthr = round_up(rpc * n / 2, 32);
     if (nthr > 256) nthr = 256;
     if (nthr < 32) nthr = 32;
@@ -126,8 +126,8 @@ cudaError_t launch_col_xform(const ColXformArgs& a, const DevPlan& pl, cudaStrea
     if (tc > 16) tc = 16;
     if (tc < 1) tc = 1;
     size_t smem = sizeof(float2) * ((size_t)2 * tc * n + pl.plan.tw_total + pl.roots_total);
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_col_xform, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_col_xform, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     dim3 grid((a.nx + tc - 1) / tc, (unsigned)a.nprob);
     k_col_xform<<<grid, 256, smem, st>>>(a, pl.plan, pl.tw, pl.roots, pl.roots_total, tc);
     return cudaGetLastError();

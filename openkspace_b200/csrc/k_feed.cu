@@ -198,10 +198,8 @@ cudaError_t launch_noise_fit(const float2* noise, int nc, long long ns, double d
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     size_t smem = sizeof(double2) * 3 * (size_t)nc * nc;
-    if (smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
+    e = cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     k_chol_inv<<<1, 128, smem, st>>>(partial_scratch, (int)parts, nc, denom, W, W64, status);
     return cudaGetLastError();
 }

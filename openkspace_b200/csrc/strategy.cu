@@ -253,6 +253,18 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
     const int nz = use_slice_axis ? std::max(max_slice + 1, 1) : std::max(std::max(A->enc_z, max_kz + 1), 1);
     const int nc = nc_obs;
     const long long N = (long long)ny * nx;
+    // output shape after maybe_crop (strategy.rs:227-253)
+    int tz = nz, ty = ny, tx = nx;
+    if (cfg->crop_to_recon_matrix) {
+        const int cz = A->rec_z >= 2 ? std::min(A->rec_z, nz) : nz;
+        const int cy = A->rec_y >= 1 ? std::min(A->rec_y, ny) : ny;
+        const int cx = A->rec_x >= 1 ? std::min(A->rec_x, nx) : nx;
+        if (cz != nz || cy != ny || cx != nx) { tz = cz; ty = cy; tx = cx; }
+    }
+    out_dims[0] = tz; out_dims[1] = ty; out_dims[2] = tx;
+    const long long nout = (long long)tz * ty * tx;
+    if (!h_out) return OKS_OK;   // shape query
+    if (out_cap < nout) return set_err(ctx, OKS_EINVAL, "output buffer holds %lld floats, need %lld", out_cap, nout);
 
     // --- 3. second pass: preprocess + placement (reader.rs:332-457) ---------
     const int ky_off = ny / 2 - A->ky_center;
@@ -344,18 +356,6 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
         int rc = okscuda_ifft1_kz(ctx, dk.as<okscuda_c64>(), nc, nz, ny, nx);
         if (rc) return rc;
     }
-    // --- 5. output shape after maybe_crop (strategy.rs:227-253) -------------
-    int tz = nz, ty = ny, tx = nx;
-    if (cfg->crop_to_recon_matrix) {
-        const int cz = A->rec_z >= 2 ? std::min(A->rec_z, nz) : nz;
-        const int cy = A->rec_y >= 1 ? std::min(A->rec_y, ny) : ny;
-        const int cx = A->rec_x >= 1 ? std::min(A->rec_x, nx) : nx;
-        if (cz != nz || cy != ny || cx != nx) { tz = cz; ty = cy; tx = cx; }
-    }
-    out_dims[0] = tz; out_dims[1] = ty; out_dims[2] = tx;
-    const long long nout = (long long)tz * ty * tx;
-    if (!h_out) return OKS_OK;   // shape query
-    if (out_cap < nout) return set_err(ctx, OKS_EINVAL, "output buffer holds %lld floats, need %lld", out_cap, nout);
     const int z0 = (nz - tz) / 2;
 
     DevBuf coils(ctx), rss(ctx);
@@ -382,8 +382,11 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
         ProfScope ps(ctx, "k_rss");
         OKS_CUDA(oks::launch_rss(ra, ctx->stream));
     }
-    OKS_CUDA(cudaMemcpyAsync(h_out, rss.p, sizeof(float) * (size_t)nout, cudaMemcpyDeviceToHost, ctx->stream));
-    OKS_CUDA(cudaStreamSynchronize(ctx->stream));
+    // device-resident mode (data_on_device): h_out is a device buffer and the
+    // call returns without waiting
+    OKS_CUDA(cudaMemcpyAsync(h_out, rss.p, sizeof(float) * (size_t)nout,
+                             A->data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    if (!A->data_on_device) OKS_CUDA(cudaStreamSynchronize(ctx->stream));
     return OKS_OK;
 }
 
