@@ -107,6 +107,21 @@ int okscuda_cs_volume(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8
                       int nz, int ny, int nx, int iters, float lambda, int ty, int tx, float* d_rss,
                       okscuda_c64* d_coils);
 
+/* No counterpart in the reference.  okscuda_cs_slice for callers that cannot
+ * allocate device memory -- applications whose allocator owns all device
+ * memory (a framework memory pool, or a scanner pipeline that reserves its
+ * budget at start-up and forbids allocation later).  It allocates nothing:
+ * coil images, FFT tables, momentum weights and the row mask live in one
+ * fixed 16 MiB device array inside the library (held by every GPU that loads
+ * it until exit), so nc * ny * nx * 8 must fit 16 MiB - 256 KiB and ny, nx
+ * <= 2048 (else OKS_ENOTSUP).  ky-only masks only.  The caller still passes
+ * d_kspace[nc, ny, nx] and d_rss[ny, nx].  The first call on a device looks
+ * up the array's device address: make it before any stream capture.  All
+ * calls share the array, so calls that overlap on the GPU race: serialise
+ * them (one stream). */
+int okscuda_cs_slice_noalloc(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nc,
+                             int ny, int nx, int iters, float lambda, float* d_rss);
+
 /* ------------------------------------------------------- feeding stages */
 /* prewhiten.rs:48-111 + 148-210 in FP64 on the device.  d_noise[nc, ns] holds
  * the samples of every noise scan with nc channels (concatenated along

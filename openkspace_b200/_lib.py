@@ -55,6 +55,7 @@ SIGNATURES = {
     "okscuda_fista_cs": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp]),
     "okscuda_cs_slice": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp, _vp]),
     "okscuda_cs_volume": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _i, _i, _vp, _vp]),
+    "okscuda_cs_slice_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp]),
     "okscuda_prewhiten_fit": (_i, [_vp, _vp, _i, _c.c_longlong, _c.c_longlong, _vp]),
     "okscuda_prewhiten_apply": (_i, [_vp, _vp, _vp, _c.c_longlong, _i, _i]),
     "okscuda_os_remove": (_i, [_vp, _vp, _vp, _c.c_longlong, _i, _i]),
