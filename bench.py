@@ -181,8 +181,155 @@ class PrecisionWorkload:
         return dt, units, f"1 slice: full feeding pipeline + FISTA on {ncoil} of {self.nc} coils (scaled)"
 
 
+class BatchedWorkload:
+    """64 slices of uneven size {256^2, 320^2, 384^2, 368x640}, 8-32 coils,
+    R in {2,3,4,6} + 24 centre lines, 30-150 iterations, in one okscuda_cs_batch
+    call per step (one register-engine launch per column length, concurrent)."""
+    name = "batched"
+    dominant = "k_fista_col_reg"
+
+    def __init__(self, n: int = 64):
+        from openkspace_b200 import synth
+        self.reqs = synth.uneven_requests(n=n)
+        self.units = n
+
+    def config(self):
+        return {"workload": f"batched_uneven_{self.units}slices", "sizes": "256^2,320^2,384^2,368x640",
+                "coils": "U{8..32}", "accel": "{2,3,4,6} + 24 centre", "iters": "U{30..150}", "lambda": 0.01,
+                "coil_iters_px_total": int(sum(r.kspace.shape[0] * r.iters * r.kspace.shape[1] * r.kspace.shape[2]
+                                               for r in self.reqs))}
+
+    def input_bytes(self):
+        return sum(r.kspace.nbytes for r in self.reqs)
+
+    def dominant_bytes_per_step(self):
+        return 40.0 * sum(r.kspace.shape[0] * r.iters * r.kspace.shape[1] * r.kspace.shape[2] for r in self.reqs)
+
+    def prepare(self, ctx):
+        import torch
+        self.ctx = ctx
+        self.d_k = [ctx.to_device(r.kspace) for r in self.reqs]
+        self.masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in self.reqs]
+        self.d_out = [ctx.empty(r.kspace.shape[1:], np.float32) for r in self.reqs]
+        self.h_k = [torch.from_numpy(r.kspace.view(np.float32)).pin_memory() for r in self.reqs]
+        self.h_out = [torch.empty(r.kspace.shape[1:], dtype=torch.float32).pin_memory() for r in self.reqs]
+        self.args = [(d, m, r.iters, r.lam) for d, m, r in zip(self.d_k, self.masks, self.reqs)]
+
+    def step_device(self):
+        self.ctx.cs_batch(self.args, outs=self.d_out)
+
+    def step_e2e(self):
+        c = self.ctx
+        for d, h in zip(self.d_k, self.h_k):
+            c.check(c.lib.okscuda_upload(c.handle, d.ptr, h.data_ptr(), d.nbytes))
+        self.step_device()
+        for d, h in zip(self.d_out, self.h_out):
+            c.check(c.lib.okscuda_download(c.handle, h.data_ptr(), d.ptr, d.nbytes))
+
+    def e2e_bytes(self):
+        return self.input_bytes(), sum(int(np.prod(r.kspace.shape[1:])) * 4 for r in self.reqs)
+
+    def cpu_sample(self, nthreads):
+        from oracle import csref
+        r = min(self.reqs, key=lambda r: r.kspace.shape[0] * r.iters * r.kspace.size)
+        ncoil = max(1, min(r.kspace.shape[0], nthreads if nthreads > 1 else 2))
+        m = np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1)
+        t = time.perf_counter()
+        csref.csrss(r.kspace[:ncoil, None], m[None], r.iters, r.lam, nthreads=nthreads)
+        dt = time.perf_counter() - t
+        # scale by work: the whole batch's coil-iteration-pixels over the sample's
+        work = sum(q.kspace.shape[0] * q.iters * q.kspace.shape[1] * q.kspace.shape[2] for q in self.reqs)
+        sample = ncoil * r.iters * r.kspace.shape[1] * r.kspace.shape[2]
+        return dt, self.units * sample / work, f"{ncoil} coils of the lightest slice, scaled by coil-iteration-pixels"
+
+
 WORKLOADS = {"plain": lambda: PlainWorkload(1), "volume": lambda: PlainWorkload(36),
-             "precision": lambda: PrecisionWorkload(36)}
+             "precision": lambda: PrecisionWorkload(36), "batched": lambda: BatchedWorkload(64)}
+
+
+def run_serving(args):
+    """Poisson arrivals of single-slice requests (the batched workload's size /
+    coil / R / iteration distribution) at several rates through the request
+    server, beside the plain per-slice drop-in (okscuda_cs_slice, one at a
+    time, host buffers).  Latency = submit -> result on the host."""
+    import threading
+
+    import torch
+    from openkspace_b200 import Context, OksError, _lib, synth
+    from openkspace_b200.server import Server
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    pool = synth.uneven_requests(n=32, workload=3)
+    pinned = [torch.from_numpy(r.kspace.view(np.float32)).pin_memory().numpy().view(np.complex64) for r in pool]
+    masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in pool]
+    for k, m, r in zip(pinned[:4], masks[:4], pool[:4]):       # warm-up: plans, tables, pools
+        ctx.cs_slice(k, m, r.iters, r.lam)
+    # plain per-slice drop-in
+    lat = []
+    t0 = time.perf_counter()
+    for k, m, r in zip(pinned, masks, pool):
+        a = time.perf_counter()
+        ctx.cs_slice(k, m, r.iters, r.lam)
+        lat.append(time.perf_counter() - a)
+    plain_rate = len(pool) / (time.perf_counter() - t0)
+    plain = {"slices_per_s": plain_rate, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+             "p99_ms": 1e3 * float(np.percentile(lat, 99))}
+    rates = [float(x) for x in args.rates.split(",")]
+    out = {}
+    rng = np.random.default_rng(7)
+    with Server(ctx, max_inflight=48, n_streams=12) as srv:
+        for rid0 in range(4):                                   # warm the server path
+            i, _ = srv.submit(pinned[rid0], masks[rid0], pool[rid0].iters, pool[rid0].lam)
+            srv.wait(i, 120000)
+        for rate in rates:
+            nreq = int(min(args.requests, max(40, rate * args.seconds)))
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+            outs = [np.empty(pool[i % len(pool)].kspace.shape[1:], np.float32) for i in range(nreq)]
+            submitted, done = {}, {}
+            lock = threading.Lock()
+            start = time.perf_counter()
+
+            def submitter():
+                for n in range(nreq):
+                    j = n % len(pool)
+                    while time.perf_counter() - start < arrivals[n]:
+                        time.sleep(0.0002)
+                    while True:
+                        try:
+                            rid, _ = srv.submit(pinned[j], masks[j], pool[j].iters, pool[j].lam, out=outs[n])
+                            break
+                        except OksError as e:
+                            if e.code != _lib.OKS_EAGAIN:
+                                raise
+                            time.sleep(0.0002)
+                    with lock:
+                        submitted[rid] = start + arrivals[n]
+
+            th = threading.Thread(target=submitter)
+            th.start()
+            while len(done) < nreq:
+                with lock:
+                    pend = [r for r in submitted if r not in done]
+                for r in pend:
+                    if srv.poll(r):
+                        done[r] = time.perf_counter()
+                time.sleep(0.0002)
+            th.join()
+            span = max(done.values()) - start
+            lats = [done[r] - submitted[r] for r in done]
+            out[str(int(rate))] = {"requests": nreq, "slices_per_s": nreq / span,
+                                   "p50_ms": 1e3 * float(np.percentile(lats, 50)),
+                                   "p99_ms": 1e3 * float(np.percentile(lats, 99))}
+    best = max(out.values(), key=lambda v: v["slices_per_s"])
+    line = {"metric": "FISTA-CS slices/s + p50/p99 latency (served vs plain)", "value": best["slices_per_s"],
+            "unit": "slices/s", "n_gpus": 1, "higher_is_better": True, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "served_poisson", "rates_req_per_s": rates,
+                       "request_distribution": "sizes {256^2,320^2,384^2,368x640}, coils U{8..32}, R {2,3,4,6}, "
+                                               "iters U{30..150}, lambda 0.01",
+                       "latency": "submit -> result in pinned host memory (host clock)"},
+            "served": out, "plain": plain, "served_over_plain": best["slices_per_s"] / plain_rate}
+    print(json.dumps(line), flush=True)
+    ctx.close()
 
 
 # ------------------------------------------------------------ measurement
@@ -260,14 +407,21 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="plain", choices=sorted(WORKLOADS) + ["served"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rates", default="50,200,800", help="served: Poisson arrival rates (req/s)")
+    ap.add_argument("--seconds", type=float, default=4.0, help="served: arrivals per rate x this many seconds")
+    ap.add_argument("--requests", type=int, default=2000, help="served: at most this many requests per rate")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "served":
+        if rank == 0 and args.impl == "ours":
+            run_serving(args)
+        return
     wl = WORKLOADS[args.workload]()
 
     if args.impl == "reference":

@@ -56,6 +56,13 @@ int okscuda_set_stream(okscuda_ctx* ctx, void* stream);
 void* okscuda_get_stream(okscuda_ctx* ctx);
 int okscuda_synchronize(okscuda_ctx* ctx);
 const char* okscuda_version(void);
+/* Tuning knobs (no reference counterpart):
+ *   "col_engine"    ky-only masks: 0 auto (register-resident kernel where a
+ *                   compile-time plan exists for ny), 1 generic shared-memory
+ *                   kernel, 2 register kernel (falls back to 1 for other ny)
+ *   "fista2d_chunk" problems per chunk of the 2-D-mask engine (0 = auto,
+ *                   sized for L2 residency) */
+int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value);
 
 /* ---------------------------------------------------------- device memory */
 int okscuda_malloc(okscuda_ctx* ctx, size_t bytes, void** d_ptr);
@@ -106,6 +113,53 @@ int okscuda_cs_slice(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_
 int okscuda_cs_volume(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nc,
                       int nz, int ny, int nx, int iters, float lambda, int ty, int tx, float* d_rss,
                       okscuda_c64* d_coils);
+
+/* A list of independent slices of uneven size, coil count, iteration count,
+ * lambda and mask (strategy.rs:850-880 for each), solved together: one
+ * launch of the register-resident column engine per column length, units
+ * ordered longest-first, length groups on concurrent streams.  Slices with
+ * masks that vary along kx take the per-slice path. */
+typedef struct {
+    const okscuda_c64* d_kspace;   /* [nc, ny, nx] placed k-space             */
+    const uint8_t* h_mask;         /* [ny, nx] host mask                      */
+    int nc, ny, nx, iters;
+    float lambda;
+    float* d_rss;                  /* [ny, nx] RSS output                     */
+    okscuda_c64* d_coils;          /* [nc, ny, nx] coil images, or NULL       */
+} okscuda_slice_req;
+int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs, int n);
+
+/* ------------------------------------------------------- request server */
+/* No counterpart in the reference (which reconstructs one file at a time).
+ * A request is one slice (strategy.rs:850-880).  Each admitted request runs
+ * upload -> FISTA -> RSS -> download on one stream of a pool, so requests
+ * that arrive while others run overlap with them on the GPU.  Admission is
+ * by an HBM budget and an in-flight limit: okscuda_server_submit returns
+ * OKS_EAGAIN when the request does not fit now.  Host buffers of a request
+ * must stay valid until it completes (pinned memory keeps the copies
+ * asynchronous).  submit / poll / wait / stats are thread-safe. */
+typedef struct okscuda_server okscuda_server;
+typedef struct {
+    int max_inflight;              /* 0: 32                                    */
+    size_t hbm_budget_bytes;       /* 0: half the free device memory           */
+    int n_streams;                 /* 0: 8                                     */
+} okscuda_server_cfg;
+typedef struct {
+    const okscuda_c64* h_kspace;   /* [nc, ny, nx] host k-space, or NULL ...   */
+    const okscuda_c64* d_kspace;   /* ... device k-space (left unmodified)     */
+    const uint8_t* h_mask;         /* [ny, nx]                                 */
+    int nc, ny, nx, iters;
+    float lambda;
+    float* h_rss;                  /* [ny, nx] host output                     */
+} okscuda_request;
+int okscuda_server_create(okscuda_ctx* ctx, const okscuda_server_cfg* cfg, okscuda_server** out);
+void okscuda_server_destroy(okscuda_server* srv);
+int okscuda_server_submit(okscuda_server* srv, const okscuda_request* req, uint64_t* id);
+/* *done = 1 once the request finished; returns its status then and forgets it. */
+int okscuda_server_poll(okscuda_server* srv, uint64_t id, int* done);
+/* Bounded wait: OKS_ETIMEDOUT after timeout_ms (< 0: no limit). */
+int okscuda_server_wait(okscuda_server* srv, uint64_t id, int timeout_ms);
+int okscuda_server_stats(okscuda_server* srv, long long* inflight, long long* completed, size_t* reserved_bytes);
 
 /* No counterpart in the reference.  okscuda_cs_slice for callers that cannot
  * allocate device memory -- applications whose allocator owns all device

@@ -41,6 +41,7 @@ SIGNATURES = {
     "okscuda_get_stream": (_vp, [_vp]),
     "okscuda_synchronize": (_i, [_vp]),
     "okscuda_version": (_c.c_char_p, []),
+    "okscuda_set_option": (_i, [_vp, _c.c_char_p, _c.c_longlong]),
     "okscuda_malloc": (_i, [_vp, _sz, _c.POINTER(_vp)]),
     "okscuda_free": (_i, [_vp, _vp]),
     "okscuda_upload": (_i, [_vp, _vp, _vp, _sz]),
@@ -56,6 +57,14 @@ SIGNATURES = {
     "okscuda_cs_slice": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp, _vp]),
     "okscuda_cs_volume": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _i, _i, _vp, _vp]),
     "okscuda_cs_slice_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp]),
+    "okscuda_cs_batch": (_i, [_vp, _vp, _i]),
+    "okscuda_server_create": (_i, [_vp, _vp, _c.POINTER(_vp)]),
+    "okscuda_server_destroy": (None, [_vp]),
+    "okscuda_server_submit": (_i, [_vp, _vp, _c.POINTER(_c.c_uint64)]),
+    "okscuda_server_poll": (_i, [_vp, _c.c_uint64, _c.POINTER(_i)]),
+    "okscuda_server_wait": (_i, [_vp, _c.c_uint64, _i]),
+    "okscuda_server_stats": (_i, [_vp, _c.POINTER(_c.c_longlong), _c.POINTER(_c.c_longlong),
+                                  _c.POINTER(_sz)]),
     "okscuda_prewhiten_fit": (_i, [_vp, _vp, _i, _c.c_longlong, _c.c_longlong, _vp]),
     "okscuda_prewhiten_apply": (_i, [_vp, _vp, _vp, _c.c_longlong, _i, _i]),
     "okscuda_os_remove": (_i, [_vp, _vp, _vp, _c.c_longlong, _i, _i]),

@@ -35,8 +35,25 @@ void okscuda_destroy(okscuda_ctx* ctx) {
     for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto e : ctx->ev_pool) cudaEventDestroy(e);
     ctx->plans.clear();
+    if (ctx->reg_tables.base) cudaFree(ctx->reg_tables.base);
+    for (auto& a : ctx->aux) { cudaStreamDestroy(a.stream); cudaEventDestroy(a.done); }
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+}
+
+int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
+    if (!ctx || !name) return OKS_EINVAL;
+    if (!std::strcmp(name, "col_engine")) {
+        if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "col_engine: 0 auto, 1 generic, 2 register");
+        ctx->col_engine = (int)value;
+    } else if (!std::strcmp(name, "fista2d_chunk")) {
+        if (value < 0) return set_err(ctx, OKS_EINVAL, "fista2d_chunk must be >= 0");
+        ctx->fista2d_chunk = value;
+    } else {
+        return set_err(ctx, OKS_EINVAL, "unknown option '%s'", name);
+    }
+    return OKS_OK;
 }
 
 int okscuda_last_error(const okscuda_ctx* ctx, char* buf, size_t len) {
@@ -325,8 +342,15 @@ int oks_fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t*
         fa.xout = out; fa.out_stride = (long long)ny * nx;
         fa.ny = ny; fa.nx = nx; fa.iters = iters; fa.lambda = lambda; fa.alpha = alpha;
         fa.nprob = nprob;
-        ProfScope ps(ctx, "k_fista_col");
-        e = oks::launch_fista_col(fa, *py, ctx->stream);
+        const bool use_reg = ctx->col_engine != 1 && oks::fista_col_reg_supported(ny);
+        if (use_reg) e = oks::reg_tables_init(&ctx->reg_tables);
+        if (e == cudaSuccess && use_reg) {
+            ProfScope ps(ctx, "k_fista_col_reg");
+            e = oks::launch_fista_col_reg(fa, ctx->reg_tables, ctx->stream);
+        } else if (e == cudaSuccess) {
+            ProfScope ps(ctx, "k_fista_col");
+            e = oks::launch_fista_col(fa, *py, ctx->stream);
+        }
     }
     stage_release(ctx, slot);
     if (e != cudaSuccess) return cuda_err(ctx, e, "fista_cs launch");

@@ -30,6 +30,11 @@ struct okscuda_ctx {
     size_t scratch_bytes = 0;
     oks::Staging staging;
     long long fista2d_chunk = 0;          // problems per 2-D-mask chunk (0 = auto)
+    int col_engine = 0;                   // ky-only masks: 0 auto, 1 generic smem, 2 register-resident
+    oks::RegTables reg_tables;
+    struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
+    std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)
+    cudaEvent_t fork_ev = nullptr;
     // per-launch CUDA-event profiling (okscuda_profile_*)
     bool prof_on = false;
     struct ProfRec { const char* name; cudaEvent_t a, b; };
@@ -148,20 +153,37 @@ inline cudaEvent_t prof_event(okscuda_ctx* ctx) {
 // Records CUDA events around one kernel launch when profiling is on.
 struct ProfScope {
     okscuda_ctx* ctx;
+    cudaStream_t st;
     okscuda_ctx::ProfRec rec{};
-    ProfScope(okscuda_ctx* c, const char* name) : ctx(c) {
+    ProfScope(okscuda_ctx* c, const char* name, cudaStream_t s = nullptr) : ctx(c), st(s ? s : c->stream) {
         if (!ctx->prof_on) return;
         rec.name = name;
         rec.a = prof_event(ctx);
         rec.b = prof_event(ctx);
-        cudaEventRecord(rec.a, ctx->stream);
+        cudaEventRecord(rec.a, st);
     }
     ~ProfScope() {
         if (!ctx->prof_on || !rec.a) return;
-        cudaEventRecord(rec.b, ctx->stream);
+        cudaEventRecord(rec.b, st);
         ctx->prof.push_back(rec);
     }
 };
+
+// Auxiliary streams for fork/join inside one entry point.
+inline int ensure_aux_streams(okscuda_ctx* ctx, int n) {
+    if (!ctx->fork_ev) {
+        cudaError_t e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "fork event");
+    }
+    while ((int)ctx->aux.size() < n) {
+        okscuda_ctx::Aux a;
+        cudaError_t e = cudaStreamCreateWithFlags(&a.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a.done, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "aux stream");
+        ctx->aux.push_back(a);
+    }
+    return OKS_OK;
+}
 
 }  // namespace oks_internal
 

@@ -1,0 +1,525 @@
+// Register-resident fused column FISTA for ky-only masks (sm_100a).
+//
+// Same mathematics as k_fista_col (k_cs.cu header comment): one column pair
+// (2j, 2j+1) of one coil runs every FISTA iteration on chip.  Here the state
+// lives in registers:
+//   * a group of T threads owns one column pair; thread t holds the elements
+//     q = t + TA*e (e < E = 2N/TA) of the interleaved pair, q = 2*row + col,
+//     for x~, z~, y' and the work vector (TA = active threads, T = TA rounded
+//     up to whole warps);
+//   * every Stockham stage reads its inputs at rows i + j N/R, which for the
+//     first forward stage and the fused middle are exactly the thread's own
+//     registers (R | E); intermediate stages exchange through padded shared
+//     memory (index + index/32 keeps the strided writes conflict-free);
+//   * the last forward stage, the data residual and the first inverse stage
+//     (same radix) run back to back in registers;
+//   * the 2x2 Haar blocks pair q^1 (column) and q^2 (row): two xor-shuffle
+//     Hadamard steps forward, two back.
+// Only y' in and the coil image out touch global memory.
+#include <cuda_runtime.h>
+
+#include "fft_dev.cuh"
+#include "kernels.h"
+
+namespace oks {
+namespace reg {
+
+__device__ __forceinline__ int padi(int i) { return i + (i >> 5); }
+
+template <int SIGN, int R>
+__device__ __forceinline__ void bfly(float2* v, const float2* __restrict__ roots) {
+    if constexpr (R == 2) bfly2<SIGN>(v);
+    else if constexpr (R == 3) bfly3<SIGN>(v);
+    else if constexpr (R == 4) bfly4<SIGN>(v);
+    else if constexpr (R == 5) bfly5<SIGN>(v);
+    else if constexpr (R == 8) bfly8<SIGN>(v);
+    else if constexpr (R == 16) bfly16<SIGN>(v);
+    else if constexpr (R == 6) {           // 3 x 2
+        float2 a[3] = {v[0], v[2], v[4]}, b[3] = {v[1], v[3], v[5]};
+        bfly3<SIGN>(a);
+        bfly3<SIGN>(b);
+        // w6^k = cos(pi k/3) + SIGN i sin(pi k/3)
+        const float h = 0.86602540378443864676f;
+        float2 b1 = cmul(b[1], make_float2(0.5f, SIGN * h));
+        float2 b2 = cmul(b[2], make_float2(-0.5f, SIGN * h));
+        v[0] = a[0] + b[0]; v[3] = a[0] - b[0];
+        v[1] = a[1] + b1;   v[4] = a[1] - b1;
+        v[2] = a[2] + b2;   v[5] = a[2] - b2;
+    } else if constexpr (R == 10) {        // 5 x 2
+        float2 a[5] = {v[0], v[2], v[4], v[6], v[8]}, b[5] = {v[1], v[3], v[5], v[7], v[9]};
+        bfly5<SIGN>(a);
+        bfly5<SIGN>(b);
+        // w10^k = cos(pi k/5) + SIGN i sin(pi k/5)
+        const float c1 = 0.80901699437494742410f, s1 = 0.58778525229247312917f;
+        const float c2 = 0.30901699437494742410f, s2 = 0.95105651629515357212f;
+        const float2 w[5] = {make_float2(1.f, 0.f), make_float2(c1, SIGN * s1), make_float2(c2, SIGN * s2),
+                             make_float2(-c2, SIGN * s2), make_float2(-c1, SIGN * s1)};
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const float2 tb = cmul(b[k], w[k]);
+            v[k] = a[k] + tb;
+            v[k + 5] = a[k] - tb;
+        }
+    } else if constexpr (R == 12) {        // 3 x 4
+        float2 a[4] = {v[0], v[3], v[6], v[9]}, b[4] = {v[1], v[4], v[7], v[10]}, c[4] = {v[2], v[5], v[8], v[11]};
+        bfly4<SIGN>(a);
+        bfly4<SIGN>(b);
+        bfly4<SIGN>(c);
+        // y[k + 4m] = sum_l w12^{l k} (DFT4 of x[l + 3n])[k] w3^{l m}
+        const float c1 = 0.86602540378443864676f, s1 = 0.5f;
+        const float2 w1[4] = {make_float2(1.f, 0.f), make_float2(c1, SIGN * s1), make_float2(s1, SIGN * c1),
+                              make_float2(0.f, SIGN * 1.f)};
+        const float2 w2[4] = {make_float2(1.f, 0.f), make_float2(s1, SIGN * c1), make_float2(-s1, SIGN * c1),
+                              make_float2(-1.f, 0.f)};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float2 t[3] = {a[k], cmul(b[k], w1[k]), cmul(c[k], w2[k])};
+            bfly3<SIGN>(t);
+            v[k] = t[0]; v[k + 4] = t[1]; v[k + 8] = t[2];
+        }
+    } else {
+        static_assert(R % 2 == 1, "unsupported even radix");
+        bfly_odd<SIGN, R>(v, roots);
+    }
+}
+
+// Plans: N, active threads TA, stage radices.
+template <int N_, int TA_, int... Rs>
+struct Plan {
+    static constexpr int N = N_;
+    static constexpr int TA = TA_;
+    static constexpr int T = (TA_ + 31) / 32 * 32;
+    static constexpr int E = 2 * N_ / TA_;
+    static constexpr int S = sizeof...(Rs);
+    static constexpr int R[S] = {Rs...};
+    static_assert(2 * N_ % TA_ == 0, "TA must divide 2N");
+    static_assert(TA_ % 4 == 0, "TA must be a multiple of 4");
+    static constexpr int prod(int k) {   // product of the first k radices
+        int p = 1;
+        for (int s = 0; s < k; ++s) p *= R[s];
+        return p;
+    }
+    static constexpr int rprod(int k) {  // product of the first k radices of the reversed order
+        int p = 1;
+        for (int s = 0; s < k; ++s) p *= R[S - 1 - s];
+        return p;
+    }
+    static_assert(prod(S) == N_, "radices must multiply to N");
+    static_assert(E % R[0] == 0 && E % R[S - 1] == 0, "first and last radix must divide E");
+    static constexpr int SMEM_X = 2 * N_ + (2 * N_) / 32 + 1;   // padded exchange buffer (float2)
+};
+
+// Twiddle table offsets: forward stage s at tw_f(s), inverse stage s at
+// tw_i(s); entries k*(R-1) + j-1 = w_{pR}^{jk} (forward sign).
+template <class P>
+struct Tw {
+    static constexpr int fwd(int s) {
+        int o = 0;
+        for (int u = 0; u < s; ++u) o += P::prod(u) * (P::R[u] - 1);
+        return o;
+    }
+    static constexpr int inv(int s) {
+        int o = fwd(P::S);
+        for (int u = 0; u < s; ++u) o += P::rprod(u) * (P::R[P::S - 1 - u] - 1);
+        return o;
+    }
+    static constexpr int total() { return inv(P::S); }
+};
+
+// One stage over smem for intermediate stages: items f = t + TA*b, both
+// columns, any radix.  src/dst are padded exchange buffers.
+template <class P, int SIGN, int R, int p>
+__device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float2* __restrict__ dst,
+                                           const float2* __restrict__ tw, const float2* __restrict__ roots, int t) {
+    constexpr int NB = P::N / R;
+    constexpr int ITEMS = 2 * NB;
+    if (P::TA != P::T && t >= P::TA) return;   // padding lanes own no element
+#pragma unroll
+    for (int b = 0; b < (ITEMS + P::TA - 1) / P::TA; ++b) {
+        const int f = t + P::TA * b;
+        if (ITEMS % P::TA != 0 && f >= ITEMS) break;
+        const int i = f >> 1, c = f & 1;
+        const int k = i % p;
+        float2 v[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            float2 x = src[padi(2 * (i + j * NB) + c)];
+            if (j > 0 && p > 1) x = twmul<SIGN>(x, tw[k * (R - 1) + j - 1]);
+            v[j] = x;
+        }
+        bfly<SIGN, R>(v, roots);
+        const int ob = (i - k) * R + k;
+#pragma unroll
+        for (int j = 0; j < R; ++j) dst[padi(2 * (ob + j * p) + c)] = v[j];
+    }
+}
+
+// A stage whose inputs are the thread's registers (w[b + j*E/R]); writes its
+// outputs to smem (exchange) or, when p*R == N, back into w in place.
+template <class P, int SIGN, int R, int p>
+__device__ __forceinline__ void stage_reg(float2* w, float2* __restrict__ dst, const float2* __restrict__ tw,
+                                          const float2* __restrict__ roots, int t) {
+    constexpr int BR = P::E / R;   // butterflies per thread
+    constexpr bool LAST = (p * R == P::N);
+    if (P::TA != P::T && t >= P::TA) return;
+#pragma unroll
+    for (int b = 0; b < BR; ++b) {
+        const int f = t + P::TA * b;
+        const int i = f >> 1, c = f & 1;
+        const int k = LAST ? i : (i % p);
+        float2 v[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            float2 x = w[b + j * BR];
+            if (j > 0 && p > 1) x = twmul<SIGN>(x, tw[k * (R - 1) + j - 1]);
+            v[j] = x;
+        }
+        bfly<SIGN, R>(v, roots);
+        if constexpr (LAST) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) w[b + j * BR] = v[j];
+        } else {
+            const int ob = (i - k) * R + k;
+#pragma unroll
+            for (int j = 0; j < R; ++j) dst[padi(2 * (ob + j * p) + c)] = v[j];
+        }
+    }
+}
+
+// Last stage reading smem, writing the thread's registers (p*R == N).
+template <class P, int SIGN, int R, int p>
+__device__ __forceinline__ void stage_to_reg(const float2* __restrict__ src, float2* w, const float2* __restrict__ tw,
+                                             const float2* __restrict__ roots, int t) {
+    static_assert(p * R == P::N, "stage_to_reg is the last stage");
+    constexpr int NB = P::N / R;
+    constexpr int BR = P::E / R;
+    if (P::TA != P::T && t >= P::TA) return;
+#pragma unroll
+    for (int b = 0; b < BR; ++b) {
+        const int f = t + P::TA * b;
+        const int i = f >> 1, c = f & 1;
+        float2 v[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            float2 x = src[padi(2 * (i + j * NB) + c)];
+            if (j > 0) x = twmul<SIGN>(x, tw[i * (R - 1) + j - 1]);
+            v[j] = x;
+        }
+        bfly<SIGN, R>(v, roots);
+#pragma unroll
+        for (int j = 0; j < R; ++j) w[b + j * BR] = v[j];
+    }
+}
+
+template <class P>
+__device__ __forceinline__ void group_sync() {
+    if constexpr (P::T == 32) __syncwarp();
+    else __syncthreads();
+}
+
+// Forward transform: registers (state layout) -> registers (mid layout of
+// the last radix).  Stages 0..S-2 go through smem buffers A/B.
+template <class P, int s>
+__device__ __forceinline__ void fwd_rest(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
+                                         int t) {
+    if constexpr (s < P::S) {
+        constexpr int R = P::R[s];
+        constexpr int p = P::prod(s);
+        constexpr int off = Tw<P>::fwd(s);
+        float2* src = (s % 2 == 1) ? A : B;
+        float2* dst = (s % 2 == 1) ? B : A;
+        if constexpr (s == P::S - 1) {
+            stage_to_reg<P, -1, R, p>(src, w, tw + off, roots, t);
+        } else {
+            stage_smem<P, -1, R, p>(src, dst, tw + off, roots, t);
+            group_sync<P>();
+            fwd_rest<P, s + 1>(w, A, B, tw, roots, t);
+        }
+    }
+}
+
+template <class P>
+__device__ __forceinline__ void forward(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
+                                        int t) {
+    constexpr int R0 = P::R[0];
+    if constexpr (P::S == 1) {
+        stage_reg<P, -1, R0, 1>(w, nullptr, tw, roots, t);
+    } else {
+        stage_reg<P, -1, R0, 1>(w, A, tw, roots, t);   // outputs to A
+        group_sync<P>();
+        fwd_rest<P, 1>(w, A, B, tw, roots, t);
+    }
+}
+
+// Inverse transform: registers (mid layout of R[S-1]) -> registers (state).
+template <class P, int s>
+__device__ __forceinline__ void inv_rest(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
+                                         int t) {
+    if constexpr (s < P::S) {
+        constexpr int R = P::R[P::S - 1 - s];
+        constexpr int p = P::rprod(s);
+        constexpr int off = Tw<P>::inv(s);
+        float2* src = (s % 2 == 1) ? A : B;
+        float2* dst = (s % 2 == 1) ? B : A;
+        if constexpr (s == P::S - 1) {
+            stage_to_reg<P, +1, R, p>(src, w, tw + off, roots, t);
+        } else {
+            stage_smem<P, +1, R, p>(src, dst, tw + off, roots, t);
+            group_sync<P>();
+            inv_rest<P, s + 1>(w, A, B, tw, roots, t);
+        }
+    }
+}
+
+template <class P>
+__device__ __forceinline__ void inverse(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
+                                        int t) {
+    constexpr int R0 = P::R[P::S - 1];
+    if constexpr (P::S == 1) {
+        stage_reg<P, +1, R0, 1>(w, nullptr, tw + Tw<P>::inv(0), roots, t);
+    } else {
+        stage_reg<P, +1, R0, 1>(w, A, tw + Tw<P>::inv(0), roots, t);
+        group_sync<P>();
+        inv_rest<P, 1>(w, A, B, tw, roots, t);
+    }
+}
+
+__device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
+    return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+__device__ __forceinline__ float2 shrink_c(float2 c, float lam) {
+    const float m = sqrtf(c.x * c.x + c.y * c.y);   // wavelet.rs:90 |z|
+    if (m <= lam) return make_float2(0.f, 0.f);
+    return c * ((m - lam) / m);
+}
+
+template <class P>
+__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1))
+k_fista_col_reg(FistaColArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
+    constexpr int N = P::N, E = P::E, TA = P::TA, T = P::T;
+    constexpr int G = (T == 32) ? 4 : 1;                 // groups (column pairs) per CTA
+    constexpr int NTW = Tw<P>::total();
+    extern __shared__ float2 sm[];
+    float2* TW = sm;
+    float2* RT = TW + NTW;
+    const int g = threadIdx.x / T;
+    const int t = threadIdx.x % T;
+    float2* A = RT + roots_total + g * 2 * P::SMEM_X;
+    float2* B = A + P::SMEM_X;
+    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    __syncthreads();
+
+    const long long unit = (long long)blockIdx.x * G + g;   // (problem, column pair)
+    bool live;
+    int nx, iters;
+    float lam;
+    const float2* yin;
+    float2* xo;
+    const uint32_t* mwords;
+    if (a.probs) {   // batched: per-problem width, iterations, lambda, mask
+        live = unit < a.nunits && t < TA;
+        const ColProblem pr = a.probs[live ? find_problem(a.probs, a.nprob, unit) : 0];
+        const int jp = live ? (int)(unit - pr.unit0) : 0;
+        nx = pr.nx;
+        iters = live ? pr.iters : 0;
+        lam = pr.lambda;
+        yin = pr.y + 2 * jp;
+        xo = pr.x + 2 * jp;
+        mwords = a.mask.words + (long long)pr.mask * a.mask.wstride;
+    } else {
+        const int npairs = a.nx / 2;
+        live = unit < (long long)a.nprob * npairs && t < TA;
+        const long long b = live ? unit / npairs : 0;
+        const int jp = live ? (int)(unit - b * npairs) : 0;
+        nx = a.nx;
+        iters = a.iters;
+        lam = a.lambda;
+        yin = a.ytil + b * a.prob_stride + 2 * jp;
+        xo = a.xout + b * a.out_stride + 2 * jp;
+        mwords = a.mask.words + (b % a.mask.mod) * a.mask.wstride;
+    }
+
+    float2 y[E], x[E], z[E], w[E];
+    uint32_t mb = 0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int q = t + TA * e;
+        const int r = q >> 1;
+        y[e] = live ? yin[(long long)r * nx + (q & 1)] : make_float2(0.f, 0.f);
+        if (live && ((__ldg(mwords + (r >> 5)) >> (r & 31)) & 1u)) mb |= 1u << e;
+    }
+    const float minv = a.minv;
+    // x~0 = z~0 = F^H (m' y')
+#pragma unroll
+    for (int e = 0; e < E; ++e) w[e] = ((mb >> e) & 1u) ? y[e] * minv : make_float2(0.f, 0.f);
+    inverse<P>(w, A, B, TW, RT, t);
+#pragma unroll
+    for (int e = 0; e < E; ++e) { x[e] = w[e]; z[e] = w[e]; }
+
+    const bool col1 = (t & 1) != 0, row1 = (t & 2) != 0;
+    for (int it = 0; it < iters; ++it) {
+        group_sync<P>();
+#pragma unroll
+        for (int e = 0; e < E; ++e) w[e] = z[e];
+        forward<P>(w, A, B, TW, RT, t);
+        // the last forward stage leaves element b + j*(E/R) = row i + j N/R,
+        // f = t + TA*b, i = f >> 1: q = t + TA*(b + j E/R), the state layout,
+        // so y and mb line up with w
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            w[e] = ((mb >> e) & 1u) ? (w[e] - y[e]) * minv : make_float2(0.f, 0.f);
+        group_sync<P>();
+        inverse<P>(w, A, B, TW, RT, t);
+        const float alpha = __ldg(a.alpha + it);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            // v~ = z~ - h ; plain Haar via two Hadamard steps across q^1, q^2
+            const float2 v = z[e] - w[e];
+            const float2 v1 = shfl_xor2(v, 1);
+            const float2 u = col1 ? (v1 - v) : (v + v1);
+            const float2 u2 = shfl_xor2(u, 2);
+            float2 c = (row1 ? (u2 - u) : (u + u2)) * 0.5f;
+            // this thread holds LL (0,0), HL (0,1), LH (1,0) or HH (1,1) of the
+            // modulated image; (1,0) is the demodulated image's LL: untouched
+            if (!(row1 && !col1)) c = shrink_c(c, lam);
+            const float2 c1 = shfl_xor2(c, 1);
+            const float2 s = col1 ? (c1 - c) : (c + c1);
+            const float2 s2 = shfl_xor2(s, 2);
+            const float2 xn = (row1 ? (s2 - s) : (s + s2)) * 0.5f;
+            z[e] = xn + (xn - x[e]) * alpha;
+            x[e] = xn;
+        }
+    }
+    if (live) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int q = t + TA * e;
+            const int r = q >> 1;
+            float2 v = x[e];
+            if (r & 1) v = make_float2(-v.x, -v.y);
+            xo[(long long)r * nx + (q & 1)] = v;
+        }
+    }
+}
+
+// ------------------------------------------------------------ dispatch
+using P256 = Plan<256, 32, 16, 16>;
+using P320 = Plan<320, 64, 10, 16, 2>;
+using P368 = Plan<368, 92, 4, 23, 4>;
+using P384 = Plan<384, 64, 12, 8, 4>;
+using P192 = Plan<192, 32, 12, 4, 4>;
+using P128 = Plan<128, 32, 8, 2, 8>;
+using P512 = Plan<512, 64, 16, 2, 16>;
+
+template <class P>
+static void host_tables(float2* tw, int* ntw) {
+    const double two_pi = 6.283185307179586476925286766559;
+    int o = 0;
+    for (int s = 0; s < P::S; ++s) {
+        const int R = P::R[s], p = P::prod(s);
+        for (int k = 0; k < p; ++k)
+            for (int j = 1; j < R; ++j) {
+                const double ang = -two_pi * j * k / ((double)p * R);
+                tw[o++] = make_float2((float)cos(ang), (float)sin(ang));
+            }
+    }
+    for (int s = 0; s < P::S; ++s) {
+        const int R = P::R[P::S - 1 - s], p = P::rprod(s);
+        for (int k = 0; k < p; ++k)
+            for (int j = 1; j < R; ++j) {
+                const double ang = -two_pi * j * k / ((double)p * R);
+                tw[o++] = make_float2((float)cos(ang), (float)sin(ang));
+            }
+    }
+    *ntw = o;
+}
+
+template <class P>
+static cudaError_t launch_p(const FistaColArgs& a, RegTables& tabs, cudaStream_t st) {
+    constexpr int NTW = Tw<P>::total();
+    constexpr int G = (P::T == 32) ? 4 : 1;
+    if (!tabs.tw[P::N]) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(float2) * (NTW + tabs.roots_n[P::N] + (size_t)G * 2 * P::SMEM_X);
+    cudaError_t e = cudaFuncSetAttribute(k_fista_col_reg<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const long long units = a.probs ? a.nunits : a.nprob * (long long)(a.nx / 2);
+    const long long grid = (units + G - 1) / G;
+    k_fista_col_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, tabs.tw[P::N], tabs.roots[P::N], tabs.roots_n[P::N]);
+    return cudaGetLastError();
+}
+
+}  // namespace reg
+
+bool fista_col_reg_supported(int ny) {
+    switch (ny) {
+        case 128: case 192: case 256: case 320: case 368: case 384: case 512: return true;
+        default: return false;
+    }
+}
+
+// Host twiddle tables of every register plan, in one allocation.
+cudaError_t reg_tables_init(RegTables* t) {
+    if (t->ready) return cudaSuccess;
+    const int ns[] = {128, 192, 256, 320, 368, 384, 512};
+    size_t total = 0;
+    int ntw[7] = {}, nrt[7] = {};
+    static float2 htw[7][4096];
+    static float2 hrt[7][64];
+    reg::host_tables<reg::P128>(htw[0], &ntw[0]);
+    reg::host_tables<reg::P192>(htw[1], &ntw[1]);
+    reg::host_tables<reg::P256>(htw[2], &ntw[2]);
+    reg::host_tables<reg::P320>(htw[3], &ntw[3]);
+    reg::host_tables<reg::P368>(htw[4], &ntw[4]);
+    reg::host_tables<reg::P384>(htw[5], &ntw[5]);
+    reg::host_tables<reg::P512>(htw[6], &ntw[6]);
+    // roots (cos, sin)(2 pi m / R) for the odd generic radix 23
+    for (int k = 0; k < 7; ++k) {
+        if (ns[k] == 368) {
+            for (int m = 0; m < 23; ++m) {
+                const double ang = 6.283185307179586476925286766559 * m / 23.0;
+                hrt[k][m] = make_float2((float)cos(ang), (float)sin(ang));
+            }
+            nrt[k] = 23;
+        } else {
+            hrt[k][0] = make_float2(1.f, 0.f);
+            nrt[k] = 1;
+        }
+        total += ntw[k] + nrt[k];
+    }
+    float2* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(float2) * total);
+    if (e != cudaSuccess) return e;
+    size_t o = 0;
+    for (int k = 0; k < 7; ++k) {
+        e = cudaMemcpy(d + o, htw[k], sizeof(float2) * ntw[k], cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        t->tw[ns[k]] = d + o;
+        o += ntw[k];
+        e = cudaMemcpy(d + o, hrt[k], sizeof(float2) * nrt[k], cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        t->roots[ns[k]] = d + o;
+        t->roots_n[ns[k]] = nrt[k];
+        o += nrt[k];
+    }
+    t->base = d;
+    t->ready = true;
+    return cudaSuccess;
+}
+
+cudaError_t launch_fista_col_reg(const FistaColArgs& a, RegTables& tabs, cudaStream_t st) {
+    if (a.nprob <= 0 || a.nx <= 0) return cudaSuccess;
+    switch (a.ny) {
+        case 128: return reg::launch_p<reg::P128>(a, tabs, st);
+        case 192: return reg::launch_p<reg::P192>(a, tabs, st);
+        case 256: return reg::launch_p<reg::P256>(a, tabs, st);
+        case 320: return reg::launch_p<reg::P320>(a, tabs, st);
+        case 368: return reg::launch_p<reg::P368>(a, tabs, st);
+        case 384: return reg::launch_p<reg::P384>(a, tabs, st);
+        case 512: return reg::launch_p<reg::P512>(a, tabs, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace oks

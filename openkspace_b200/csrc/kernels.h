@@ -55,6 +55,18 @@ struct ColXformArgs {
 };
 cudaError_t launch_col_xform(const ColXformArgs& a, const DevPlan& pl, cudaStream_t st);
 
+// One problem (one coil of one slice) of a batched launch with per-problem
+// width, iteration count, lambda and mask (FistaColArgs::probs).
+struct ColProblem {
+    const float2* y;          // prepared y' [ny][nx]
+    float2* x;                // coil image out [ny][nx] (may equal y)
+    int nx;
+    int iters;
+    float lambda;
+    int mask;                 // mask index into FistaColArgs::mask.words
+    long long unit0;          // first (problem, column pair) unit of this problem
+};
+
 // Fused per-column-pair FISTA for ky-only masks (see k_fista_col).
 struct FistaColArgs {
     const float2* ytil;       // prepared hybrid data y' ([ny][nx] per problem)
@@ -67,8 +79,39 @@ struct FistaColArgs {
     float lambda;
     const float* alpha;       // [iters] FISTA momentum weights
     long long nprob;
+    // batched form: when probs != nullptr the launch covers `nunits`
+    // (problem, column pair) units of problems[0..nprob); problem p owns
+    // units [probs[p].unit0, probs[p].unit0 + nx/2) and its own nx, iters,
+    // lambda and mask; ytil/xout/nx/iters/lambda above are then unused
+    const ColProblem* probs;
+    long long nunits;
 };
 cudaError_t launch_fista_col(const FistaColArgs& a, const DevPlan& pl, cudaStream_t st);
+
+// Resolves a unit of a batched launch (binary search over unit0).
+__device__ __forceinline__ int find_problem(const ColProblem* probs, long long nprob, long long unit) {
+    long long lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        const long long mid = (lo + hi + 1) >> 1;
+        if (probs[mid].unit0 <= unit) lo = mid;
+        else hi = mid - 1;
+    }
+    return (int)lo;
+}
+
+// Register-resident column FISTA (k_fista_reg.cu) for the column lengths it
+// has compile-time plans for; twiddle tables for every plan live in one
+// device allocation made on first use.
+struct RegTables {
+    bool ready = false;
+    float2* base = nullptr;
+    float2* tw[1025] = {};
+    float2* roots[1025] = {};
+    int roots_n[1025] = {};
+};
+bool fista_col_reg_supported(int ny);
+cudaError_t reg_tables_init(RegTables* t);
+cudaError_t launch_fista_col_reg(const FistaColArgs& a, RegTables& tabs, cudaStream_t st);
 
 // FISTA for arbitrary 2-D masks (k_fista2d.cu): state X~, Z~, S per problem.
 struct Fista2dArgs {
@@ -121,7 +164,7 @@ struct Staging {
         size_t cap = 0;
         cudaEvent_t ev = nullptr;
     };
-    static constexpr int kSlots = 8;
+    static constexpr int kSlots = 64;   // >= requests in flight on the request server
     Slot slots[kSlots];
     int next = 0;
     void release() {

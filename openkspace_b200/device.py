@@ -14,6 +14,13 @@ from . import _lib
 from ._lib import OksError
 
 
+class _SliceReq(ctypes.Structure):
+    """okscuda_slice_req (include/okscuda.h)."""
+    _fields_ = [("d_kspace", ctypes.c_void_p), ("h_mask", ctypes.c_void_p), ("nc", ctypes.c_int),
+                ("ny", ctypes.c_int), ("nx", ctypes.c_int), ("iters", ctypes.c_int), ("lambda_", ctypes.c_float),
+                ("d_rss", ctypes.c_void_p), ("d_coils", ctypes.c_void_p)]
+
+
 class DeviceArray:
     """Owned device allocation with a numpy-like shape/dtype."""
 
@@ -201,6 +208,29 @@ class Context:
         self.check(self.lib.okscuda_cs_volume(self.handle, d.ptr, m.ctypes.data, nc, nz, ny, nx, int(iters),
                                               float(lam), ty, tx, o.ptr, coils.ptr if coils else None))
         return o if out is not None else o.to_host()
+
+    def cs_batch(self, slices, outs=None):
+        """okscuda_cs_batch over ``slices`` = [(kspace [nc,ny,nx], mask [ny,nx],
+        iters, lambda), ...] (kspace host array or DeviceArray).  Returns the
+        RSS images (host) or fills the DeviceArrays in ``outs``."""
+        keep = []
+        arr = (_SliceReq * max(len(slices), 1))()
+        for i, (k, m, iters, lam) in enumerate(slices):
+            d, _ = self._dev(k)
+            nc, ny, nx = d.shape
+            mm = np.ascontiguousarray(m, dtype=np.uint8)
+            if mm.shape != (ny, nx):
+                raise OksError(_lib.OKS_ESHAPE, f"mask shape {mm.shape} != {(ny, nx)}")
+            o = outs[i] if outs is not None else self.empty((ny, nx), np.float32)
+            keep += [d, mm, o]
+            arr[i] = _SliceReq(d.ptr, mm.ctypes.data, nc, ny, nx, int(iters), float(lam), o.ptr, None)
+        self.check(self.lib.okscuda_cs_batch(self.handle, arr, len(slices)))
+        if outs is not None:
+            return outs
+        return [keep[3 * i + 2].to_host() for i in range(len(slices))]
+
+    def set_option(self, name: str, value: int):
+        self.check(self.lib.okscuda_set_option(self.handle, name.encode(), int(value)))
 
     # -- profiling ----------------------------------------------------------
     def profile(self, on: bool = True):
