@@ -67,7 +67,8 @@ class PlainWorkload:
 
     # state-model algorithmic bytes of the fused FISTA kernel per launch:
     # 40 B per pixel per coil per iteration (read z, x, y; write x', z')
-    dominant = "k_fista_col"
+    dominant = ("k_fista_col_reg", "k_fista_col")   # register form where a plan exists
+    bytes_model = "state model: 40 B per pixel per coil per iteration (read z, x, y; write x', z')"
 
     def dominant_bytes_per_step(self):
         return 40.0 * self.ny * self.nx * self.nc * self.iters * self.nslices
@@ -112,22 +113,24 @@ class PrecisionWorkload:
     (FP64 noise fit, prewhitening, oversampling removal, placement, FISTA at
     the reference's 368 x 640 grid with partial-row masks, RSS, crop to 320)."""
     name = "precision"
-    dominant = "k2d_row"
+    dominant = ("k2d_row_reg", "k2d_row")
+    bytes_model = "row pass: 48 B per pixel per problem per iteration (read S, Z, X; write X, Z, S), 32 B init"
 
-    def __init__(self, nz: int = 36):
+    def __init__(self, nz: int = 36, iters: int = 120):
         from openkspace_b200 import synth
         from openkspace_b200.strategy import CsRss, oversampled_acquisitions
         self.vol = synth.oversampled_volume(nz=nz)
         self.acqs = oversampled_acquisitions(self.vol)
-        self.strategy = CsRss(iters=120, lambda_=0.005)
+        self.iters = iters
+        self.strategy = CsRss(iters=iters, lambda_=0.005)
         self.nz, self.nc = nz, self.vol.lines.shape[2]
         self.ny, self.nx = self.vol.ny, self.vol.enc_x
         self.units = nz
 
     def config(self):
-        return {"workload": f"precision_{self.nc}c_{self.vol.enc_x}x{self.ny}_os2_{self.nz}slices_I120",
+        return {"workload": f"precision_{self.nc}c_{self.vol.enc_x}x{self.ny}_os2_{self.nz}slices_I{self.iters}",
                 "coils": self.nc, "slices_per_step": self.nz, "readout": self.vol.enc_x, "ky": self.ny,
-                "recon_x": self.vol.rec_x, "fista_grid": f"{self.ny}x{self.nx}", "iters": 120, "lambda": 0.005,
+                "recon_x": self.vol.rec_x, "fista_grid": f"{self.ny}x{self.nx}", "iters": self.iters, "lambda": 0.005,
                 "mask": "ky R=4 + 8% centre; rows partial in kx after oversampling removal",
                 "noise": "256 samples/coil, cond(Psi)=50", "pipeline": "CsRss (strategy.rs:782-891)"}
 
@@ -137,7 +140,7 @@ class PrecisionWorkload:
     def dominant_bytes_per_step(self):
         # k2d_row per problem: the init pass reads S, writes X~, Z~, S (32 B
         # per pixel); every iteration reads S, Z~, X~ and writes X~, Z~, S (48 B)
-        return (48.0 * 120 + 32.0) * self.ny * self.nx * self.nc * self.nz
+        return (48.0 * self.iters + 32.0) * self.ny * self.nx * self.nc * self.nz
 
     def prepare(self, ctx):
         import torch
@@ -175,7 +178,7 @@ class PrecisionWorkload:
         x0 = self.nx // 2 - vol.rec_x // 2
         k[:, 0, vol.ky_index[0], x0:x0 + vol.rec_x] = np.transpose(os, (1, 0, 2))
         m[0, vol.ky_index[0], x0:x0 + vol.rec_x] = True
-        csref.csrss(k[:ncoil], m, 120, 0.005, nthreads=nthreads)
+        csref.csrss(k[:ncoil], m, self.iters, 0.005, nthreads=nthreads)
         dt = time.perf_counter() - t
         units = ncoil / self.nc
         return dt, units, f"1 slice: full feeding pipeline + FISTA on {ncoil} of {self.nc} coils (scaled)"
@@ -186,7 +189,8 @@ class BatchedWorkload:
     R in {2,3,4,6} + 24 centre lines, 30-150 iterations, in one okscuda_cs_batch
     call per step (one register-engine launch per column length, concurrent)."""
     name = "batched"
-    dominant = "k_fista_col_reg"
+    dominant = ("k_fista_col_reg",)
+    bytes_model = "state model: 40 B per pixel per coil per iteration (read z, x, y; write x', z')"
 
     def __init__(self, n: int = 64):
         from openkspace_b200 import synth
@@ -244,7 +248,9 @@ class BatchedWorkload:
 
 
 WORKLOADS = {"plain": lambda: PlainWorkload(1), "volume": lambda: PlainWorkload(36),
-             "precision": lambda: PrecisionWorkload(36), "batched": lambda: BatchedWorkload(64)}
+             "precision": lambda: PrecisionWorkload(36), "batched": lambda: BatchedWorkload(64),
+             # reduced sizes of the same kernels, for profiler captures only
+             "precision_small": lambda: PrecisionWorkload(2, 4), "batched_small": lambda: BatchedWorkload(6)}
 
 
 def run_serving(args):
@@ -491,10 +497,16 @@ def main():
     value = units / (ms / 1e3)
     e2e_value = units / (ms_e2e / 1e3)
     hbm, peak_kind = peaks()
-    dom_ms, dom_n = prof.get(wl.dominant, (0.0, 0))
+    dom_name = next((k for k in wl.dominant if k in prof), wl.dominant[0])
+    dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
     # algorithmic bytes of the dominant kernel over the timed steps / its device time
     achieved = wl.dominant_bytes_per_step() * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     launches = int(sum(n for _, n in prof.values()))
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "dram_traffic.json")   # per-launch ncu DRAM bytes, by workload
+    if os.path.exists(tfile):
+        t = json.load(open(tfile)).get(wl.config()["workload"], {}).get(dom_name)
+        traffic = float(t) if t is not None else None
 
     if rank != 0:
         return
@@ -509,9 +521,9 @@ def main():
         "e2e": {"value": e2e_value, "unit": "slices/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof.items()},
-        "roofline": {"bound": "hbm", "kernel": wl.dominant, "achieved": achieved, "peak": hbm,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                     "model": "state model: 40 B per pixel per coil per iteration"},
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "model": wl.bytes_model},
         "clocks": clk,
     }
     if not args.no_cpu_baseline:

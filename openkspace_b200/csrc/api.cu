@@ -234,8 +234,21 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     rc = get_alpha(ctx, iters, &alpha);
     if (rc) return rc;
     const long long N = (long long)ny * nx;
+    // byte masks followed (16-byte aligned) by per-mask bits of the kx columns
+    // that hold any sample
+    const int cw = (nx + 31) / 32;
+    const size_t mbytes = (size_t)nmask * N, cb_off = (mbytes + 15) & ~size_t(15);
+    std::vector<uint8_t> up(cb_off + sizeof(uint32_t) * (size_t)nmask * cw, 0);
+    std::memcpy(up.data(), h_mask, mbytes);
+    uint32_t* colbits = reinterpret_cast<uint32_t*>(up.data() + cb_off);
+    for (int k = 0; k < nmask; ++k)
+        for (int r = 0; r < ny; ++r) {
+            const uint8_t* row = h_mask + (size_t)k * N + (size_t)r * nx;
+            for (int x = 0; x < nx; ++x)
+                if (row[x]) colbits[(size_t)k * cw + (x >> 5)] |= 1u << (x & 31);
+        }
     oks::Staging::Slot* slot = nullptr;
-    rc = stage_upload(ctx, h_mask, (size_t)nmask * N, &slot);
+    rc = stage_upload(ctx, up.data(), up.size(), &slot);
     if (rc) return rc;
     long long chunk = ctx->fista2d_chunk > 0 ? ctx->fista2d_chunk
                                              : std::max<long long>(1, (64ll << 20) / (4 * N * 8));
@@ -244,6 +257,15 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     cudaError_t e = cudaMallocAsync(&scratch, sizeof(float2) * 3 * chunk * N, ctx->stream);
     if (e != cudaSuccess) { stage_release(ctx, slot); return cuda_err(ctx, e, "cudaMallocAsync(fista2d)"); }
     const int hs = ((ny / 2) + (nx / 2)) & 1;
+    // register-resident passes where a compile-time plan exists (col_engine 1
+    // forces the generic shared-memory passes)
+    const bool col_reg = ctx->col_engine != 1 && oks::fista2d_reg_supported(ny);
+    const bool row_reg = ctx->col_engine != 1 && oks::fista2d_reg_supported(nx);
+    if ((col_reg || row_reg) && (e = oks::reg_tables_init(&ctx->reg_tables)) != cudaSuccess) {
+        cudaFreeAsync(scratch, ctx->stream);
+        stage_release(ctx, slot);
+        return cuda_err(ctx, e, "register tables");
+    }
     for (long long p0 = 0; p0 < nprob && e == cudaSuccess; p0 += chunk) {
         oks::Fista2dArgs a{};
         a.nprob = std::min(chunk, nprob - p0);
@@ -253,6 +275,8 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         a.mask_mod = nmask;
         a.mask_stride = N;
         a.mask = static_cast<const uint8_t*>(slot->dev);
+        a.colbits = reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(slot->dev) + cb_off);
+        a.col_wstride = cw;
         a.X = static_cast<float2*>(scratch) + 2 * chunk * N;
         a.Z = static_cast<float2*>(scratch);
         a.S = a.Z + chunk * N;
@@ -263,23 +287,27 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         a.lambda = lambda;
         a.alpha = alpha;
         a.mask_offset = p0 % nmask;
-        {
+        auto col = [&](int mode) {
+            if (col_reg) {
+                ProfScope ps(ctx, "k2d_col_reg");
+                return oks::launch_fista2d_col_reg(a, ctx->reg_tables, mode, ctx->stream);
+            }
             ProfScope ps(ctx, "k2d_col");
-            e = oks::launch_fista2d_col(a, *py, 0, ctx->stream);
-        }
-        if (e == cudaSuccess) {
+            return oks::launch_fista2d_col(a, *py, mode, ctx->stream);
+        };
+        auto row = [&](int mode, int it) {
+            if (row_reg) {
+                ProfScope ps(ctx, "k2d_row_reg");
+                return oks::launch_fista2d_row_reg(a, ctx->reg_tables, mode, it, ctx->stream);
+            }
             ProfScope ps(ctx, "k2d_row");
-            e = oks::launch_fista2d_row(a, *px, 0, 0, ctx->stream);
-        }
+            return oks::launch_fista2d_row(a, *px, mode, it, ctx->stream);
+        };
+        e = col(0);
+        if (e == cudaSuccess) e = row(0, 0);
         for (int it = 0; it < iters && e == cudaSuccess; ++it) {
-            {
-                ProfScope ps(ctx, "k2d_col");
-                e = oks::launch_fista2d_col(a, *py, 1, ctx->stream);
-            }
-            if (e == cudaSuccess) {
-                ProfScope ps(ctx, "k2d_row");
-                e = oks::launch_fista2d_row(a, *px, 1, it, ctx->stream);
-            }
+            e = col(1);
+            if (e == cudaSuccess) e = row(1, it);
         }
         if (e == cudaSuccess) {
             ProfScope ps(ctx, "k2d_demod");

@@ -205,6 +205,12 @@ __device__ void stage_smem(const float2* __restrict__ src, float2* __restrict__ 
             case 5: { OKS_LOAD(5) bfly5<SIGN>(v); OKS_STORE(5) } break;
             case 8: { OKS_LOAD(8) bfly8<SIGN>(v); OKS_STORE(8) } break;
             case 16: { OKS_LOAD(16) bfly16<SIGN>(v); OKS_STORE(16) } break;
+            case 7: { OKS_LOAD(7) bfly_odd<SIGN, 7>(v, roots); OKS_STORE(7) } break;
+            case 11: { OKS_LOAD(11) bfly_odd<SIGN, 11>(v, roots); OKS_STORE(11) } break;
+            case 13: { OKS_LOAD(13) bfly_odd<SIGN, 13>(v, roots); OKS_STORE(13) } break;
+            case 17: { OKS_LOAD(17) bfly_odd<SIGN, 17>(v, roots); OKS_STORE(17) } break;
+            case 19: { OKS_LOAD(19) bfly_odd<SIGN, 19>(v, roots); OKS_STORE(19) } break;
+            case 23: { OKS_LOAD(23) bfly_odd<SIGN, 23>(v, roots); OKS_STORE(23) } break;
             default: {
                 // any other radix: direct DFT, inputs re-read from smem
                 for (int q = 0; q < R; ++q) {

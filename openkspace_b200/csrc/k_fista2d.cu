@@ -43,8 +43,17 @@ __global__ void k2d_col(Fista2dArgs a, FftPlan pl, const float2* __restrict__ gt
     const int tid = threadIdx.x, nthr = blockDim.x;
     const long long p = blockIdx.y;
     const int x0 = blockIdx.x * tc;
+    const long long mi = (p + a.mask_offset) % a.mask_mod;
+    // a tile of kx columns the mask never samples contributes nothing: the
+    // row pass reads those columns of S as zero, so skip the tile entirely
+    {
+        const uint32_t* cb = a.colbits + mi * a.col_wstride;
+        bool any = false;
+        for (int c = 0; c < tc && x0 + c < nx; ++c) any |= ((cb[(x0 + c) >> 5] >> ((x0 + c) & 31)) & 1u) != 0;
+        if (!any) return;
+    }
     const float2* y = a.y + p * a.y_stride;
-    const uint8_t* mk = a.mask + ((p + a.mask_offset) % a.mask_mod) * a.mask_stride;
+    const uint8_t* mk = a.mask + mi * a.mask_stride;
     float2* S = a.S + p * a.st_stride;
     for (int q = tid; q < pl.tw_total; q += nthr) TW[q] = gtw[q];
     for (int q = tid; q < roots_total; q += nthr) RT[q] = groots[q];
@@ -102,7 +111,12 @@ __global__ void k2d_row(Fista2dArgs a, FftPlan pl, const float2* __restrict__ gt
     float2* Z = a.Z + p * a.st_stride + (long long)r0 * n;
     for (int q = tid; q < pl.tw_total; q += nthr) TW[q] = gtw[q];
     for (int q = tid; q < roots_total; q += nthr) RT[q] = groots[q];
-    for (int q = tid; q < rpc * n; q += nthr) A[q] = (q / n < nrow) ? S[q] : make_float2(0.f, 0.f);
+    const uint32_t* cb = a.colbits + ((p + a.mask_offset) % a.mask_mod) * a.col_wstride;
+    for (int q = tid; q < rpc * n; q += nthr) {
+        const int x = q % n;
+        const bool on = (q / n < nrow) && ((cb[x >> 5] >> (x & 31)) & 1u);
+        A[q] = on ? S[q] : make_float2(0.f, 0.f);   // unsampled kx columns of S are zero
+    }
     __syncthreads();
     float2* H = fft_smem<+1, false>(A, A, B, pl, TW, RT, rpc, n, 1, tid, nthr);
     float2* O = (H == A) ? B : A;   // the free buffer receives z~'
@@ -154,7 +168,10 @@ __global__ void k2d_row(Fista2dArgs a, FftPlan pl, const float2* __restrict__ gt
     }
     __syncthreads();
     float2* F = fft_smem<-1, false>(O, O, H, pl, TW, RT, rpc, n, 1, tid, nthr);
-    for (int q = tid; q < nrow * n; q += nthr) S[q] = F[q];
+    for (int q = tid; q < nrow * n; q += nthr) {
+        const int x = q % n;
+        if ((cb[x >> 5] >> (x & 31)) & 1u) S[q] = F[q];   // only sampled columns are read back
+    }
 }
 
 // ------------------------------------------------------- demodulated copy

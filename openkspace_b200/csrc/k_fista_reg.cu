@@ -404,6 +404,160 @@ k_fista_col_reg(FistaColArgs a, const float2* __restrict__ gtw, const float2* __
     }
 }
 
+// ------------------------------------------- 2-D-mask engine, register form
+// Same passes as k_fista2d.cu (see its header), one column pair (column
+// pass) or one row pair (row pass) per thread group, data in registers.
+// Column pass: element q = 2*row + col of the pair; the FFT runs along y.
+template <class P>
+__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1))
+k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float2* __restrict__ groots,
+            int roots_total) {
+    constexpr int E = P::E, TA = P::TA, T = P::T;
+    constexpr int G = (T == 32) ? 4 : 1;
+    constexpr int NTW = Tw<P>::total();
+    extern __shared__ float2 sm[];
+    float2* TW = sm;
+    float2* RT = TW + NTW;
+    const int g = threadIdx.x / T, t = threadIdx.x % T;
+    float2* A = RT + roots_total + g * 2 * P::SMEM_X;
+    float2* B = A + P::SMEM_X;
+    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    __syncthreads();
+    const int nx = a.nx, npairs = nx / 2;
+    const long long unit = (long long)blockIdx.x * G + g;
+    if (unit >= a.nprob * npairs) return;                    // whole group
+    const long long p = unit / npairs;
+    const int x0 = 2 * (int)(unit - p * npairs);
+    const long long mi = (p + a.mask_offset) % a.mask_mod;
+    const uint32_t* cb = a.colbits + mi * a.col_wstride;
+    if (((cb[x0 >> 5] >> (x0 & 31)) & 3u) == 0) return;      // neither column sampled: S there is read as 0
+    const bool live = t < TA;
+    const float2* y = a.y + p * a.y_stride;
+    const uint8_t* mk = a.mask + mi * a.mask_stride;
+    float2* S = a.S + p * a.st_stride;
+    const float minv = a.minv, ysc = a.ysc;
+    float2 w[E], yv[E];
+    uint32_t mb = 0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int q = t + TA * e;
+        const int r = q >> 1, x = x0 + (q & 1);
+        const long long off = (long long)r * nx + x;
+        const bool m = live && mk[off] != 0;
+        yv[e] = m ? y[off] * (((r + x) & 1) ? -ysc : ysc) : make_float2(0.f, 0.f);
+        if (m) mb |= 1u << e;
+        w[e] = mode ? (live ? S[off] : make_float2(0.f, 0.f)) : (m ? yv[e] * minv : make_float2(0.f, 0.f));
+    }
+    if (mode) {
+        forward<P>(w, A, B, TW, RT, t);
+#pragma unroll
+        for (int e = 0; e < E; ++e) w[e] = ((mb >> e) & 1u) ? (w[e] - yv[e]) * minv : make_float2(0.f, 0.f);
+        group_sync<P>();
+    }
+    inverse<P>(w, A, B, TW, RT, t);
+    if (live) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int q = t + TA * e;
+            S[(long long)(q >> 1) * nx + x0 + (q & 1)] = w[e];
+        }
+    }
+}
+
+// Row pass: element q = 2*x + r of the row pair (r = which row), the FFT
+// runs along x; lane bit 0 pairs the rows, lane bit 1 the columns.
+template <class P>
+__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1))
+k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, const float2* __restrict__ groots,
+            int roots_total) {
+    constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
+    constexpr int G = (T == 32) ? 4 : 1;
+    constexpr int NTW = Tw<P>::total();
+    extern __shared__ float2 sm[];
+    float2* TW = sm;
+    float2* RT = TW + NTW;
+    const int g = threadIdx.x / T, t = threadIdx.x % T;
+    float2* A = RT + roots_total + g * 2 * P::SMEM_X;
+    float2* B = A + P::SMEM_X;
+    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    __syncthreads();
+    const int nrp = a.ny / 2;
+    const long long unit = (long long)blockIdx.x * G + g;
+    if (unit >= a.nprob * nrp) return;
+    const long long p = unit / nrp;
+    const int r0 = 2 * (int)(unit - p * nrp);
+    const bool live = t < TA;
+    const long long mi = (p + a.mask_offset) % a.mask_mod;
+    const uint32_t* cb = a.colbits + mi * a.col_wstride;
+    const long long base = p * a.st_stride + (long long)r0 * N;
+    float2* S = a.S + base;
+    float2* X = a.X + base;
+    float2* Z = a.Z + base;
+    float2 w[E];
+    uint32_t cm = 0;                       // column sampled, per element
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int q = t + TA * e;
+        const int x = q >> 1;
+        const bool on = live && ((cb[x >> 5] >> (x & 31)) & 1u);
+        if (on) cm |= 1u << e;
+        w[e] = on ? S[(long long)(q & 1) * N + x] : make_float2(0.f, 0.f);
+    }
+    inverse<P>(w, A, B, TW, RT, t);
+    if (mode == 0) {
+        if (live) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int q = t + TA * e;
+                const long long off = (long long)(q & 1) * N + (q >> 1);
+                X[off] = w[e];
+                Z[off] = w[e];
+            }
+        }
+    } else {
+        const float alpha = __ldg(a.alpha + it);
+        const float lam = a.lambda;
+        const bool b0 = (t & 1) != 0, b1 = (t & 2) != 0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int q = t + TA * e;
+            const long long off = (long long)(q & 1) * N + (q >> 1);
+            const float2 zo = live ? Z[off] : make_float2(0.f, 0.f);
+            const float2 xo = live ? X[off] : make_float2(0.f, 0.f);
+            const float2 v = zo - w[e];
+            const float2 v1 = shfl_xor2(v, 1);
+            const float2 u = b0 ? (v1 - v) : (v + v1);
+            const float2 u2 = shfl_xor2(u, 2);
+            float2 c = (b1 ? (u2 - u) : (u + u2)) * 0.5f;
+            // (row-difference, column-difference) band of the modulated image
+            // is the demodulated image's LL: untouched
+            if (!(b0 && b1)) c = shrink_c(c, lam);
+            const float2 c1 = shfl_xor2(c, 1);
+            const float2 s = b0 ? (c1 - c) : (c + c1);
+            const float2 s2 = shfl_xor2(s, 2);
+            const float2 xn = (b1 ? (s2 - s) : (s + s2)) * 0.5f;
+            const float2 zn = xn + (xn - xo) * alpha;
+            if (live) {
+                X[off] = xn;
+                Z[off] = zn;
+            }
+            w[e] = zn;
+        }
+    }
+    group_sync<P>();
+    forward<P>(w, A, B, TW, RT, t);
+    if (live) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            if (!((cm >> e) & 1u)) continue;   // only sampled columns of S are read back
+            const int q = t + TA * e;
+            S[(long long)(q & 1) * N + (q >> 1)] = w[e];
+        }
+    }
+}
+
 // ------------------------------------------------------------ dispatch
 using P256 = Plan<256, 32, 16, 16>;
 using P320 = Plan<320, 64, 10, 16, 2>;
@@ -412,6 +566,35 @@ using P384 = Plan<384, 64, 12, 8, 4>;
 using P192 = Plan<192, 32, 12, 4, 4>;
 using P128 = Plan<128, 32, 8, 2, 8>;
 using P512 = Plan<512, 64, 16, 2, 16>;
+using P640 = Plan<640, 160, 8, 10, 8>;
+
+template <class P, class K>
+static cudaError_t launch_2d(K kern, const Fista2dArgs& a, long long units, RegTables& tabs, cudaStream_t st,
+                             int mode, int it, bool row) {
+    constexpr int NTW = Tw<P>::total();
+    constexpr int G = (P::T == 32) ? 4 : 1;
+    if (!tabs.tw[P::N]) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(float2) * (NTW + tabs.roots_n[P::N] + (size_t)G * 2 * P::SMEM_X);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const long long grid = (units + G - 1) / G;
+    if (row)
+        k2d_row_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, it, tabs.tw[P::N], tabs.roots[P::N],
+                                                                tabs.roots_n[P::N]);
+    else
+        k2d_col_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, tabs.tw[P::N], tabs.roots[P::N],
+                                                                tabs.roots_n[P::N]);
+    return cudaGetLastError();
+}
+
+template <class P>
+static cudaError_t col2d(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st) {
+    return launch_2d<P>(k2d_col_reg<P>, a, a.nprob * (a.nx / 2), tabs, st, mode, 0, false);
+}
+template <class P>
+static cudaError_t row2d(const Fista2dArgs& a, RegTables& tabs, int mode, int it, cudaStream_t st) {
+    return launch_2d<P>(k2d_row_reg<P>, a, a.nprob * (a.ny / 2), tabs, st, mode, it, true);
+}
 
 template <class P>
 static void host_tables(float2* tw, int* ntw) {
@@ -459,14 +642,17 @@ bool fista_col_reg_supported(int ny) {
     }
 }
 
+bool fista2d_reg_supported(int n) { return fista_col_reg_supported(n) || n == 640; }
+
 // Host twiddle tables of every register plan, in one allocation.
 cudaError_t reg_tables_init(RegTables* t) {
     if (t->ready) return cudaSuccess;
-    const int ns[] = {128, 192, 256, 320, 368, 384, 512};
+    constexpr int K = 8;
+    const int ns[K] = {128, 192, 256, 320, 368, 384, 512, 640};
     size_t total = 0;
-    int ntw[7] = {}, nrt[7] = {};
-    static float2 htw[7][4096];
-    static float2 hrt[7][64];
+    int ntw[K] = {}, nrt[K] = {};
+    static float2 htw[K][4096];
+    static float2 hrt[K][64];
     reg::host_tables<reg::P128>(htw[0], &ntw[0]);
     reg::host_tables<reg::P192>(htw[1], &ntw[1]);
     reg::host_tables<reg::P256>(htw[2], &ntw[2]);
@@ -474,8 +660,9 @@ cudaError_t reg_tables_init(RegTables* t) {
     reg::host_tables<reg::P368>(htw[4], &ntw[4]);
     reg::host_tables<reg::P384>(htw[5], &ntw[5]);
     reg::host_tables<reg::P512>(htw[6], &ntw[6]);
+    reg::host_tables<reg::P640>(htw[7], &ntw[7]);
     // roots (cos, sin)(2 pi m / R) for the odd generic radix 23
-    for (int k = 0; k < 7; ++k) {
+    for (int k = 0; k < K; ++k) {
         if (ns[k] == 368) {
             for (int m = 0; m < 23; ++m) {
                 const double ang = 6.283185307179586476925286766559 * m / 23.0;
@@ -492,7 +679,7 @@ cudaError_t reg_tables_init(RegTables* t) {
     cudaError_t e = cudaMalloc(&d, sizeof(float2) * total);
     if (e != cudaSuccess) return e;
     size_t o = 0;
-    for (int k = 0; k < 7; ++k) {
+    for (int k = 0; k < K; ++k) {
         e = cudaMemcpy(d + o, htw[k], sizeof(float2) * ntw[k], cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return e;
         t->tw[ns[k]] = d + o;
@@ -518,6 +705,36 @@ cudaError_t launch_fista_col_reg(const FistaColArgs& a, RegTables& tabs, cudaStr
         case 368: return reg::launch_p<reg::P368>(a, tabs, st);
         case 384: return reg::launch_p<reg::P384>(a, tabs, st);
         case 512: return reg::launch_p<reg::P512>(a, tabs, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_fista2d_col_reg(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st) {
+    if (a.nprob <= 0) return cudaSuccess;
+    switch (a.ny) {
+        case 128: return reg::col2d<reg::P128>(a, tabs, mode, st);
+        case 192: return reg::col2d<reg::P192>(a, tabs, mode, st);
+        case 256: return reg::col2d<reg::P256>(a, tabs, mode, st);
+        case 320: return reg::col2d<reg::P320>(a, tabs, mode, st);
+        case 368: return reg::col2d<reg::P368>(a, tabs, mode, st);
+        case 384: return reg::col2d<reg::P384>(a, tabs, mode, st);
+        case 512: return reg::col2d<reg::P512>(a, tabs, mode, st);
+        case 640: return reg::col2d<reg::P640>(a, tabs, mode, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_fista2d_row_reg(const Fista2dArgs& a, RegTables& tabs, int mode, int it, cudaStream_t st) {
+    if (a.nprob <= 0) return cudaSuccess;
+    switch (a.nx) {
+        case 128: return reg::row2d<reg::P128>(a, tabs, mode, it, st);
+        case 192: return reg::row2d<reg::P192>(a, tabs, mode, it, st);
+        case 256: return reg::row2d<reg::P256>(a, tabs, mode, it, st);
+        case 320: return reg::row2d<reg::P320>(a, tabs, mode, it, st);
+        case 368: return reg::row2d<reg::P368>(a, tabs, mode, it, st);
+        case 384: return reg::row2d<reg::P384>(a, tabs, mode, it, st);
+        case 512: return reg::row2d<reg::P512>(a, tabs, mode, it, st);
+        case 640: return reg::row2d<reg::P640>(a, tabs, mode, it, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -121,6 +121,8 @@ struct Fista2dArgs {
     long long mask_stride;
     int mask_mod;
     long long mask_offset;    // problem p uses mask (p + mask_offset) % mask_mod
+    const uint32_t* colbits;  // per mask: kx columns with any sample (ceil(nx/32) words each)
+    int col_wstride;
     float2* X;
     float2* Z;
     float2* S;
@@ -134,6 +136,11 @@ struct Fista2dArgs {
 };
 cudaError_t launch_fista2d_col(const Fista2dArgs& a, const DevPlan& py, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_row(const Fista2dArgs& a, const DevPlan& px, int mode, int it, cudaStream_t st);
+// Register-resident forms of the two passes (k_fista_reg.cu) for lengths
+// with a compile-time plan (column pass: ny; row pass: nx).
+bool fista2d_reg_supported(int n);
+cudaError_t launch_fista2d_col_reg(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st);
+cudaError_t launch_fista2d_row_reg(const Fista2dArgs& a, RegTables& tabs, int mode, int it, cudaStream_t st);
 cudaError_t launch_fista2d_demod(const float2* X, float2* out, long long nprob, int ny, int nx, long long in_stride,
                                  long long out_stride, cudaStream_t st);
 

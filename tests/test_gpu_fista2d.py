@@ -37,6 +37,24 @@ def test_partial_row_masks(ctx, rng, ny, nx, iters):
     assert rel_l2(got, want32) < TOL_CS
 
 
+@pytest.mark.parametrize("ny,nx,iters", [(368, 640, 6), (256, 256, 10), (320, 384, 5), (384, 320, 5),
+                                         (192, 512, 4), (512, 192, 4)])
+def test_register_passes_match_generic_and_oracle(ctx, rng, ny, nx, iters):
+    """Register-resident column/row passes (compile-time plans) against the
+    generic shared-memory passes and FP64, including the reference's
+    368 x 640 partial-row grid of the oversampled workload."""
+    m = partial_row_mask(rng, ny, nx)
+    k = np.where(m[None], crandn(rng, (2, ny, nx)), 0).astype(np.complex64)
+    got = ctx.fista_cs(k, m, iters, 0.02)
+    ctx.set_option("col_engine", 1)
+    try:
+        gen = ctx.fista_cs(k, m, iters, 0.02)
+    finally:
+        ctx.set_option("col_engine", 0)
+    assert rel_l2(got, gen) < 1e-5
+    assert rel_l2(got, o64.fista_cs_single_coil(k, m, iters, 0.02)) < TOL_CS
+
+
 @pytest.mark.parametrize("ny,nx", [(20, 28), (32, 32), (10, 6)])
 def test_random_2d_masks(ctx, rng, ny, nx):
     m = rng.random((ny, nx)) < 0.45

@@ -42,13 +42,13 @@ def test_admission_by_budget(ctx, rng):
     m = np.ones((64, 64), bool)
     need = 4 * 64 * 64 * 8 * 4 + 64 * 64 * 4
     with Server(ctx, max_inflight=4, hbm_budget_bytes=need + 10) as srv:
-        rid, out = srv.submit(k, m, 200, 0.01)
+        rid, out = srv.submit(k, m, 20000, 0.01)   # long enough to still run below
         with pytest.raises(OksError) as e:
             srv.submit(k, m, 5, 0.01)        # budget holds one request
         assert e.value.code == _lib.OKS_EAGAIN
-        srv.wait(rid, 60000)
-        rid2, out2 = srv.submit(k, m, 200, 0.01)   # admitted once memory is back
-        srv.wait(rid2, 60000)
+        srv.wait(rid, 120000)
+        rid2, out2 = srv.submit(k, m, 20000, 0.01)   # admitted once memory is back
+        srv.wait(rid2, 120000)
         assert np.array_equal(out, out2)
 
 
