@@ -129,6 +129,22 @@ typedef struct {
 } okscuda_slice_req;
 int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs, int n);
 
+/* ------------------------------------------------------------ SENSE mode */
+/* Extension mode (no counterpart in the reference's per-coil cs, which
+ * cs.rs:23-26 leaves SENSE-CS as a follow-up): one coil-combined image per
+ * slice, min 1/2 sum_c ||M F S_c x - y_c||^2 + lambda ||W x||_1 by FISTA with
+ * step 1/L (warm start A^H y, threshold lambda/L, LL band untouched,
+ * cs.rs:99-137 momentum).  Maps S_c: Walsh's method (sensitivity.rs:37-142,
+ * window walsh_window, walsh_iters power steps) on the low-resolution images
+ * of the ACS block (longest run of sampled ky rows, grappa.rs:50-87;
+ * strategy.rs:658-669), normalised to unit root-sum-of-squares.  L = ||A||^2
+ * by an FP64 power iteration (power_iters steps).  ky-only masks, nc <= 32.
+ * Outputs |x| to d_mag[ny, nx]; optionally the maps d_maps[nc, ny, nx], the
+ * image d_x[ny, nx] and L.  Synchronous (L is read back). */
+int okscuda_sense_cs(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nc, int ny, int nx,
+                     int iters, float lambda, int walsh_window, int walsh_iters, int power_iters, float* d_mag,
+                     okscuda_c64* d_maps, okscuda_c64* d_x, double* h_lipschitz);
+
 /* ------------------------------------------------------- request server */
 /* No counterpart in the reference (which reconstructs one file at a time).
  * A request is one slice (strategy.rs:850-880).  Each admitted request runs

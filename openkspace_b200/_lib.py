@@ -58,6 +58,8 @@ SIGNATURES = {
     "okscuda_cs_volume": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _i, _i, _vp, _vp]),
     "okscuda_cs_slice_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp]),
     "okscuda_cs_batch": (_i, [_vp, _vp, _i]),
+    "okscuda_sense_cs": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _i, _i, _i, _vp, _vp, _vp,
+                              _c.POINTER(_c.c_double)]),
     "okscuda_server_create": (_i, [_vp, _vp, _c.POINTER(_vp)]),
     "okscuda_server_destroy": (None, [_vp]),
     "okscuda_server_submit": (_i, [_vp, _vp, _c.POINTER(_c.c_uint64)]),

@@ -425,42 +425,45 @@ k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
     __syncthreads();
     const int nx = a.nx, npairs = nx / 2;
-    const long long unit = (long long)blockIdx.x * G + g;
-    if (unit >= a.nprob * npairs) return;                    // whole group
-    const long long p = unit / npairs;
-    const int x0 = 2 * (int)(unit - p * npairs);
-    const long long mi = (p + a.mask_offset) % a.mask_mod;
-    const uint32_t* cb = a.colbits + mi * a.col_wstride;
-    if (((cb[x0 >> 5] >> (x0 & 31)) & 3u) == 0) return;      // neither column sampled: S there is read as 0
     const bool live = t < TA;
-    const float2* y = a.y + p * a.y_stride;
-    const uint8_t* mk = a.mask + mi * a.mask_stride;
-    float2* S = a.S + p * a.st_stride;
     const float minv = a.minv, ysc = a.ysc;
-    float2 w[E], yv[E];
-    uint32_t mb = 0;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int q = t + TA * e;
-        const int r = q >> 1, x = x0 + (q & 1);
-        const long long off = (long long)r * nx + x;
-        const bool m = live && mk[off] != 0;
-        yv[e] = m ? y[off] * (((r + x) & 1) ? -ysc : ysc) : make_float2(0.f, 0.f);
-        if (m) mb |= 1u << e;
-        w[e] = mode ? (live ? S[off] : make_float2(0.f, 0.f)) : (m ? yv[e] * minv : make_float2(0.f, 0.f));
-    }
-    if (mode) {
-        forward<P>(w, A, B, TW, RT, t);
-#pragma unroll
-        for (int e = 0; e < E; ++e) w[e] = ((mb >> e) & 1u) ? (w[e] - yv[e]) * minv : make_float2(0.f, 0.f);
-        group_sync<P>();
-    }
-    inverse<P>(w, A, B, TW, RT, t);
-    if (live) {
+    // persistent: the tables above are loaded once, units are grid-strided
+    for (long long unit = (long long)blockIdx.x * G + g; unit < a.nprob * npairs;
+         unit += (long long)gridDim.x * G) {
+        const long long p = unit / npairs;
+        const int x0 = 2 * (int)(unit - p * npairs);
+        const long long mi = (p + a.mask_offset) % a.mask_mod;
+        const uint32_t* cb = a.colbits + mi * a.col_wstride;
+        if (((cb[x0 >> 5] >> (x0 & 31)) & 3u) == 0) continue;   // neither column sampled: S there reads as 0
+        const float2* __restrict__ y = a.y + p * a.y_stride;
+        const uint8_t* __restrict__ mk = a.mask + mi * a.mask_stride;
+        float2* __restrict__ S = a.S + p * a.st_stride;
+        float2 w[E], yv[E];
+        uint32_t mb = 0;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int q = t + TA * e;
-            S[(long long)(q >> 1) * nx + x0 + (q & 1)] = w[e];
+            const int r = q >> 1, x = x0 + (q & 1);
+            const long long off = (long long)r * nx + x;
+            const bool m = live && mk[off] != 0;
+            yv[e] = m ? y[off] * (((r + x) & 1) ? -ysc : ysc) : make_float2(0.f, 0.f);
+            if (m) mb |= 1u << e;
+            w[e] = mode ? (live ? S[off] : make_float2(0.f, 0.f)) : (m ? yv[e] * minv : make_float2(0.f, 0.f));
+        }
+        group_sync<P>();                     // the previous unit's last stage has read A/B
+        if (mode) {
+            forward<P>(w, A, B, TW, RT, t);
+#pragma unroll
+            for (int e = 0; e < E; ++e) w[e] = ((mb >> e) & 1u) ? (w[e] - yv[e]) * minv : make_float2(0.f, 0.f);
+            group_sync<P>();
+        }
+        inverse<P>(w, A, B, TW, RT, t);
+        if (live) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int q = t + TA * e;
+                S[(long long)(q >> 1) * nx + x0 + (q & 1)] = w[e];
+            }
         }
     }
 }
@@ -484,76 +487,187 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
     __syncthreads();
     const int nrp = a.ny / 2;
-    const long long unit = (long long)blockIdx.x * G + g;
-    if (unit >= a.nprob * nrp) return;
-    const long long p = unit / nrp;
-    const int r0 = 2 * (int)(unit - p * nrp);
     const bool live = t < TA;
-    const long long mi = (p + a.mask_offset) % a.mask_mod;
-    const uint32_t* cb = a.colbits + mi * a.col_wstride;
-    const long long base = p * a.st_stride + (long long)r0 * N;
-    float2* S = a.S + base;
-    float2* X = a.X + base;
-    float2* Z = a.Z + base;
-    float2 w[E];
-    uint32_t cm = 0;                       // column sampled, per element
+    const float alpha = mode ? __ldg(a.alpha + it) : 0.f;
+    const float lam = a.lambda;
+    const bool b0 = (t & 1) != 0, b1 = (t & 2) != 0;
+    for (long long unit = (long long)blockIdx.x * G + g; unit < a.nprob * nrp; unit += (long long)gridDim.x * G) {
+        const long long p = unit / nrp;
+        const int r0 = 2 * (int)(unit - p * nrp);
+        const long long mi = (p + a.mask_offset) % a.mask_mod;
+        const uint32_t* cb = a.colbits + mi * a.col_wstride;
+        const long long base = p * a.st_stride + (long long)r0 * N;
+        float2* __restrict__ S = a.S + base;
+        float2* __restrict__ X = a.X + base;
+        float2* __restrict__ Z = a.Z + base;
+        // every global load of the unit is issued before any store
+        float2 w[E], zo[E], xo[E];
+        uint32_t cm = 0;                       // column sampled, per element
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int q = t + TA * e;
-        const int x = q >> 1;
-        const bool on = live && ((cb[x >> 5] >> (x & 31)) & 1u);
-        if (on) cm |= 1u << e;
-        w[e] = on ? S[(long long)(q & 1) * N + x] : make_float2(0.f, 0.f);
-    }
-    inverse<P>(w, A, B, TW, RT, t);
-    if (mode == 0) {
-        if (live) {
+        for (int e = 0; e < E; ++e) {
+            const int q = t + TA * e;
+            const int x = q >> 1;
+            const long long off = (long long)(q & 1) * N + x;
+            const bool on = live && ((cb[x >> 5] >> (x & 31)) & 1u);
+            if (on) cm |= 1u << e;
+            w[e] = on ? S[off] : make_float2(0.f, 0.f);
+            zo[e] = (mode && live) ? Z[off] : make_float2(0.f, 0.f);
+            xo[e] = (mode && live) ? X[off] : make_float2(0.f, 0.f);
+        }
+        group_sync<P>();                       // the previous unit's last stage has read A/B
+        inverse<P>(w, A, B, TW, RT, t);
+        if (mode == 0) {
+            if (live) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int q = t + TA * e;
+                    const long long off = (long long)(q & 1) * N + (q >> 1);
+                    X[off] = w[e];
+                    Z[off] = w[e];
+                }
+            }
+        } else {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int q = t + TA * e;
                 const long long off = (long long)(q & 1) * N + (q >> 1);
-                X[off] = w[e];
-                Z[off] = w[e];
+                const float2 v = zo[e] - w[e];
+                const float2 v1 = shfl_xor2(v, 1);
+                const float2 u = b0 ? (v1 - v) : (v + v1);
+                const float2 u2 = shfl_xor2(u, 2);
+                float2 c = (b1 ? (u2 - u) : (u + u2)) * 0.5f;
+                // (row-difference, column-difference) band of the modulated
+                // image is the demodulated image's LL: untouched
+                if (!(b0 && b1)) c = shrink_c(c, lam);
+                const float2 c1 = shfl_xor2(c, 1);
+                const float2 s = b0 ? (c1 - c) : (c + c1);
+                const float2 s2 = shfl_xor2(s, 2);
+                const float2 xn = (b1 ? (s2 - s) : (s + s2)) * 0.5f;
+                const float2 zn = xn + (xn - xo[e]) * alpha;
+                if (live) {
+                    X[off] = xn;
+                    Z[off] = zn;
+                }
+                w[e] = zn;
             }
         }
-    } else {
-        const float alpha = __ldg(a.alpha + it);
-        const float lam = a.lambda;
-        const bool b0 = (t & 1) != 0, b1 = (t & 2) != 0;
+        group_sync<P>();
+        forward<P>(w, A, B, TW, RT, t);
+        if (live) {
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int q = t + TA * e;
-            const long long off = (long long)(q & 1) * N + (q >> 1);
-            const float2 zo = live ? Z[off] : make_float2(0.f, 0.f);
-            const float2 xo = live ? X[off] : make_float2(0.f, 0.f);
-            const float2 v = zo - w[e];
-            const float2 v1 = shfl_xor2(v, 1);
-            const float2 u = b0 ? (v1 - v) : (v + v1);
-            const float2 u2 = shfl_xor2(u, 2);
-            float2 c = (b1 ? (u2 - u) : (u + u2)) * 0.5f;
-            // (row-difference, column-difference) band of the modulated image
-            // is the demodulated image's LL: untouched
-            if (!(b0 && b1)) c = shrink_c(c, lam);
-            const float2 c1 = shfl_xor2(c, 1);
-            const float2 s = b0 ? (c1 - c) : (c + c1);
-            const float2 s2 = shfl_xor2(s, 2);
-            const float2 xn = (b1 ? (s2 - s) : (s + s2)) * 0.5f;
-            const float2 zn = xn + (xn - xo) * alpha;
-            if (live) {
-                X[off] = xn;
-                Z[off] = zn;
+            for (int e = 0; e < E; ++e) {
+                if (!((cm >> e) & 1u)) continue;   // only sampled columns of S are read back
+                const int q = t + TA * e;
+                S[(long long)(q & 1) * N + (q >> 1)] = w[e];
             }
-            w[e] = zn;
         }
     }
-    group_sync<P>();
-    forward<P>(w, A, B, TW, RT, t);
+}
+
+// ------------------------------------------- SENSE mode, register form
+// One image per slice: g = sum_c S_c^* F_y^H m (F_y (S_c z~) - y'_c) per
+// column pair (ky-only mask; maps are diagonal, so they commute with the
+// row modulation), v~ = z~ - g / L, prox with lambda / L, momentum.  Maps
+// and y'_c are streamed from L2 every iteration; x~, z~, g stay in registers.
+template <class P>
+__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1))
+k_sense_col_reg(SenseArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
+    constexpr int E = P::E, TA = P::TA, T = P::T;
+    constexpr int G = (T == 32) ? 4 : 1;
+    constexpr int NTW = Tw<P>::total();
+    extern __shared__ float2 sm[];
+    float2* TW = sm;
+    float2* RT = TW + NTW;
+    const int g = threadIdx.x / T, t = threadIdx.x % T;
+    float2* A = RT + roots_total + g * 2 * P::SMEM_X;
+    float2* B = A + P::SMEM_X;
+    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    __syncthreads();
+    const int nx = a.nx, npairs = nx / 2;
+    const long long unit = (long long)blockIdx.x * G + g;
+    if (unit >= npairs) return;
+    const int x0 = 2 * (int)unit;
+    const bool live = t < TA;
+    const long long npix = (long long)a.ny * nx;
+    const float minv = a.minv;
+    uint32_t mb = 0;
+    long long offs[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int q = t + TA * e;
+        const int r = q >> 1;
+        offs[e] = (long long)r * nx + x0 + (q & 1);
+        if (live && ((__ldg(a.mask.words + (r >> 5)) >> (r & 31)) & 1u)) mb |= 1u << e;
+    }
+    float2 x[E], z[E], gr[E], w[E], s[E];
+    // atb = sum_c S_c^* F^H (m' y'_c)
+#pragma unroll
+    for (int e = 0; e < E; ++e) gr[e] = make_float2(0.f, 0.f);
+    for (int c = 0; c < a.nc; ++c) {
+        const float2* yc = a.ytil + c * npix;
+        const float2* sc = a.maps + c * npix;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            w[e] = ((mb >> e) & 1u) ? yc[offs[e]] * minv : make_float2(0.f, 0.f);
+            s[e] = live ? sc[offs[e]] : make_float2(0.f, 0.f);
+        }
+        group_sync<P>();
+        inverse<P>(w, A, B, TW, RT, t);
+#pragma unroll
+        for (int e = 0; e < E; ++e) gr[e] = gr[e] + cmulc(w[e], s[e]);
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) { x[e] = gr[e]; z[e] = gr[e]; }
+    const float lam = a.lambda_l, il = a.inv_l;
+    const bool col1 = (t & 1) != 0, row1 = (t & 2) != 0;
+    for (int it = 0; it < a.iters; ++it) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) gr[e] = make_float2(0.f, 0.f);
+        for (int c = 0; c < a.nc; ++c) {
+            const float2* yc = a.ytil + c * npix;
+            const float2* sc = a.maps + c * npix;
+            float2 yv[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                s[e] = live ? sc[offs[e]] : make_float2(0.f, 0.f);
+                yv[e] = ((mb >> e) & 1u) ? yc[offs[e]] : make_float2(0.f, 0.f);
+                w[e] = cmul(s[e], z[e]);
+            }
+            group_sync<P>();
+            forward<P>(w, A, B, TW, RT, t);
+#pragma unroll
+            for (int e = 0; e < E; ++e) w[e] = ((mb >> e) & 1u) ? (w[e] - yv[e]) * minv : make_float2(0.f, 0.f);
+            group_sync<P>();
+            inverse<P>(w, A, B, TW, RT, t);
+#pragma unroll
+            for (int e = 0; e < E; ++e) gr[e] = gr[e] + cmulc(w[e], s[e]);   // S^* h
+        }
+        const float alpha = __ldg(a.alpha + it);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const float2 v = z[e] - gr[e] * il;
+            const float2 v1 = shfl_xor2(v, 1);
+            const float2 u = col1 ? (v1 - v) : (v + v1);
+            const float2 u2 = shfl_xor2(u, 2);
+            float2 c = (row1 ? (u2 - u) : (u + u2)) * 0.5f;
+            if (!(row1 && !col1)) c = shrink_c(c, lam);   // (1,0) is the demodulated LL
+            const float2 c1 = shfl_xor2(c, 1);
+            const float2 sv = col1 ? (c1 - c) : (c + c1);
+            const float2 s2 = shfl_xor2(sv, 2);
+            const float2 xn = (row1 ? (s2 - sv) : (sv + s2)) * 0.5f;
+            z[e] = xn + (xn - x[e]) * alpha;
+            x[e] = xn;
+        }
+    }
     if (live) {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            if (!((cm >> e) & 1u)) continue;   // only sampled columns of S are read back
             const int q = t + TA * e;
-            S[(long long)(q & 1) * N + (q >> 1)] = w[e];
+            float2 v = x[e];
+            if ((q >> 1) & 1) v = make_float2(-v.x, -v.y);
+            if (a.xout) a.xout[offs[e]] = v;
+            a.mag[offs[e]] = sqrtf(v.x * v.x + v.y * v.y);
         }
     }
 }
@@ -577,7 +691,17 @@ static cudaError_t launch_2d(K kern, const Fista2dArgs& a, long long units, RegT
     const size_t smem = sizeof(float2) * (NTW + tabs.roots_n[P::N] + (size_t)G * 2 * P::SMEM_X);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const long long grid = (units + G - 1) / G;
+    // persistent grid: every resident CTA slot once (tables loaded once per CTA)
+    static int per_sm = 0, nsm = 0;
+    if (!per_sm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::T * G, smem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    long long grid = (units + G - 1) / G;
+    if (grid > (long long)per_sm * nsm) grid = (long long)per_sm * nsm;
     if (row)
         k2d_row_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, it, tabs.tw[P::N], tabs.roots[P::N],
                                                                 tabs.roots_n[P::N]);
@@ -643,6 +767,90 @@ bool fista_col_reg_supported(int ny) {
 }
 
 bool fista2d_reg_supported(int n) { return fista_col_reg_supported(n) || n == 640; }
+
+// ---------------------------------------------------------- SENSE launch
+namespace reg {
+// E = 8 plans: the SENSE kernel holds five register arrays per element
+using S128 = Plan<128, 32, 8, 2, 8>;
+using S192 = Plan<192, 48, 8, 3, 8>;
+using S256 = Plan<256, 64, 8, 4, 8>;
+using S320 = Plan<320, 64, 10, 16, 2>;
+using S368 = Plan<368, 92, 4, 23, 4>;
+using S384 = Plan<384, 96, 8, 6, 8>;
+using S512 = Plan<512, 128, 8, 8, 8>;
+
+// Twiddle / root tables of plan P on the current device, built on first use
+// and kept for the life of the process (a few KB per plan and device).
+template <class P>
+static cudaError_t plan_tables(const float2** tw, const float2** roots, int* nroots) {
+    static float2* d_tab[64] = {};
+    static int d_nrt[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!d_tab[dev]) {
+        static float2 h[4096 + 64];
+        int ntw = 0;
+        host_tables<P>(h, &ntw);
+        int nrt = 1;
+        h[ntw] = make_float2(1.f, 0.f);
+        for (int s = 0; s < P::S; ++s)
+            if (P::R[s] % 2 == 1 && P::R[s] > 5) {   // generic odd radix: (cos, sin)(2 pi m / R)
+                nrt = P::R[s];
+                for (int m = 0; m < nrt; ++m) {
+                    const double ang = 6.283185307179586476925286766559 * m / nrt;
+                    h[ntw + m] = make_float2((float)cos(ang), (float)sin(ang));
+                }
+            }
+        float2* d = nullptr;
+        cudaError_t e = cudaMalloc(&d, sizeof(float2) * (ntw + nrt));
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(d, h, sizeof(float2) * (ntw + nrt), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        d_tab[dev] = d;
+        d_nrt[dev] = nrt;
+    }
+    *tw = d_tab[dev];
+    *roots = d_tab[dev] + Tw<P>::total();
+    *nroots = d_nrt[dev];
+    return cudaSuccess;
+}
+
+template <class P>
+static cudaError_t sense_p(const SenseArgs& a, cudaStream_t st) {
+    const float2 *tw, *rt;
+    int nrt;
+    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
+    if (e != cudaSuccess) return e;
+    constexpr int G = (P::T == 32) ? 4 : 1;
+    const size_t smem = sizeof(float2) * (Tw<P>::total() + nrt + (size_t)G * 2 * P::SMEM_X);
+    e = cudaFuncSetAttribute(k_sense_col_reg<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const long long grid = (a.nx / 2 + G - 1) / G;
+    k_sense_col_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, tw, rt, nrt);
+    return cudaGetLastError();
+}
+}  // namespace reg
+
+bool sense_reg_supported(int ny) {
+    switch (ny) {
+        case 128: case 192: case 256: case 320: case 368: case 384: case 512: return true;
+        default: return false;
+    }
+}
+
+cudaError_t launch_sense_col_reg(const SenseArgs& a, cudaStream_t st) {
+    switch (a.ny) {
+        case 128: return reg::sense_p<reg::S128>(a, st);
+        case 192: return reg::sense_p<reg::S192>(a, st);
+        case 256: return reg::sense_p<reg::S256>(a, st);
+        case 320: return reg::sense_p<reg::S320>(a, st);
+        case 368: return reg::sense_p<reg::S368>(a, st);
+        case 384: return reg::sense_p<reg::S384>(a, st);
+        case 512: return reg::sense_p<reg::S512>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
 
 // Host twiddle tables of every register plan, in one allocation.
 cudaError_t reg_tables_init(RegTables* t) {

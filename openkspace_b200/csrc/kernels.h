@@ -144,6 +144,26 @@ cudaError_t launch_fista2d_row_reg(const Fista2dArgs& a, RegTables& tabs, int mo
 cudaError_t launch_fista2d_demod(const float2* X, float2* out, long long nprob, int ny, int nx, long long in_stride,
                                  long long out_stride, cudaStream_t st);
 
+// SENSE extension mode (k_sense.cu, k_fista_reg.cu).
+struct SenseArgs {
+    const float2* ytil;       // [nc][ny][nx] prepared y'_c (row pass output)
+    const float2* maps;       // [nc][ny][nx] sensitivity maps (unit RSS)
+    int nc, ny, nx, iters;
+    float minv;               // 1/ny
+    float lambda_l;           // lambda / L
+    float inv_l;              // 1 / L
+    RowMasks mask;            // the slice's row mask
+    const float* alpha;
+    float2* xout;             // [ny][nx] complex image, or nullptr
+    float* mag;               // [ny][nx] |x|
+};
+bool sense_reg_supported(int ny);
+cudaError_t launch_sense_col_reg(const SenseArgs& a, cudaStream_t st);
+cudaError_t launch_walsh(const float2* imgs, float2* maps, int nc, int ny, int nx, int window, int power_iters,
+                         int normalise, cudaStream_t st);
+cudaError_t launch_sense_power(const float2* maps, const uint32_t* rowbits, int nc, int ny, int nx, int iters,
+                               double2* v, double2* acc, const double2* wtab, double* norms, cudaStream_t st);
+
 // RSS over coils with centre crop, per slice s:
 //   out[s][y][x] = sqrt(sum_c |coils[c * coil_stride + s * slice_stride + (y0+y) nx + x0+x]|^2)
 struct RssArgs {

@@ -30,9 +30,15 @@ struct okscuda_server {
         size_t bytes = 0;
         int status = OKS_OK;
         bool finished = false;
+        // pageable output: the device result goes to a pinned bounce buffer
+        // and is copied to the caller's buffer when completion is observed
+        void* bounce = nullptr;
+        size_t bounce_bytes = 0;
+        void* user_out = nullptr;
     };
     std::unordered_map<uint64_t, Req> reqs;
     std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<void*, size_t>> pinned_pool;   // free pinned bounce buffers
     long long completed = 0;
 };
 
@@ -47,9 +53,38 @@ void reap(okscuda_server* s) {
         if (q == cudaErrorNotReady) continue;
         r.finished = true;
         if (q != cudaSuccess) r.status = OKS_ECUDA;
+        if (r.bounce) {
+            if (r.status == OKS_OK) std::memcpy(r.user_out, r.bounce, r.bounce_bytes);
+            s->pinned_pool.push_back({r.bounce, r.bounce_bytes});
+            r.bounce = nullptr;
+        }
         s->reserved -= r.bytes;
         s->completed += 1;
     }
+}
+
+// A pinned buffer of at least `bytes` from the pool (or a new one).
+void* take_pinned(okscuda_server* s, size_t bytes, size_t* got) {
+    for (size_t i = 0; i < s->pinned_pool.size(); ++i)
+        if (s->pinned_pool[i].second >= bytes) {
+            auto b = s->pinned_pool[i];
+            s->pinned_pool.erase(s->pinned_pool.begin() + i);
+            *got = b.second;
+            return b.first;
+        }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+    *got = bytes;
+    return p;
+}
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
 }
 
 cudaEvent_t take_event(okscuda_server* s) {
@@ -102,7 +137,11 @@ void okscuda_server_destroy(okscuda_server* s) {
     if (!s) return;
     cudaSetDevice(s->ctx->device);
     for (auto st : s->streams) cudaStreamSynchronize(st);
-    for (auto& kv : s->reqs) cudaEventDestroy(kv.second.done);
+    for (auto& kv : s->reqs) {
+        cudaEventDestroy(kv.second.done);
+        if (kv.second.bounce) cudaFreeHost(kv.second.bounce);
+    }
+    for (auto& b : s->pinned_pool) cudaFreeHost(b.first);
     for (auto e : s->ev_pool) cudaEventDestroy(e);
     for (auto st : s->streams) cudaStreamDestroy(st);
     delete s;
@@ -154,9 +193,19 @@ int okscuda_server_submit(okscuda_server* s, const okscuda_request* q, uint64_t*
     if (!rc) rc = oks_fista_core(ctx, static_cast<const okscuda_c64*>(dk), q->h_mask, 1, q->nc, q->ny, q->nx,
                                  q->iters, q->lambda, work);
     if (!rc) rc = okscuda_rss_crop(ctx, work, q->nc, q->ny, q->nx, q->ny, q->nx, static_cast<float*>(drss));
+    void* bounce = nullptr;
+    size_t bounce_cap = 0;
     if (!rc) {
-        e = cudaMemcpyAsync(q->h_rss, drss, sizeof(float) * N, cudaMemcpyDeviceToHost, st);
-        if (e != cudaSuccess) rc = cuda_err(ctx, e, "server_submit: download");
+        // a copy into pageable memory would block this call until the chain
+        // ends; bounce through pinned memory instead
+        void* dst = q->h_rss;
+        if (!is_pinned(q->h_rss)) {
+            bounce = take_pinned(s, sizeof(float) * N, &bounce_cap);
+            if (!bounce) rc = set_err(ctx, OKS_ENOMEM, "server_submit: pinned bounce buffer");
+            dst = bounce;
+        }
+        if (!rc) e = cudaMemcpyAsync(dst, drss, sizeof(float) * N, cudaMemcpyDeviceToHost, st);
+        if (!rc && e != cudaSuccess) rc = cuda_err(ctx, e, "server_submit: download");
     }
     if (q->h_kspace && dk) cudaFreeAsync(dk, st);
     if (coils) cudaFreeAsync(coils, st);
@@ -166,9 +215,14 @@ int okscuda_server_submit(okscuda_server* s, const okscuda_request* q, uint64_t*
     cudaEventRecord(r.done, st);
     ctx->stream = saved;
     if (rc) {
+        cudaEventSynchronize(r.done);
+        if (bounce) s->pinned_pool.push_back({bounce, bounce_cap});
         s->ev_pool.push_back(r.done);
         return rc;
     }
+    r.bounce = bounce;
+    r.bounce_bytes = sizeof(float) * N;
+    r.user_out = q->h_rss;
     r.bytes = need;
     s->reserved += need;
     *id = s->next_id++;

@@ -229,6 +229,23 @@ class Context:
             return outs
         return [keep[3 * i + 2].to_host() for i in range(len(slices))]
 
+    def sense_cs(self, kspace, mask, iters: int, lam: float, walsh_window: int = 3, walsh_iters: int = 6,
+                 power_iters: int = 30):
+        """okscuda_sense_cs on one slice: returns (|x|, x, maps, L) on the host."""
+        d, _ = self._dev(kspace)
+        nc, ny, nx = d.shape
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        if m.shape != (ny, nx):
+            raise OksError(_lib.OKS_ESHAPE, f"mask shape {m.shape} != {(ny, nx)}")
+        mag = self.empty((ny, nx), np.float32)
+        x = self.empty((ny, nx))
+        maps = self.empty((nc, ny, nx))
+        L = ctypes.c_double()
+        self.check(self.lib.okscuda_sense_cs(self.handle, d.ptr, m.ctypes.data, nc, ny, nx, int(iters), float(lam),
+                                             int(walsh_window), int(walsh_iters), int(power_iters), mag.ptr, maps.ptr,
+                                             x.ptr, ctypes.byref(L)))
+        return mag.to_host(), x.to_host(), maps.to_host(), L.value
+
     def set_option(self, name: str, value: int):
         self.check(self.lib.okscuda_set_option(self.handle, name.encode(), int(value)))
 
