@@ -47,6 +47,11 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
     if (!std::strcmp(name, "col_engine")) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "col_engine: 0 auto, 1 generic, 2 register");
         ctx->col_engine = (int)value;
+    } else if (!std::strcmp(name, "col_variant")) {
+        if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "col_variant: 0 or 1");
+        ctx->col_variant = (int)value;
+    } else if (!std::strcmp(name, "persist2d")) {
+        ctx->persist2d = value != 0;
     } else if (!std::strcmp(name, "fista2d_chunk")) {
         if (value < 0) return set_err(ctx, OKS_EINVAL, "fista2d_chunk must be >= 0");
         ctx->fista2d_chunk = value;
@@ -287,6 +292,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         a.lambda = lambda;
         a.alpha = alpha;
         a.mask_offset = p0 % nmask;
+        a.persist = ctx->persist2d;
         auto col = [&](int mode) {
             if (col_reg) {
                 ProfScope ps(ctx, "k2d_col_reg");
@@ -370,6 +376,7 @@ int oks_fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t*
         fa.xout = out; fa.out_stride = (long long)ny * nx;
         fa.ny = ny; fa.nx = nx; fa.iters = iters; fa.lambda = lambda; fa.alpha = alpha;
         fa.nprob = nprob;
+        fa.variant = ctx->col_variant;
         const bool use_reg = ctx->col_engine != 1 && oks::fista_col_reg_supported(ny);
         if (use_reg) e = oks::reg_tables_init(&ctx->reg_tables);
         if (e == cudaSuccess && use_reg) {

@@ -139,6 +139,7 @@ extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs,
             fa.probs = static_cast<const oks::ColProblem*>(tslot->dev) + spans[k].first;
             fa.nprob = (long long)(spans[k].second - spans[k].first);
             fa.nunits = nunits[k];
+            fa.variant = ctx->col_variant;
             fa.nx = 2;   // unused in the batched form; keeps the launch guard open
             {
                 ProfScope ps(ctx, "k_fista_col_reg", s);

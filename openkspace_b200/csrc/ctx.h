@@ -31,6 +31,8 @@ struct okscuda_ctx {
     oks::Staging staging;
     long long fista2d_chunk = 0;          // problems per 2-D-mask chunk (0 = auto)
     int col_engine = 0;                   // ky-only masks: 0 auto, 1 generic smem, 2 register-resident
+    int col_variant = 0;                  // register column engine plan variant
+    int persist2d = 0;                    // 2-D register passes: persistent grid
     oks::RegTables reg_tables;
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)

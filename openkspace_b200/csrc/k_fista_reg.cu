@@ -140,17 +140,53 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
         if (ITEMS % P::TA != 0 && f >= ITEMS) break;
         const int i = f >> 1, c = f & 1;
         const int k = i % p;
-        float2 v[R];
-#pragma unroll
-        for (int j = 0; j < R; ++j) {
-            float2 x = src[padi(2 * (i + j * NB) + c)];
-            if (j > 0 && p > 1) x = twmul<SIGN>(x, tw[k * (R - 1) + j - 1]);
-            v[j] = x;
-        }
-        bfly<SIGN, R>(v, roots);
         const int ob = (i - k) * R + k;
+        if constexpr (R % 2 == 1 && R > 5) {
+            // large odd radix: fold to a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j}
+            // and store each output pair as soon as it is formed, so only
+            // R - 1 complex values stay live (bfly_odd keeps 3R)
+            constexpr int H = (R - 1) / 2;
+            float2 a[H], b[H];
+            const float2 x0 = src[padi(2 * i + c)];
+            float2 y0 = x0;
 #pragma unroll
-        for (int j = 0; j < R; ++j) dst[padi(2 * (ob + j * p) + c)] = v[j];
+            for (int j = 1; j <= H; ++j) {
+                float2 u = src[padi(2 * (i + j * NB) + c)];
+                float2 w = src[padi(2 * (i + (R - j) * NB) + c)];
+                if (p > 1) {
+                    u = twmul<SIGN>(u, tw[k * (R - 1) + j - 1]);
+                    w = twmul<SIGN>(w, tw[k * (R - 1) + R - j - 1]);
+                }
+                a[j - 1] = u + w;
+                b[j - 1] = u - w;
+                y0 = y0 + a[j - 1];
+            }
+            dst[padi(2 * ob + c)] = y0;
+#pragma unroll
+            for (int q = 1; q <= H; ++q) {
+                float2 re = x0, im = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int j = 1; j <= H; ++j) {
+                    const float2 w = roots[(j * q) % R];
+                    re.x += a[j - 1].x * w.x; re.y += a[j - 1].y * w.x;
+                    im.x += b[j - 1].x * w.y; im.y += b[j - 1].y * w.y;
+                }
+                const float2 si = mul_si<SIGN>(im);
+                dst[padi(2 * (ob + q * p) + c)] = re + si;
+                dst[padi(2 * (ob + (R - q) * p) + c)] = re - si;
+            }
+        } else {
+            float2 v[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                float2 x = src[padi(2 * (i + j * NB) + c)];
+                if (j > 0 && p > 1) x = twmul<SIGN>(x, tw[k * (R - 1) + j - 1]);
+                v[j] = x;
+            }
+            bfly<SIGN, R>(v, roots);
+#pragma unroll
+            for (int j = 0; j < R; ++j) dst[padi(2 * (ob + j * p) + c)] = v[j];
+        }
     }
 }
 
@@ -682,32 +718,40 @@ using P128 = Plan<128, 32, 8, 2, 8>;
 using P512 = Plan<512, 64, 16, 2, 16>;
 using P640 = Plan<640, 160, 8, 10, 8>;
 
+template <class P>
+static cudaError_t plan_tables(const float2** tw, const float2** roots, int* nroots);
+
 template <class P, class K>
 static cudaError_t launch_2d(K kern, const Fista2dArgs& a, long long units, RegTables& tabs, cudaStream_t st,
                              int mode, int it, bool row) {
     constexpr int NTW = Tw<P>::total();
     constexpr int G = (P::T == 32) ? 4 : 1;
-    if (!tabs.tw[P::N]) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(float2) * (NTW + tabs.roots_n[P::N] + (size_t)G * 2 * P::SMEM_X);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    (void)tabs;
+    const float2 *tw, *rt;
+    int nrt;
+    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    // persistent grid: every resident CTA slot once (tables loaded once per CTA)
-    static int per_sm = 0, nsm = 0;
-    if (!per_sm) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::T * G, smem);
-        if (per_sm < 1) per_sm = 1;
-    }
+    const size_t smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X);
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     long long grid = (units + G - 1) / G;
-    if (grid > (long long)per_sm * nsm) grid = (long long)per_sm * nsm;
+    // persistent form: every resident CTA slot once, units grid-strided
+    // (the kernels accept any grid)
+    if (a.persist) {
+        static int per_sm = 0, nsm = 0;
+        if (!per_sm) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::T * G, smem);
+            if (per_sm < 1) per_sm = 1;
+        }
+        if (grid > (long long)per_sm * nsm) grid = (long long)per_sm * nsm;
+    }
     if (row)
-        k2d_row_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, it, tabs.tw[P::N], tabs.roots[P::N],
-                                                                tabs.roots_n[P::N]);
+        k2d_row_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, it, tw, rt, nrt);
     else
-        k2d_col_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, tabs.tw[P::N], tabs.roots[P::N],
-                                                                tabs.roots_n[P::N]);
+        k2d_col_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, tw, rt, nrt);
     return cudaGetLastError();
 }
 
@@ -744,16 +788,19 @@ static void host_tables(float2* tw, int* ntw) {
 }
 
 template <class P>
-static cudaError_t launch_p(const FistaColArgs& a, RegTables& tabs, cudaStream_t st) {
+static cudaError_t launch_p(const FistaColArgs& a, cudaStream_t st) {
     constexpr int NTW = Tw<P>::total();
     constexpr int G = (P::T == 32) ? 4 : 1;
-    if (!tabs.tw[P::N]) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(float2) * (NTW + tabs.roots_n[P::N] + (size_t)G * 2 * P::SMEM_X);
-    cudaError_t e = cudaFuncSetAttribute(k_fista_col_reg<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const float2 *tw, *rt;
+    int nrt;
+    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X);
+    e = cudaFuncSetAttribute(k_fista_col_reg<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const long long units = a.probs ? a.nunits : a.nprob * (long long)(a.nx / 2);
     const long long grid = (units + G - 1) / G;
-    k_fista_col_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, tabs.tw[P::N], tabs.roots[P::N], tabs.roots_n[P::N]);
+    k_fista_col_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, tw, rt, nrt);
     return cudaGetLastError();
 }
 
@@ -904,18 +951,31 @@ cudaError_t reg_tables_init(RegTables* t) {
 }
 
 cudaError_t launch_fista_col_reg(const FistaColArgs& a, RegTables& tabs, cudaStream_t st) {
+    (void)tabs;
     if (a.nprob <= 0 || a.nx <= 0) return cudaSuccess;
+    // variant 1: the E = 8 plans (more threads per column pair, fewer registers each)
+    if (a.variant == 1) {
+        switch (a.ny) {
+            case 192: return reg::launch_p<reg::S192>(a, st);
+            case 256: return reg::launch_p<reg::S256>(a, st);
+            case 384: return reg::launch_p<reg::S384>(a, st);
+            case 512: return reg::launch_p<reg::S512>(a, st);
+            default: break;
+        }
+    }
     switch (a.ny) {
-        case 128: return reg::launch_p<reg::P128>(a, tabs, st);
-        case 192: return reg::launch_p<reg::P192>(a, tabs, st);
-        case 256: return reg::launch_p<reg::P256>(a, tabs, st);
-        case 320: return reg::launch_p<reg::P320>(a, tabs, st);
-        case 368: return reg::launch_p<reg::P368>(a, tabs, st);
-        case 384: return reg::launch_p<reg::P384>(a, tabs, st);
-        case 512: return reg::launch_p<reg::P512>(a, tabs, st);
+        case 128: return reg::launch_p<reg::P128>(a, st);
+        case 192: return reg::launch_p<reg::P192>(a, st);
+        case 256: return reg::launch_p<reg::P256>(a, st);
+        case 320: return reg::launch_p<reg::P320>(a, st);
+        case 368: return reg::launch_p<reg::P368>(a, st);
+        case 384: return reg::launch_p<reg::P384>(a, st);
+        case 512: return reg::launch_p<reg::P512>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }
+
+int fista_col_reg_variants(int ny) { return (ny == 192 || ny == 256 || ny == 384 || ny == 512) ? 2 : 1; }
 
 cudaError_t launch_fista2d_col_reg(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st) {
     if (a.nprob <= 0) return cudaSuccess;

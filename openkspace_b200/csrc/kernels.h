@@ -85,6 +85,7 @@ struct FistaColArgs {
     // lambda and mask; ytil/xout/nx/iters/lambda above are then unused
     const ColProblem* probs;
     long long nunits;
+    int variant;              // register engine: 0 primary plan, 1 alternative plan where one exists
 };
 cudaError_t launch_fista_col(const FistaColArgs& a, const DevPlan& pl, cudaStream_t st);
 
@@ -112,6 +113,7 @@ struct RegTables {
 bool fista_col_reg_supported(int ny);
 cudaError_t reg_tables_init(RegTables* t);
 cudaError_t launch_fista_col_reg(const FistaColArgs& a, RegTables& tabs, cudaStream_t st);
+int fista_col_reg_variants(int ny);   // number of register plans for this column length
 
 // FISTA for arbitrary 2-D masks (k_fista2d.cu): state X~, Z~, S per problem.
 struct Fista2dArgs {
@@ -133,6 +135,7 @@ struct Fista2dArgs {
     float lambda;
     const float* alpha;
     long long nprob;
+    int persist;              // register passes: grid of resident CTAs, units grid-strided
 };
 cudaError_t launch_fista2d_col(const Fista2dArgs& a, const DevPlan& py, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_row(const Fista2dArgs& a, const DevPlan& px, int mode, int it, cudaStream_t st);

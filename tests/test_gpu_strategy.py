@@ -36,7 +36,8 @@ def test_prewhiten_fit_lcg_fixture(ctx):
     assert rel_l2(w, o64.prewhitener_from_noise([data])) < 1e-6
     assert rel_l2(w, csref.prewhiten_fit(data)) < 1e-4
     d = ctx.to_device(data[None])
-    ctx.check(ctx.lib.okscuda_prewhiten_apply(ctx.handle, ctx.to_device(w).ptr, d.ptr, 1, 4, data.shape[1]))
+    dw = ctx.to_device(w)   # keep the device array alive until the call has been made
+    ctx.check(ctx.lib.okscuda_prewhiten_apply(ctx.handle, dw.ptr, d.ptr, 1, 4, data.shape[1]))
     out = d.to_host()[0]
     cov = out @ np.conj(out.T) / (data.shape[1] - 1)
     assert np.max(np.abs(cov - np.eye(4))) < 0.08
@@ -53,7 +54,8 @@ def test_prewhiten_fit_apply_sizes(ctx, rng, nc):
     assert rel_l2(w, o64.prewhitener_from_noise([noise])) < 1e-5
     data = crandn(rng, (5, nc, 96))
     d = ctx.to_device(data)
-    ctx.check(ctx.lib.okscuda_prewhiten_apply(ctx.handle, ctx.to_device(w).ptr, d.ptr, 5, nc, 96))
+    dw = ctx.to_device(w)
+    ctx.check(ctx.lib.okscuda_prewhiten_apply(ctx.handle, dw.ptr, d.ptr, 5, nc, 96))
     assert rel_l2(d.to_host(), o64.prewhiten_apply(w.astype(np.complex128), data)) < 1e-5
 
 
@@ -79,7 +81,8 @@ def test_prewhiten_skip_cases(ctx, rng):
 def test_os_remove(ctx, rng, enc, rec):
     d = crandn(rng, (3, 4, enc))
     out = ctx.empty((3, 4, rec))
-    ctx.check(ctx.lib.okscuda_os_remove(ctx.handle, ctx.to_device(d).ptr, out.ptr, 12, enc, rec))
+    dd = ctx.to_device(d)
+    ctx.check(ctx.lib.okscuda_os_remove(ctx.handle, dd.ptr, out.ptr, 12, enc, rec))
     assert rel_l2(out.to_host(), o64.oversampling_apply(d, enc, rec)) < 1e-5
 
 
@@ -87,10 +90,11 @@ def test_os_remove_dc_and_invalid(ctx):
     d = np.zeros((1, 16), np.complex64)
     d[0, 8] = 10.0
     out = ctx.empty((1, 8))
-    ctx.check(ctx.lib.okscuda_os_remove(ctx.handle, ctx.to_device(d).ptr, out.ptr, 1, 16, 8))
+    dd = ctx.to_device(d)
+    ctx.check(ctx.lib.okscuda_os_remove(ctx.handle, dd.ptr, out.ptr, 1, 16, 8))
     o = out.to_host()[0]
     assert abs(o[4] - 5.0) < 1e-4 and np.max(np.abs(np.delete(o, 4))) < 1e-4
-    assert ctx.lib.okscuda_os_remove(ctx.handle, ctx.to_device(d).ptr, out.ptr, 1, 300, 256) == _lib.OKS_ESKIP
+    assert ctx.lib.okscuda_os_remove(ctx.handle, dd.ptr, out.ptr, 1, 300, 256) == _lib.OKS_ESKIP
 
 
 @pytest.mark.parametrize("nz", [4, 5, 192, 1])
