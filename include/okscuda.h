@@ -60,8 +60,19 @@ const char* okscuda_version(void);
  *   "col_engine"    ky-only masks: 0 auto (register-resident kernel where a
  *                   compile-time plan exists for ny), 1 generic shared-memory
  *                   kernel, 2 register kernel (falls back to 1 for other ny)
+ *   "col_variant"   register column engine: 0 primary plan, 1 the E = 8
+ *                   alternative plan where one exists (192, 256, 384, 512)
  *   "fista2d_chunk" problems per chunk of the 2-D-mask engine (0 = auto,
- *                   sized for L2 residency) */
+ *                   sized for L2 residency)
+ *   "fista2d_streams" chunks of the 2-D-mask engine in flight at once, on
+ *                   forked streams with separate state (1 to 8, default 2)
+ *   "persist2d"     2-D register passes: 1 (default) = one CTA per resident
+ *                   slot, units grid-strided; 0 = one CTA per unit
+ *   "mask_bits"     2-D column pass: 1 = separable masks are read as row
+ *                   and column bits instead of mask bytes
+ *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
+ *                   least 12 warps resident per SM, 0 = registers as needed
+ * Any other name returns OKS_EINVAL. */
 int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value);
 
 /* ---------------------------------------------------------- device memory */

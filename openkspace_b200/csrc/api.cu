@@ -52,6 +52,13 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         ctx->col_variant = (int)value;
     } else if (!std::strcmp(name, "persist2d")) {
         ctx->persist2d = value != 0;
+    } else if (!std::strcmp(name, "mask_bits")) {
+        ctx->mask_bits = value != 0;
+    } else if (!std::strcmp(name, "occ2d")) {
+        ctx->occ2d = value != 0;
+    } else if (!std::strcmp(name, "fista2d_streams")) {
+        if (value < 1 || value > 8) return set_err(ctx, OKS_EINVAL, "fista2d_streams: 1 to 8");
+        ctx->fista2d_streams = (int)value;
     } else if (!std::strcmp(name, "fista2d_chunk")) {
         if (value < 0) return set_err(ctx, OKS_EINVAL, "fista2d_chunk must be >= 0");
         ctx->fista2d_chunk = value;
@@ -240,17 +247,34 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     if (rc) return rc;
     const long long N = (long long)ny * nx;
     // byte masks followed (16-byte aligned) by per-mask bits of the kx columns
-    // that hold any sample
-    const int cw = (nx + 31) / 32;
+    // and of the ky rows that hold any sample
+    const int cw = (nx + 31) / 32, rw = (ny + 31) / 32;
     const size_t mbytes = (size_t)nmask * N, cb_off = (mbytes + 15) & ~size_t(15);
-    std::vector<uint8_t> up(cb_off + sizeof(uint32_t) * (size_t)nmask * cw, 0);
+    const size_t rb_off = cb_off + sizeof(uint32_t) * (size_t)nmask * cw;
+    std::vector<uint8_t> up(rb_off + sizeof(uint32_t) * (size_t)nmask * rw, 0);
     std::memcpy(up.data(), h_mask, mbytes);
     uint32_t* colbits = reinterpret_cast<uint32_t*>(up.data() + cb_off);
+    uint32_t* rowbits = reinterpret_cast<uint32_t*>(up.data() + rb_off);
     for (int k = 0; k < nmask; ++k)
         for (int r = 0; r < ny; ++r) {
             const uint8_t* row = h_mask + (size_t)k * N + (size_t)r * nx;
             for (int x = 0; x < nx; ++x)
-                if (row[x]) colbits[(size_t)k * cw + (x >> 5)] |= 1u << (x & 31);
+                if (row[x]) {
+                    colbits[(size_t)k * cw + (x >> 5)] |= 1u << (x & 31);
+                    rowbits[(size_t)k * rw + (r >> 5)] |= 1u << (r & 31);
+                }
+        }
+    // separable: every sampled row holds exactly the mask's sampled columns
+    bool separable = true;
+    for (int k = 0; k < nmask && separable; ++k)
+        for (int r = 0; r < ny && separable; ++r) {
+            if (!((rowbits[(size_t)k * rw + (r >> 5)] >> (r & 31)) & 1u)) continue;
+            const uint8_t* row = h_mask + (size_t)k * N + (size_t)r * nx;
+            for (int x = 0; x < nx; ++x)
+                if ((row[x] != 0) != (((colbits[(size_t)k * cw + (x >> 5)] >> (x & 31)) & 1u) != 0)) {
+                    separable = false;
+                    break;
+                }
         }
     oks::Staging::Slot* slot = nullptr;
     rc = stage_upload(ctx, up.data(), up.size(), &slot);
@@ -258,8 +282,12 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     long long chunk = ctx->fista2d_chunk > 0 ? ctx->fista2d_chunk
                                              : std::max<long long>(1, (64ll << 20) / (4 * N * 8));
     if (chunk > nprob) chunk = nprob;
+    // independent chunks run concurrently on `ns` forked streams, each with
+    // its own state, so that one chunk's launch tails overlap the other's
+    const long long nchunks = (nprob + chunk - 1) / chunk;
+    const int ns = (int)std::max<long long>(1, std::min<long long>(ctx->fista2d_streams, nchunks));
     void* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(&scratch, sizeof(float2) * 3 * chunk * N, ctx->stream);
+    cudaError_t e = cudaMallocAsync(&scratch, sizeof(float2) * 3 * chunk * N * ns, ctx->stream);
     if (e != cudaSuccess) { stage_release(ctx, slot); return cuda_err(ctx, e, "cudaMallocAsync(fista2d)"); }
     const int hs = ((ny / 2) + (nx / 2)) & 1;
     // register-resident passes where a compile-time plan exists (col_engine 1
@@ -271,7 +299,23 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         stage_release(ctx, slot);
         return cuda_err(ctx, e, "register tables");
     }
-    for (long long p0 = 0; p0 < nprob && e == cudaSuccess; p0 += chunk) {
+    if (ns > 1) {
+        rc = ensure_aux_streams(ctx, ns);
+        if (!rc && (e = cudaEventRecord(ctx->fork_ev, ctx->stream)) != cudaSuccess) rc = cuda_err(ctx, e, "fork");
+        for (int k = 0; k < ns && !rc; ++k)
+            if ((e = cudaStreamWaitEvent(ctx->aux[k].stream, ctx->fork_ev, 0)) != cudaSuccess)
+                rc = cuda_err(ctx, e, "fork");
+        if (rc) {
+            cudaFreeAsync(scratch, ctx->stream);
+            stage_release(ctx, slot);
+            return rc;
+        }
+    }
+    long long ci = 0;
+    for (long long p0 = 0; p0 < nprob && e == cudaSuccess; p0 += chunk, ++ci) {
+        const int k = (int)(ci % ns);
+        cudaStream_t st = ns > 1 ? ctx->aux[k].stream : ctx->stream;
+        float2* base = static_cast<float2*>(scratch) + (size_t)k * 3 * chunk * N;
         oks::Fista2dArgs a{};
         a.nprob = std::min(chunk, nprob - p0);
         a.y = reinterpret_cast<const float2*>(d_kspace) + p0 * N;
@@ -282,8 +326,11 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         a.mask = static_cast<const uint8_t*>(slot->dev);
         a.colbits = reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(slot->dev) + cb_off);
         a.col_wstride = cw;
-        a.X = static_cast<float2*>(scratch) + 2 * chunk * N;
-        a.Z = static_cast<float2*>(scratch);
+        a.rowbits = reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(slot->dev) + rb_off);
+        a.row_wstride = rw;
+        a.separable = separable && ctx->mask_bits != 0;
+        a.X = base + 2 * chunk * N;
+        a.Z = base;
         a.S = a.Z + chunk * N;
         a.st_stride = N;
         a.ny = ny; a.nx = nx;
@@ -293,21 +340,22 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         a.alpha = alpha;
         a.mask_offset = p0 % nmask;
         a.persist = ctx->persist2d;
+        a.occ = ctx->occ2d;
         auto col = [&](int mode) {
             if (col_reg) {
-                ProfScope ps(ctx, "k2d_col_reg");
-                return oks::launch_fista2d_col_reg(a, ctx->reg_tables, mode, ctx->stream);
+                ProfScope ps(ctx, "k2d_col_reg", st);
+                return oks::launch_fista2d_col_reg(a, ctx->reg_tables, mode, st);
             }
-            ProfScope ps(ctx, "k2d_col");
-            return oks::launch_fista2d_col(a, *py, mode, ctx->stream);
+            ProfScope ps(ctx, "k2d_col", st);
+            return oks::launch_fista2d_col(a, *py, mode, st);
         };
         auto row = [&](int mode, int it) {
             if (row_reg) {
-                ProfScope ps(ctx, "k2d_row_reg");
-                return oks::launch_fista2d_row_reg(a, ctx->reg_tables, mode, it, ctx->stream);
+                ProfScope ps(ctx, "k2d_row_reg", st);
+                return oks::launch_fista2d_row_reg(a, ctx->reg_tables, mode, it, st);
             }
-            ProfScope ps(ctx, "k2d_row");
-            return oks::launch_fista2d_row(a, *px, mode, it, ctx->stream);
+            ProfScope ps(ctx, "k2d_row", st);
+            return oks::launch_fista2d_row(a, *px, mode, it, st);
         };
         e = col(0);
         if (e == cudaSuccess) e = row(0, 0);
@@ -316,9 +364,14 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             if (e == cudaSuccess) e = row(1, it);
         }
         if (e == cudaSuccess) {
-            ProfScope ps(ctx, "k2d_demod");
-            e = oks::launch_fista2d_demod(a.X, reinterpret_cast<float2*>(d_out) + p0 * N, a.nprob, ny, nx, N, N, ctx->stream);
+            ProfScope ps(ctx, "k2d_demod", st);
+            e = oks::launch_fista2d_demod(a.X, reinterpret_cast<float2*>(d_out) + p0 * N, a.nprob, ny, nx, N, N, st);
         }
+    }
+    // join (also after a launch error: the scratch is freed on ctx->stream)
+    for (int k = 0; k < ns && ns > 1; ++k) {
+        cudaEventRecord(ctx->aux[k].done, ctx->aux[k].stream);
+        cudaStreamWaitEvent(ctx->stream, ctx->aux[k].done, 0);
     }
     cudaFreeAsync(scratch, ctx->stream);
     stage_release(ctx, slot);

@@ -32,7 +32,10 @@ struct okscuda_ctx {
     long long fista2d_chunk = 0;          // problems per 2-D-mask chunk (0 = auto)
     int col_engine = 0;                   // ky-only masks: 0 auto, 1 generic smem, 2 register-resident
     int col_variant = 0;                  // register column engine plan variant
-    int persist2d = 0;                    // 2-D register passes: persistent grid
+    int persist2d = 1;                    // 2-D register passes: persistent grid
+    int mask_bits = 1;                    // 2-D passes: separable masks read as row/column bits
+    int occ2d = 1;                        // 2-D register passes: 1 = launch bounds for 12 warps per SM
+    int fista2d_streams = 2;              // 2-D engine: chunks in flight at once (forked streams)
     oks::RegTables reg_tables;
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)

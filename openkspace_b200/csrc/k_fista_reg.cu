@@ -133,6 +133,53 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
                                            const float2* __restrict__ tw, const float2* __restrict__ roots, int t) {
     constexpr int NB = P::N / R;
     constexpr int ITEMS = 2 * NB;
+    constexpr bool BIG_ODD = (R % 2 == 1 && R > 5);
+    constexpr int NS = BIG_ODD ? P::T / ITEMS : 1;   // threads sharing one butterfly
+    if constexpr (NS >= 2) {
+        // Fewer butterflies than threads: NS threads share each one.  All of
+        // them fold the inputs (a_j, b_j); thread s of the group forms the
+        // output pairs q = s+1, s+1+NS, ... and thread 0 also the DC term.
+        // Every lane takes part, padding lanes too: this stage only reads
+        // and writes shared memory.
+        constexpr int H = (R - 1) / 2;
+        if (t >= NS * ITEMS) return;
+        const int f = t % ITEMS, s = t / ITEMS;
+        const int i = f >> 1, c = f & 1;
+        const int k = i % p;
+        const int ob = (i - k) * R + k;
+        float2 a[H], b[H];
+        const float2 x0 = src[padi(2 * i + c)];
+        float2 y0 = x0;
+#pragma unroll
+        for (int j = 1; j <= H; ++j) {
+            float2 u = src[padi(2 * (i + j * NB) + c)];
+            float2 w = src[padi(2 * (i + (R - j) * NB) + c)];
+            if (p > 1) {
+                u = twmul<SIGN>(u, tw[k * (R - 1) + j - 1]);
+                w = twmul<SIGN>(w, tw[k * (R - 1) + R - j - 1]);
+            }
+            a[j - 1] = u + w;
+            b[j - 1] = u - w;
+            y0 = y0 + a[j - 1];
+        }
+        if (s == 0) dst[padi(2 * ob + c)] = y0;
+        for (int q = s + 1; q <= H; q += NS) {
+            float2 re = x0, im = make_float2(0.f, 0.f);
+            int m = 0;                                   // j q mod R
+#pragma unroll
+            for (int j = 1; j <= H; ++j) {
+                m += q;
+                if (m >= R) m -= R;
+                const float2 w = roots[m];
+                re.x += a[j - 1].x * w.x; re.y += a[j - 1].y * w.x;
+                im.x += b[j - 1].x * w.y; im.y += b[j - 1].y * w.y;
+            }
+            const float2 si = mul_si<SIGN>(im);
+            dst[padi(2 * (ob + q * p) + c)] = re + si;
+            dst[padi(2 * (ob + (R - q) * p) + c)] = re - si;
+        }
+        return;
+    }
     if (P::TA != P::T && t >= P::TA) return;   // padding lanes own no element
 #pragma unroll
     for (int b = 0; b < (ITEMS + P::TA - 1) / P::TA; ++b) {
@@ -355,11 +402,14 @@ k_fista_col_reg(FistaColArgs a, const float2* __restrict__ gtw, const float2* __
     float2* xo;
     const uint32_t* mwords;
     if (a.probs) {   // batched: per-problem width, iterations, lambda, mask
-        live = unit < a.nunits && t < TA;
-        const ColProblem pr = a.probs[live ? find_problem(a.probs, a.nprob, unit) : 0];
-        const int jp = live ? (int)(unit - pr.unit0) : 0;
+        // every lane of the group, padding lanes included, runs the unit's
+        // iteration count: shared-memory stages use all T lanes
+        const bool uv = unit < a.nunits;
+        live = uv && t < TA;
+        const ColProblem pr = a.probs[uv ? find_problem(a.probs, a.nprob, unit) : 0];
+        const int jp = uv ? (int)(unit - pr.unit0) : 0;
         nx = pr.nx;
-        iters = live ? pr.iters : 0;
+        iters = uv ? pr.iters : 0;
         lam = pr.lambda;
         yin = pr.y + 2 * jp;
         xo = pr.x + 2 * jp;
@@ -444,8 +494,8 @@ k_fista_col_reg(FistaColArgs a, const float2* __restrict__ gtw, const float2* __
 // Same passes as k_fista2d.cu (see its header), one column pair (column
 // pass) or one row pair (row pass) per thread group, data in registers.
 // Column pass: element q = 2*row + col of the pair; the FFT runs along y.
-template <class P>
-__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1))
+template <class P, int MINB>
+__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1), MINB)
 k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float2* __restrict__ groots,
             int roots_total) {
     constexpr int E = P::E, TA = P::TA, T = P::T;
@@ -470,9 +520,11 @@ k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float
         const int x0 = 2 * (int)(unit - p * npairs);
         const long long mi = (p + a.mask_offset) % a.mask_mod;
         const uint32_t* cb = a.colbits + mi * a.col_wstride;
-        if (((cb[x0 >> 5] >> (x0 & 31)) & 3u) == 0) continue;   // neither column sampled: S there reads as 0
+        const uint32_t cpair = (__ldg(cb + (x0 >> 5)) >> (x0 & 31)) & 3u;
+        if (cpair == 0) continue;   // neither column sampled: S there reads as 0
         const float2* __restrict__ y = a.y + p * a.y_stride;
         const uint8_t* __restrict__ mk = a.mask + mi * a.mask_stride;
+        const uint32_t* __restrict__ rb = a.rowbits + mi * a.row_wstride;
         float2* __restrict__ S = a.S + p * a.st_stride;
         float2 w[E], yv[E];
         uint32_t mb = 0;
@@ -481,7 +533,10 @@ k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float
             const int q = t + TA * e;
             const int r = q >> 1, x = x0 + (q & 1);
             const long long off = (long long)r * nx + x;
-            const bool m = live && mk[off] != 0;
+            // separable masks: row bit and column bit (both L1-resident)
+            // instead of a byte of the mask per element
+            const bool m = live && (a.separable ? (((__ldg(rb + (r >> 5)) >> (r & 31)) & (cpair >> (q & 1)) & 1u) != 0)
+                                                : mk[off] != 0);
             yv[e] = m ? y[off] * (((r + x) & 1) ? -ysc : ysc) : make_float2(0.f, 0.f);
             if (m) mb |= 1u << e;
             w[e] = mode ? (live ? S[off] : make_float2(0.f, 0.f)) : (m ? yv[e] * minv : make_float2(0.f, 0.f));
@@ -506,8 +561,8 @@ k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float
 
 // Row pass: element q = 2*x + r of the row pair (r = which row), the FFT
 // runs along x; lane bit 0 pairs the rows, lane bit 1 the columns.
-template <class P>
-__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1))
+template <class P, int MINB>
+__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1), MINB)
 k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, const float2* __restrict__ groots,
             int roots_total) {
     constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
@@ -721,47 +776,63 @@ using P640 = Plan<640, 160, 8, 10, 8>;
 template <class P>
 static cudaError_t plan_tables(const float2** tw, const float2** roots, int* nroots);
 
-template <class P, class K>
-static cudaError_t launch_2d(K kern, const Fista2dArgs& a, long long units, RegTables& tabs, cudaStream_t st,
-                             int mode, int it, bool row) {
+// Minimum resident CTAs per SM for the 12-warp occupancy form of the 2-D
+// passes (a.occ = 1); the register budget per thread follows from it.
+template <class P>
+constexpr int occ_blocks() {
+    constexpr int threads = P::T * (P::T == 32 ? 4 : 1);
+    return (12 * 32 + threads - 1) / threads;
+}
+
+template <class P, int MINB>
+static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream_t st, int mode, int it, bool row) {
     constexpr int NTW = Tw<P>::total();
     constexpr int G = (P::T == 32) ? 4 : 1;
-    (void)tabs;
     const float2 *tw, *rt;
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
     const size_t smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X);
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (row) e = cudaFuncSetAttribute(k2d_row_reg<P, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else e = cudaFuncSetAttribute(k2d_col_reg<P, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     long long grid = (units + G - 1) / G;
     // persistent form: every resident CTA slot once, units grid-strided
     // (the kernels accept any grid)
     if (a.persist) {
-        static int per_sm = 0, nsm = 0;
-        if (!per_sm) {
+        static int per_sm[2] = {0, 0}, nsm = 0;
+        if (!per_sm[row]) {
             int dev = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::T * G, smem);
-            if (per_sm < 1) per_sm = 1;
+            if (row) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k2d_row_reg<P, MINB>, P::T * G, smem);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k2d_col_reg<P, MINB>, P::T * G, smem);
+            if (per_sm[row] < 1) per_sm[row] = 1;
         }
-        if (grid > (long long)per_sm * nsm) grid = (long long)per_sm * nsm;
+        if (grid > (long long)per_sm[row] * nsm) grid = (long long)per_sm[row] * nsm;
     }
     if (row)
-        k2d_row_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, it, tw, rt, nrt);
+        k2d_row_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, it, tw, rt, nrt);
     else
-        k2d_col_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, tw, rt, nrt);
+        k2d_col_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, tw, rt, nrt);
     return cudaGetLastError();
 }
 
 template <class P>
+static cudaError_t launch_2d(const Fista2dArgs& a, long long units, cudaStream_t st, int mode, int it, bool row) {
+    if (a.occ) return launch_2d_k<P, occ_blocks<P>()>(a, units, st, mode, it, row);
+    return launch_2d_k<P, 1>(a, units, st, mode, it, row);
+}
+
+template <class P>
 static cudaError_t col2d(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st) {
-    return launch_2d<P>(k2d_col_reg<P>, a, a.nprob * (a.nx / 2), tabs, st, mode, 0, false);
+    (void)tabs;
+    return launch_2d<P>(a, a.nprob * (a.nx / 2), st, mode, 0, false);
 }
 template <class P>
 static cudaError_t row2d(const Fista2dArgs& a, RegTables& tabs, int mode, int it, cudaStream_t st) {
-    return launch_2d<P>(k2d_row_reg<P>, a, a.nprob * (a.ny / 2), tabs, st, mode, it, true);
+    (void)tabs;
+    return launch_2d<P>(a, a.nprob * (a.ny / 2), st, mode, it, true);
 }
 
 template <class P>

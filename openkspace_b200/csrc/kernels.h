@@ -125,6 +125,11 @@ struct Fista2dArgs {
     long long mask_offset;    // problem p uses mask (p + mask_offset) % mask_mod
     const uint32_t* colbits;  // per mask: kx columns with any sample (ceil(nx/32) words each)
     int col_wstride;
+    // every mask is separable, mask = rowbits (x) colbits: the register
+    // column pass reads these bits instead of the byte masks
+    const uint32_t* rowbits;  // per mask: ky rows with any sample (ceil(ny/32) words each)
+    int row_wstride;
+    int separable;
     float2* X;
     float2* Z;
     float2* S;
@@ -136,6 +141,7 @@ struct Fista2dArgs {
     const float* alpha;
     long long nprob;
     int persist;              // register passes: grid of resident CTAs, units grid-strided
+    int occ;                  // register passes: 0 registers as needed, 1 at least 12 warps per SM
 };
 cudaError_t launch_fista2d_col(const Fista2dArgs& a, const DevPlan& py, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_row(const Fista2dArgs& a, const DevPlan& px, int mode, int it, cudaStream_t st);

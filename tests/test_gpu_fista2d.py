@@ -92,3 +92,46 @@ def test_volume_with_partial_rows_matches_oracle(ctx, rng):
     rss = ctx.cs_volume(k, m, 12, 0.02, crop=(24, 16))
     want = o64.maybe_crop(o64.csrss_from_kspace(k, m, 12, 0.02), (16, 24, 1))
     assert o64.nrmse(rss, want) < TOL_CS
+
+
+def ragged_row_mask(rng, ny, nx, frac=0.35):
+    """Sampled rows with windows of different extent per row: not
+    separable, so the column pass reads the byte mask."""
+    rows = np.flatnonzero(rng.random(ny) < frac)
+    m = np.zeros((ny, nx), bool)
+    for r in rows:
+        lo = int(rng.integers(0, nx // 4)) * 2
+        m[r, lo:nx - int(rng.integers(0, nx // 4)) * 2] = True
+    m[ny // 2, :] = True
+    return m
+
+
+@pytest.mark.parametrize("ny,nx,iters", [(368, 640, 5), (256, 256, 6), (384, 320, 4)])
+def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
+    """Separable masks read as row/column bits vs as bytes, the two register
+    budgets of the 2-D passes, persistent vs one-CTA-per-unit grids and one
+    vs two chunks in flight give the same result; a ragged (non-separable)
+    mask takes the byte path and matches FP64."""
+    m = partial_row_mask(rng, ny, nx)
+    k = np.where(m[None], crandn(rng, (5, ny, nx)), 0).astype(np.complex64)
+    want = o64.fista_cs_single_coil(k, m, iters, 0.02)
+    forms = [dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2),
+             dict(mask_bits=0, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2),
+             dict(mask_bits=1, occ2d=0, persist2d=0, fista2d_streams=1, fista2d_chunk=2),
+             dict(mask_bits=1, occ2d=1, persist2d=0, fista2d_streams=3, fista2d_chunk=1)]
+    default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0)
+    results = []
+    try:
+        for form in forms:
+            for name, v in form.items():
+                ctx.set_option(name, v)
+            results.append(ctx.fista_cs(k, m, iters, 0.02))
+    finally:
+        for name, v in default.items():
+            ctx.set_option(name, v)
+    for r in results:
+        assert rel_l2(r, results[0]) < 1e-6
+        assert rel_l2(r, want) < TOL_CS
+    mr = ragged_row_mask(rng, ny, nx)
+    kr = np.where(mr[None], crandn(rng, (2, ny, nx)), 0).astype(np.complex64)
+    assert rel_l2(ctx.fista_cs(kr, mr, iters, 0.02), o64.fista_cs_single_coil(kr, mr, iters, 0.02)) < TOL_CS
