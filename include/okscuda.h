@@ -89,6 +89,18 @@ int okscuda_host_free(okscuda_ctx* ctx, void* h_ptr);
  * in place: ifftshift -> DFT rows -> DFT columns -> fftshift -> 1/sqrt(ny nx). */
 int okscuda_centred_fft2(okscuda_ctx* ctx, okscuda_c64* d_data, int batch, int ny, int nx,
                          int inverse);
+/* The row (readout-direction) pass of cs.rs:141-178: nrows rows of length n,
+ * each transformed by an unnormalised DFT (inverse = 1: e^{+}), with the
+ * ifftshift/fftshift pair of shift.rs:11-26 when centred = 1.  d_out may
+ * equal d_in.  engine 0: SIMT mixed-radix FFT in FP32; engine 1: the DFT as
+ * one GEMM on the tcgen05 tensor cores, split precision 3xBF16 with FP32
+ * accumulation (n <= 2048; OKS_ENOTSUP beyond). */
+int okscuda_dft_rows(okscuda_ctx* ctx, const okscuda_c64* d_in, okscuda_c64* d_out, long long nrows, int n,
+                     int inverse, int centred, int engine);
+/* Reads and clears the tensor-core kernels' error flag (synchronises the
+ * context stream): 0 = no bounded wait ran out since the last read.  No
+ * reference counterpart. */
+int okscuda_tc_status(okscuda_ctx* ctx, int* status);
 /* wavelet.rs:32-52 haar_forward / wavelet.rs:55-75 haar_inverse, batch x [ny, nx]. */
 int okscuda_haar_forward(okscuda_ctx* ctx, const okscuda_c64* d_in, okscuda_c64* d_out, int batch,
                          int ny, int nx);

@@ -49,6 +49,8 @@ SIGNATURES = {
     "okscuda_host_alloc": (_i, [_vp, _sz, _c.POINTER(_vp)]),
     "okscuda_host_free": (_i, [_vp, _vp]),
     "okscuda_centred_fft2": (_i, [_vp, _vp, _i, _i, _i, _i]),
+    "okscuda_dft_rows": (_i, [_vp, _vp, _vp, _c.c_longlong, _i, _i, _i, _i]),
+    "okscuda_tc_status": (_i, [_vp, _c.POINTER(_i)]),
     "okscuda_haar_forward": (_i, [_vp, _vp, _vp, _i, _i, _i]),
     "okscuda_haar_inverse": (_i, [_vp, _vp, _vp, _i, _i, _i]),
     "okscuda_soft_threshold_details": (_i, [_vp, _vp, _i, _i, _i, _f]),

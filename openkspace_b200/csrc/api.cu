@@ -36,6 +36,8 @@ void okscuda_destroy(okscuda_ctx* ctx) {
     for (auto e : ctx->ev_pool) cudaEventDestroy(e);
     ctx->plans.clear();
     if (ctx->reg_tables.base) cudaFree(ctx->reg_tables.base);
+    for (auto& kv : ctx->tc_mats) { cudaFree(kv.second.hi); cudaFree(kv.second.lo); }
+    if (ctx->tc_err) cudaFree(ctx->tc_err);
     for (auto& a : ctx->aux) { cudaStreamDestroy(a.stream); cudaEventDestroy(a.done); }
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

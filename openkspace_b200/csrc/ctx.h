@@ -37,6 +37,10 @@ struct okscuda_ctx {
     int occ2d = 1;                        // 2-D register passes: 1 = launch bounds for 12 warps per SM
     int fista2d_streams = 2;              // 2-D engine: chunks in flight at once (forked streams)
     oks::RegTables reg_tables;
+    // tensor-core row DFT: split B operands per (n, sign, centred), error flag
+    struct TcMat { void* hi = nullptr; void* lo = nullptr; };
+    std::map<long long, TcMat> tc_mats;
+    int* tc_err = nullptr;
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)
     cudaEvent_t fork_ev = nullptr;

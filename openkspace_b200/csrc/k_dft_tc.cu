@@ -1,0 +1,354 @@
+// Readout-direction DFT on the 5th-generation tensor cores (sm_100a).
+//
+// Rows of complex64 are transformed by a dense complex matrix W (the DFT,
+// optionally centred) written as ONE real GEMM:
+//   Y[m][n'] = sum_k' X[m][k'] B[n'][k'],   X viewed as [M][2n] real,
+// with B[2j][2k] = c, B[2j][2k+1] = -s, B[2j+1][2k] = s, B[2j+1][2k+1] = c
+// for W[k][j] = c + i s, so the FP32 accumulator row is already the
+// interleaved complex64 output row.  Split precision (3xBF16): every operand
+// is a = a_hi + a_lo with a_hi = bf16(a), a_lo = bf16(a - a_hi), and
+//   X B ~= X_hi B_hi + X_hi B_lo + X_lo B_hi
+// is accumulated in FP32 in tensor memory (the lo*lo term is below the FP32
+// rounding of the sum).
+//
+// Kernel (one CTA per 128 x 256 output tile, 128 threads):
+//   * warp 0 lane 0: TMA producer.  A (X_hi, X_lo) and B (B_hi, B_lo) tiles
+//     of 64 bf16 along K (128 B = one 128-byte swizzle row) go to a 2-stage
+//     shared-memory ring, completion on an mbarrier per stage;
+//   * warp 1 lane 0: MMA issuer.  tcgen05.mma kind::f16 (bf16 in, f32
+//     accumulate), M = 128, N = 256, K = 16 per instruction, 3 products per
+//     K step; tcgen05.commit frees the stage and finally signals the epilogue;
+//   * all four warps: epilogue.  tcgen05.ld of the warp's 32 TMEM lanes
+//     (= output rows), scale, store.
+// Every wait is bounded (about two seconds); on time-out the kernel records
+// an error in *err, lets what it issued drain, frees its tensor memory and
+// returns (okscuda_tc_status reads and clears the flag).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "kernels.h"
+
+namespace oks {
+namespace tc {
+
+constexpr int BM = 128, BN = 256, BK = 64;
+constexpr int NST = 2;
+constexpr int A_BYTES = BM * BK * 2;                    // 16 KB
+constexpr int B_BYTES = BN * BK * 2;                    // 32 KB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
+constexpr int SMEM_BYTES = NST * STAGE_BYTES + 1024 + 128;
+constexpr long long kWaitCycles = 4000000000ll;         // ~2 s at 1.9 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on phase `parity`; false (and *err set) when it ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
+    if (mbar_try(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+        if (clock64() - t0 > kWaitCycles) {
+            atomicExch(err, code);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, rows of 128 B,
+// 8-row groups 1024 B apart (stride byte offset), sm_100 descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor: D f32, A/B bf16, both K-major, N = BN, M = BM.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                            ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct Epilogue {
+    float* out;          // [M][ld] floats (complex64 rows viewed as real)
+    long long ld;        // row stride in floats
+    long long M;         // rows
+    int ncols;           // real output columns stored (2n)
+    float scale;
+};
+
+__global__ void __launch_bounds__(128, 1)
+k_dft_tc(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
+         const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo, int nk,
+         Epilogue ep, int* err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-byte aligned tile area (the 128-byte swizzle repeats every 1024 B)
+    uint8_t* tiles = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(tiles + NST * STAGE_BYTES);   // full[NST], empty[NST], done
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * NST + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n_tile = blockIdx.x, m_tile = blockIdx.y;
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + NST), done = smem_u32(bars + 2 * NST);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NST; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (threadIdx.x == 0) {
+        // ---- TMA producer
+        int issued = 0;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % NST;
+            if (kb >= NST && !mbar_wait(empty0 + 8 * s, ((kb / NST) & 1) ^ 1, err, 1)) break;
+            uint8_t* st = tiles + s * STAGE_BYTES;
+            const uint32_t fb = full0 + 8 * s;
+            mbar_expect_tx(fb, STAGE_BYTES);
+            tma_load_2d(smem_u32(st), &map_ahi, fb, kb * BK, m_tile * BM);
+            tma_load_2d(smem_u32(st + A_BYTES), &map_alo, fb, kb * BK, m_tile * BM);
+            tma_load_2d(smem_u32(st + 2 * A_BYTES), &map_bhi, fb, kb * BK, n_tile * BN);
+            tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &map_blo, fb, kb * BK, n_tile * BN);
+            issued = kb + 1;
+        }
+        // copies still in flight complete before the CTA may exit
+        for (int kb = issued - NST < 0 ? 0 : issued - NST; kb < issued; ++kb)
+            mbar_wait(full0 + 8 * (kb % NST), (kb / NST) & 1, err, 2);
+    } else if (threadIdx.x == 32) {
+        // ---- MMA issuer
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % NST;
+            if (!mbar_wait(full0 + 8 * s, (kb / NST) & 1, err, 3)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a_hi = smem_u32(tiles + s * STAGE_BYTES);
+            const uint32_t a_lo = a_hi + A_BYTES, b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+                const uint32_t o = kk * 32;   // 16 bf16 along K inside the 128-byte row
+                mma_bf16(tmem, sw128_desc(a_hi + o), sw128_desc(b_hi + o), (kb | kk) != 0);
+                mma_bf16(tmem, sw128_desc(a_hi + o), sw128_desc(b_lo + o), 1u);
+                mma_bf16(tmem, sw128_desc(a_lo + o), sw128_desc(b_hi + o), 1u);
+            }
+            mma_commit(empty0 + 8 * s);   // the stage is free once these MMAs have read it
+        }
+        mma_commit(done);                 // every MMA issued above has completed
+    }
+    __syncwarp();
+
+    // ---- epilogue: warp w owns TMEM lanes (= tile rows) 32w .. 32w+31
+    const bool ok = mbar_wait(done, 0, err, 4);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const long long row = (long long)m_tile * BM + warp * 32 + lane;
+    const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int c = 0; c < BN; c += 16) {
+        float v[16];
+        tmem_ld16(tl + (uint32_t)c, v);
+        const int col0 = n_tile * BN + c;
+        if (!ok || row >= ep.M || col0 >= ep.ncols) continue;
+        float* dst = ep.out + row * ep.ld + col0;
+        if (col0 + 16 <= ep.ncols && (ep.ld % 4) == 0) {
+#pragma unroll
+            for (int i = 0; i < 16; i += 4)
+                *reinterpret_cast<float4*>(dst + i) =
+                    make_float4(v[i] * ep.scale, v[i + 1] * ep.scale, v[i + 2] * ep.scale, v[i + 3] * ep.scale);
+        } else {
+            for (int i = 0; i < 16 && col0 + i < ep.ncols; ++i) dst[i] = v[i] * ep.scale;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
+}
+
+// X (complex rows, [M][ld] complex) -> hi/lo bf16 [M][kp] (real view, zero
+// padded from 2n to kp columns).
+__global__ void k_split_rows(const float* __restrict__ x, long long ld, long long M, int n2, int kp,
+                             __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    const long long total = M * (long long)kp;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long m = i / kp;
+        const int k = (int)(i - m * kp);
+        const float v = k < n2 ? x[m * 2 * ld + k] : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        hi[i] = h;
+        lo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+}
+
+// ------------------------------------------------------------------ host
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// bf16 [rows][kp] row-major, box {BK, box_rows}, 128-byte swizzle.
+static bool make_map(CUtensorMap* map, const void* base, long long rows, int kp, int box_rows) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kp * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static uint16_t bf16_bits(float f) {   // round to nearest even
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+static float bf16_float(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+int kpad(int n) { return (2 * n + BK - 1) / BK * BK; }
+int npad(int n) { return (2 * n + BN - 1) / BN * BN; }
+
+// B operand of the (centred) DFT of length n, sign -1 forward / +1 inverse:
+// hi and lo, each [npad][kpad] bf16 (B^T, K-major), built in FP64.
+void dft_matrix_split(int n, int sign, int centred, std::vector<uint16_t>* hi, std::vector<uint16_t>* lo) {
+    const int kp = kpad(n), np = npad(n);
+    hi->assign((size_t)np * kp, 0);
+    lo->assign((size_t)np * kp, 0);
+    const long long h = n / 2;
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int j = 0; j < n; ++j)
+        for (int k = 0; k < n; ++k) {
+            long long e;
+            if (centred) e = (((long long)(j - h) * (k - h)) % n + n) % n;   // fftshift o DFT o ifftshift
+            else e = ((long long)j * k) % n;
+            const double ang = two_pi * (double)e / n;
+            const double c = std::cos(ang), s = sign * std::sin(ang);
+            const double vals[4] = {c, -s, s, c};   // [2j][2k], [2j][2k+1], [2j+1][2k], [2j+1][2k+1]
+            const size_t idx[4] = {(size_t)(2 * j) * kp + 2 * k, (size_t)(2 * j) * kp + 2 * k + 1,
+                                   (size_t)(2 * j + 1) * kp + 2 * k, (size_t)(2 * j + 1) * kp + 2 * k + 1};
+            for (int q = 0; q < 4; ++q) {
+                const float f = (float)vals[q];
+                const uint16_t bh = bf16_bits(f);
+                (*hi)[idx[q]] = bh;
+                (*lo)[idx[q]] = bf16_bits((float)((double)f - (double)bf16_float(bh)));
+            }
+        }
+}
+
+}  // namespace tc
+
+bool dft_tc_available() { return tc::encode_fn() != nullptr; }
+
+size_t dft_tc_scratch_bytes(long long M, int n) { return (size_t)M * tc::kpad(n) * 2 * 2; }
+
+cudaError_t launch_dft_tc(const float2* in, long long ld_in, float2* out, long long ld_out, long long M, int n,
+                          const void* b_hi, const void* b_lo, void* scratch, float scale, int* err, cudaStream_t st) {
+    using namespace tc;
+    const int kp = kpad(n), np = npad(n);
+    __nv_bfloat16* a_hi = static_cast<__nv_bfloat16*>(scratch);
+    __nv_bfloat16* a_lo = a_hi + (size_t)M * kp;
+    {
+        const long long total = M * (long long)kp;
+        const int threads = 256;
+        const long long blocks = std::min<long long>((total + threads - 1) / threads, 148ll * 16);
+        k_split_rows<<<(unsigned)blocks, threads, 0, st>>>(reinterpret_cast<const float*>(in), ld_in, M, 2 * n, kp,
+                                                           a_hi, a_lo);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    CUtensorMap m_ahi, m_alo, m_bhi, m_blo;
+    if (!make_map(&m_ahi, a_hi, M, kp, BM) || !make_map(&m_alo, a_lo, M, kp, BM) ||
+        !make_map(&m_bhi, b_hi, np, kp, BN) || !make_map(&m_blo, b_lo, np, kp, BN))
+        return cudaErrorInvalidValue;
+    e = cudaFuncSetAttribute(k_dft_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    Epilogue ep{reinterpret_cast<float*>(out), 2 * ld_out, M, 2 * n, scale};
+    dim3 grid((unsigned)(np / BN), (unsigned)((M + BM - 1) / BM));
+    k_dft_tc<<<grid, 128, SMEM_BYTES, st>>>(m_ahi, m_alo, m_bhi, m_blo, kp / BK, ep, err);
+    return cudaGetLastError();
+}
+
+}  // namespace oks

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "fft_dev.cuh"
 
 namespace oks {
@@ -212,5 +214,18 @@ struct Staging {
         }
     }
 };
+
+// Tensor-core (tcgen05, split 3xBF16) row DFT (k_dft_tc.cu).
+namespace tc {
+int kpad(int n);
+int npad(int n);
+void dft_matrix_split(int n, int sign, int centred, std::vector<uint16_t>* hi, std::vector<uint16_t>* lo);
+}  // namespace tc
+bool dft_tc_available();
+size_t dft_tc_scratch_bytes(long long M, int n);
+// out[m] = scale * in[m] W for M rows (row strides in complex elements);
+// b_hi/b_lo from tc::dft_matrix_split; scratch of dft_tc_scratch_bytes.
+cudaError_t launch_dft_tc(const float2* in, long long ld_in, float2* out, long long ld_out, long long M, int n,
+                          const void* b_hi, const void* b_lo, void* scratch, float scale, int* err, cudaStream_t st);
 
 }  // namespace oks

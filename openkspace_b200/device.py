@@ -140,6 +140,24 @@ class Context:
         self.check(self.lib.okscuda_centred_fft2(self.handle, d.ptr, h.size // (ny * nx), ny, nx, int(inverse)))
         return d.to_host()
 
+    def dft_rows(self, x, inverse: bool = False, centred: bool = True, engine: int = 0,
+                 in_place: bool = False) -> np.ndarray:
+        """Unnormalised (centred) DFT along the last axis: the readout pass of
+        cs.rs:141-178.  engine 0 = SIMT FFT, 1 = tcgen05 3xBF16 DFT-as-GEMM."""
+        h = np.ascontiguousarray(x, dtype=np.complex64)
+        n = h.shape[-1]
+        d = self.to_device(h)
+        o = d if in_place else self.empty(h.shape)
+        self.check(self.lib.okscuda_dft_rows(self.handle, d.ptr, o.ptr, h.size // n, n, int(inverse), int(centred),
+                                             int(engine)))
+        return o.to_host()
+
+    def tc_status(self) -> int:
+        """Reads and clears the tensor-core kernels' bounded-wait error flag."""
+        st = ctypes.c_int(0)
+        self.check(self.lib.okscuda_tc_status(self.handle, ctypes.byref(st)))
+        return st.value
+
     def haar_forward(self, x) -> np.ndarray:
         h = np.ascontiguousarray(x, dtype=np.complex64)
         ny, nx = h.shape[-2:]

@@ -1,0 +1,59 @@
+"""Readout-direction row DFT through the C-ABI: the SIMT mixed-radix FFT and
+the tcgen05 tensor-core DFT-as-GEMM (split 3xBF16, FP32 accumulation)
+against the FP64 centred transform of cs.rs:141-178 (shift.rs:11-26 shifts).
+Tolerances, relative L2: 1e-5 for the FP32 FFT, 3e-5 for the 3xBF16 GEMM
+(bf16 hi + lo carries 16 of FP32's 24 mantissa bits per operand)."""
+import numpy as np
+import pytest
+
+from oracle import cs_fp64 as o64
+from tests.conftest import crandn, rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL_SIMT = 1e-5
+TOL_TC = 3e-5
+
+
+def ref_rows(x, inverse, centred):
+    a = x.astype(np.complex128)
+    if centred:
+        a = o64.ifftshift_axis(a, -1)
+    a = np.fft.ifft(a, axis=-1) * a.shape[-1] if inverse else np.fft.fft(a, axis=-1)
+    if centred:
+        a = o64.fftshift_axis(a, -1)
+    return a
+
+
+def test_tc_small_first(ctx, rng):
+    """Smallest case first: one 128-row tile, one 256-column tile."""
+    x = crandn(rng, (128, 64))
+    got = ctx.dft_rows(x, inverse=False, centred=False, engine=1)
+    assert ctx.tc_status() == 0
+    assert rel_l2(got, ref_rows(x, False, False)) < TOL_TC
+
+
+@pytest.mark.parametrize("rows,n", [(300, 64), (128, 128), (1000, 320), (736, 368), (515, 640), (40, 30),
+                                    (260, 1000), (3, 2048)])
+@pytest.mark.parametrize("inverse,centred", [(0, 1), (1, 1), (0, 0)])
+def test_engines_match_fp64(ctx, rng, rows, n, inverse, centred):
+    x = crandn(rng, (rows, n))
+    want = ref_rows(x, inverse, centred)
+    simt = ctx.dft_rows(x, inverse=bool(inverse), centred=bool(centred), engine=0)
+    tc = ctx.dft_rows(x, inverse=bool(inverse), centred=bool(centred), engine=1)
+    assert ctx.tc_status() == 0
+    assert rel_l2(simt, want) < TOL_SIMT
+    assert rel_l2(tc, want) < TOL_TC
+
+
+def test_tc_in_place_and_errors(ctx, rng):
+    from openkspace_b200 import OksError, _lib
+    x = crandn(rng, (200, 320))
+    got = ctx.dft_rows(x, inverse=True, centred=True, engine=1, in_place=True)
+    assert ctx.tc_status() == 0
+    assert rel_l2(got, ref_rows(x, 1, 1)) < TOL_TC
+    with pytest.raises(OksError) as e:
+        ctx.dft_rows(crandn(rng, (2, 4096)), engine=1)
+    assert e.value.code == _lib.OKS_ENOTSUP
+    d = ctx.to_device(x)
+    assert ctx.lib.okscuda_dft_rows(ctx.handle, d.ptr, d.ptr, 200, 320, 0, 1, 7) == _lib.OKS_EINVAL
+    assert ctx.lib.okscuda_dft_rows(ctx.handle, d.ptr, d.ptr, 0, 320, 0, 1, 1) == 0
