@@ -64,6 +64,10 @@ const char* okscuda_version(void);
  *                   alternative plan where one exists (192, 256, 384, 512)
  *   "fista2d_chunk" problems per chunk of the 2-D-mask engine (0 = auto,
  *                   sized for L2 residency)
+ *   "row_engine"    2-D-mask engine, readout-direction transforms: 0 (default)
+ *                   SIMT FFT fused with the prox; 1 tensor-core DFT-as-GEMM
+ *                   (split 3xBF16, okscuda_dft_rows engine 1) over the sampled
+ *                   kx columns, with the prox in between (nx <= 2048)
  *   "fista2d_streams" chunks of the 2-D-mask engine in flight at once, on
  *                   forked streams with separate state (1 to 8, default 2)
  *   "persist2d"     2-D register passes: 1 (default) = one CTA per resident

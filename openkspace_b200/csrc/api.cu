@@ -36,7 +36,12 @@ void okscuda_destroy(okscuda_ctx* ctx) {
     for (auto e : ctx->ev_pool) cudaEventDestroy(e);
     ctx->plans.clear();
     if (ctx->reg_tables.base) cudaFree(ctx->reg_tables.base);
-    for (auto& kv : ctx->tc_mats) { cudaFree(kv.second.hi); cudaFree(kv.second.lo); }
+    for (auto& kv : ctx->tc_mats) {
+        cudaFree(kv.second.hi);
+        cudaFree(kv.second.lo);
+        cudaFree(kv.second.in_cols);
+        cudaFree(kv.second.out_cols);
+    }
     if (ctx->tc_err) cudaFree(ctx->tc_err);
     for (auto& a : ctx->aux) { cudaStreamDestroy(a.stream); cudaEventDestroy(a.done); }
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
@@ -58,6 +63,9 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         ctx->mask_bits = value != 0;
     } else if (!std::strcmp(name, "occ2d")) {
         ctx->occ2d = value != 0;
+    } else if (!std::strcmp(name, "row_engine")) {
+        if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "row_engine: 0 SIMT FFT, 1 tensor-core DFT");
+        ctx->row_engine = (int)value;
     } else if (!std::strcmp(name, "fista2d_streams")) {
         if (value < 1 || value > 8) return set_err(ctx, OKS_EINVAL, "fista2d_streams: 1 to 8");
         ctx->fista2d_streams = (int)value;
@@ -288,8 +296,37 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     // its own state, so that one chunk's launch tails overlap the other's
     const long long nchunks = (nprob + chunk - 1) / chunk;
     const int ns = (int)std::max<long long>(1, std::min<long long>(ctx->fista2d_streams, nchunks));
+    // row pass on the tensor cores (row_engine 1): F_x^H restricted to the kx
+    // columns any mask samples, prox, F_x back onto those columns
+    const bool use_tc = ctx->row_engine == 1;
+    std::vector<int> tcols;
+    const okscuda_ctx::TcMat *m_inv = nullptr, *m_fwd = nullptr;
+    size_t per_stream = 3 * (size_t)chunk * N;   // float2 elements: Z, S, X
+    size_t tc_split = 0;                           // bytes of bf16 split operands per stream
+    if (use_tc) {
+        if (nx > 2048 || !oks::dft_tc_available() || (long long)chunk * ny > 65535ll * 128) {
+            stage_release(ctx, slot);
+            return set_err(ctx, OKS_ENOTSUP, "row_engine 1: tensor-core row DFT unavailable for nx = %d", nx);
+        }
+        for (int x = 0; x < nx; ++x) {
+            bool any = false;
+            for (int k = 0; k < nmask && !any; ++k) any = (colbits[(size_t)k * cw + (x >> 5)] >> (x & 31)) & 1u;
+            if (any) tcols.push_back(x);
+        }
+        if (tcols.empty()) tcols.push_back(0);   // nothing sampled: one (zero) column keeps the GEMMs non-empty
+        if ((rc = tc_matrix(ctx, nx, +1, 0, tcols, {}, &m_inv)) || (rc = tc_matrix(ctx, nx, -1, 0, {}, tcols, &m_fwd)) ||
+            (rc = tc_err_flag(ctx))) {
+            stage_release(ctx, slot);
+            return rc;
+        }
+        per_stream += (size_t)chunk * N;   // W = F_x^H S
+        tc_split = std::max(oks::dft_tc_scratch_bytes(chunk * ny, (int)tcols.size()),
+                            oks::dft_tc_scratch_bytes(chunk * ny, nx));
+        tc_split = (tc_split + 255) & ~size_t(255);
+    }
+    const size_t stream_bytes = ((sizeof(float2) * per_stream + 255) & ~size_t(255)) + tc_split;
     void* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(&scratch, sizeof(float2) * 3 * chunk * N * ns, ctx->stream);
+    cudaError_t e = cudaMallocAsync(&scratch, stream_bytes * ns, ctx->stream);
     if (e != cudaSuccess) { stage_release(ctx, slot); return cuda_err(ctx, e, "cudaMallocAsync(fista2d)"); }
     const int hs = ((ny / 2) + (nx / 2)) & 1;
     // register-resident passes where a compile-time plan exists (col_engine 1
@@ -317,7 +354,10 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     for (long long p0 = 0; p0 < nprob && e == cudaSuccess; p0 += chunk, ++ci) {
         const int k = (int)(ci % ns);
         cudaStream_t st = ns > 1 ? ctx->aux[k].stream : ctx->stream;
-        float2* base = static_cast<float2*>(scratch) + (size_t)k * 3 * chunk * N;
+        uint8_t* sbase = static_cast<uint8_t*>(scratch) + (size_t)k * stream_bytes;
+        float2* base = reinterpret_cast<float2*>(sbase);
+        float2* W = base + 3 * chunk * N;                                      // tensor-core mode only
+        void* split = sbase + ((sizeof(float2) * per_stream + 255) & ~size_t(255));
         oks::Fista2dArgs a{};
         a.nprob = std::min(chunk, nprob - p0);
         a.y = reinterpret_cast<const float2*>(d_kspace) + p0 * N;
@@ -352,6 +392,42 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             return oks::launch_fista2d_col(a, *py, mode, st);
         };
         auto row = [&](int mode, int it) {
+            if (use_tc) {
+                const bool contiguous = tcols.back() - tcols.front() + 1 == (int)tcols.size();
+                oks::DftTcArgs t{};
+                t.M = a.nprob * ny;
+                t.scale = 1.0f;
+                t.scratch = split;
+                t.err = ctx->tc_err;
+                // h = F_x^H S over the sampled columns
+                t.in = a.S; t.ld_in = nx; t.nin = (int)tcols.size();
+                t.in_cols = contiguous ? nullptr : m_inv->in_cols;
+                t.in_col0 = contiguous ? tcols.front() : 0;
+                t.out = W; t.ld_out = nx; t.nout = nx;
+                t.b_hi = m_inv->hi; t.b_lo = m_inv->lo;
+                cudaError_t e1;
+                {
+                    ProfScope ps(ctx, "k_dft_tc", st);
+                    e1 = oks::launch_dft_tc(t, st);
+                }
+                if (e1 != cudaSuccess) return e1;
+                {
+                    ProfScope ps(ctx, "k2d_prox", st);
+                    e1 = oks::launch_fista2d_prox(a, W, mode, it, st);
+                }
+                if (e1 != cudaSuccess) return e1;
+                // S = F_x z~' on the sampled columns, zero where the row's mask is clear
+                oks::DftTcArgs f = t;
+                f.in = a.Z; f.nin = nx; f.in_cols = nullptr; f.in_col0 = 0;
+                f.out = a.S; f.nout = (int)tcols.size();
+                f.out_cols = contiguous ? nullptr : m_fwd->out_cols;
+                f.out_col0 = contiguous ? tcols.front() : 0;
+                f.colbits = a.colbits; f.col_wstride = cw; f.rows_per_prob = ny;
+                f.mask_offset = a.mask_offset; f.mask_mod = nmask;
+                f.b_hi = m_fwd->hi; f.b_lo = m_fwd->lo;
+                ProfScope ps(ctx, "k_dft_tc", st);
+                return oks::launch_dft_tc(f, st);
+            }
             if (row_reg) {
                 ProfScope ps(ctx, "k2d_row_reg", st);
                 return oks::launch_fista2d_row_reg(a, ctx->reg_tables, mode, it, st);
@@ -359,7 +435,10 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             ProfScope ps(ctx, "k2d_row", st);
             return oks::launch_fista2d_row(a, *px, mode, it, st);
         };
-        e = col(0);
+        // the tensor-core row pass reads every sampled column of S, also
+        // those of column pairs the column pass skips for this problem's mask
+        if (use_tc) e = cudaMemsetAsync(a.S, 0, sizeof(float2) * a.nprob * N, st);
+        if (e == cudaSuccess) e = col(0);
         if (e == cudaSuccess) e = row(0, 0);
         for (int it = 0; it < iters && e == cudaSuccess; ++it) {
             e = col(1);

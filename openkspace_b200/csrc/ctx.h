@@ -37,10 +37,12 @@ struct okscuda_ctx {
     int occ2d = 1;                        // 2-D register passes: 1 = launch bounds for 12 warps per SM
     int fista2d_streams = 2;              // 2-D engine: chunks in flight at once (forked streams)
     oks::RegTables reg_tables;
-    // tensor-core row DFT: split B operands per (n, sign, centred), error flag
-    struct TcMat { void* hi = nullptr; void* lo = nullptr; };
-    std::map<long long, TcMat> tc_mats;
+    // tensor-core row DFT: split B operands per (n, sign, centred, column
+    // sets), device column lists, error flag
+    struct TcMat { void* hi = nullptr; void* lo = nullptr; int* in_cols = nullptr; int* out_cols = nullptr; };
+    std::map<std::string, TcMat> tc_mats;
     int* tc_err = nullptr;
+    int row_engine = 0;                   // 2-D engine row pass: 0 SIMT FFT, 1 tensor-core DFT
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)
     cudaEvent_t fork_ev = nullptr;
@@ -190,6 +192,57 @@ inline int ensure_aux_streams(okscuda_ctx* ctx, int n) {
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a.done, cudaEventDisableTiming);
         if (e != cudaSuccess) return cuda_err(ctx, e, "aux stream");
         ctx->aux.push_back(a);
+    }
+    return OKS_OK;
+}
+
+// Split (3xBF16) DFT matrix of length n from the columns in_idx to the
+// columns out_idx (empty = all n), built once per context; the index lists
+// are also kept on the device (nullptr when empty).
+inline int tc_matrix(okscuda_ctx* ctx, int n, int sign, int centred, const std::vector<int>& in_idx,
+                     const std::vector<int>& out_idx, const okscuda_ctx::TcMat** out) {
+    std::string key = std::to_string(n) + "/" + std::to_string(sign) + "/" + std::to_string(centred) + "/i";
+    for (int v : in_idx) key += std::to_string(v) + ",";
+    key += "/o";
+    for (int v : out_idx) key += std::to_string(v) + ",";
+    auto it = ctx->tc_mats.find(key);
+    if (it == ctx->tc_mats.end()) {
+        std::vector<uint16_t> h, l;
+        oks::tc::dft_matrix_split(n, sign, centred, in_idx, out_idx, &h, &l);
+        okscuda_ctx::TcMat m;
+        const size_t bytes = h.size() * sizeof(uint16_t);
+        cudaError_t e = cudaMalloc(&m.hi, bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&m.lo, bytes);
+        // pageable sources: each copy completes before cudaMemcpy returns
+        if (e == cudaSuccess) e = cudaMemcpy(m.hi, h.data(), bytes, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(m.lo, l.data(), bytes, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !in_idx.empty()) {
+            e = cudaMalloc(&m.in_cols, sizeof(int) * in_idx.size());
+            if (e == cudaSuccess)
+                e = cudaMemcpy(m.in_cols, in_idx.data(), sizeof(int) * in_idx.size(), cudaMemcpyHostToDevice);
+        }
+        if (e == cudaSuccess && !out_idx.empty()) {
+            e = cudaMalloc(&m.out_cols, sizeof(int) * out_idx.size());
+            if (e == cudaSuccess)
+                e = cudaMemcpy(m.out_cols, out_idx.data(), sizeof(int) * out_idx.size(), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) {
+            cudaFree(m.hi);
+            cudaFree(m.lo);
+            cudaFree(m.in_cols);
+            cudaFree(m.out_cols);
+            return cuda_err(ctx, e, "tensor-core DFT matrix");
+        }
+        it = ctx->tc_mats.emplace(key, m).first;
+    }
+    *out = &it->second;
+    return OKS_OK;
+}
+
+inline int tc_err_flag(okscuda_ctx* ctx) {
+    if (!ctx->tc_err) {
+        OKS_CUDA(cudaMalloc(&ctx->tc_err, sizeof(int)));
+        OKS_CUDA(cudaMemset(ctx->tc_err, 0, sizeof(int)));
     }
     return OKS_OK;
 }

@@ -5,43 +5,6 @@
 // unnormalised, with the fftshift/ifftshift pair when `centred` is set.
 #include "ctx.h"
 
-namespace {
-
-int tc_matrix(okscuda_ctx* ctx, int n, int sign, int centred, const void** hi, const void** lo) {
-    const long long key = ((long long)n << 2) | ((sign > 0) << 1) | (centred != 0);
-    auto it = ctx->tc_mats.find(key);
-    if (it == ctx->tc_mats.end()) {
-        std::vector<uint16_t> h, l;
-        oks::tc::dft_matrix_split(n, sign, centred, &h, &l);
-        okscuda_ctx::TcMat m;
-        const size_t bytes = h.size() * sizeof(uint16_t);
-        OKS_CUDA(cudaMalloc(&m.hi, bytes));
-        cudaError_t e = cudaMalloc(&m.lo, bytes);
-        if (e != cudaSuccess) { cudaFree(m.hi); return cuda_err(ctx, e, "cudaMalloc(dft matrix)"); }
-        // pageable source: the copies complete before cudaMemcpy returns
-        if ((e = cudaMemcpy(m.hi, h.data(), bytes, cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (e = cudaMemcpy(m.lo, l.data(), bytes, cudaMemcpyHostToDevice)) != cudaSuccess) {
-            cudaFree(m.hi);
-            cudaFree(m.lo);
-            return cuda_err(ctx, e, "dft matrix upload");
-        }
-        it = ctx->tc_mats.emplace(key, m).first;
-    }
-    *hi = it->second.hi;
-    *lo = it->second.lo;
-    return OKS_OK;
-}
-
-int tc_err_flag(okscuda_ctx* ctx) {
-    if (!ctx->tc_err) {
-        OKS_CUDA(cudaMalloc(&ctx->tc_err, sizeof(int)));
-        OKS_CUDA(cudaMemset(ctx->tc_err, 0, sizeof(int)));
-    }
-    return OKS_OK;
-}
-
-}  // namespace
-
 extern "C" int okscuda_dft_rows(okscuda_ctx* ctx, const okscuda_c64* d_in, okscuda_c64* d_out, long long nrows,
                                 int n, int inverse, int centred, int engine) {
     OKS_CHECK_CTX();
@@ -70,17 +33,26 @@ extern "C" int okscuda_dft_rows(okscuda_ctx* ctx, const okscuda_c64* d_in, okscu
                        65535ll * 128);
     if (!oks::dft_tc_available())
         return set_err(ctx, OKS_ENOTSUP, "dft_rows: cuTensorMapEncodeTiled is not available from the driver");
-    const void *bhi, *blo;
-    int rc = tc_matrix(ctx, n, sign, centred, &bhi, &blo);
+    const okscuda_ctx::TcMat* mat;
+    int rc = tc_matrix(ctx, n, sign, centred != 0, {}, {}, &mat);
     if (rc) return rc;
     if ((rc = tc_err_flag(ctx))) return rc;
     void* scratch = nullptr;
     OKS_CUDA(cudaMallocAsync(&scratch, oks::dft_tc_scratch_bytes(nrows, n), ctx->stream));
+    oks::DftTcArgs a{};
+    a.in = reinterpret_cast<const float2*>(d_in);
+    a.ld_in = n; a.nin = n;
+    a.out = reinterpret_cast<float2*>(d_out);
+    a.ld_out = n; a.nout = n;
+    a.M = nrows;
+    a.scale = 1.0f;
+    a.b_hi = mat->hi; a.b_lo = mat->lo;
+    a.scratch = scratch;
+    a.err = ctx->tc_err;
     cudaError_t e;
     {
         ProfScope ps(ctx, "k_dft_tc");
-        e = oks::launch_dft_tc(reinterpret_cast<const float2*>(d_in), n, reinterpret_cast<float2*>(d_out), n, nrows,
-                               n, bhi, blo, scratch, 1.0f, ctx->tc_err, ctx->stream);
+        e = oks::launch_dft_tc(a, ctx->stream);
     }
     cudaFreeAsync(scratch, ctx->stream);
     if (e != cudaSuccess) return cuda_err(ctx, e, "dft_rows (tensor cores)");

@@ -132,8 +132,19 @@ struct Epilogue {
     float* out;          // [M][ld] floats (complex64 rows viewed as real)
     long long ld;        // row stride in floats
     long long M;         // rows
-    int ncols;           // real output columns stored (2n)
+    int ncols;           // real output columns stored (2 nout)
     float scale;
+    // complex output column j goes to column cols[j] (cols != nullptr) or
+    // col0 + j; with colbits, a column whose bit is clear in the row's mask
+    // (problem m / rows_per_prob, mask (problem + mask_offset) % mask_mod) is
+    // stored as zero
+    const int* cols;
+    int col0;
+    const uint32_t* colbits;
+    int col_wstride;
+    int rows_per_prob;
+    long long mask_offset;
+    int mask_mod;
 };
 
 __global__ void __launch_bounds__(128, 1)
@@ -212,19 +223,33 @@ k_dft_tc(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CU
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const long long row = (long long)m_tile * BM + warp * 32 + lane;
     const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t* rbits = nullptr;
+    if (ep.colbits && row < ep.M)
+        rbits = ep.colbits + ((row / ep.rows_per_prob + ep.mask_offset) % ep.mask_mod) * ep.col_wstride;
+    float* orow = ep.out + row * ep.ld;
     for (int c = 0; c < BN; c += 16) {
         float v[16];
         tmem_ld16(tl + (uint32_t)c, v);
-        const int col0 = n_tile * BN + c;
-        if (!ok || row >= ep.M || col0 >= ep.ncols) continue;
-        float* dst = ep.out + row * ep.ld + col0;
-        if (col0 + 16 <= ep.ncols && (ep.ld % 4) == 0) {
+        const int rc0 = n_tile * BN + c;   // real output column of v[0]
+        if (!ok || row >= ep.M || rc0 >= ep.ncols) continue;
+        if (!ep.cols && !rbits && rc0 + 16 <= ep.ncols && ((ep.ld | ep.col0) % 2) == 0) {
+            float* dst = orow + 2 * ep.col0 + rc0;
+            if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
 #pragma unroll
-            for (int i = 0; i < 16; i += 4)
-                *reinterpret_cast<float4*>(dst + i) =
-                    make_float4(v[i] * ep.scale, v[i + 1] * ep.scale, v[i + 2] * ep.scale, v[i + 3] * ep.scale);
-        } else {
-            for (int i = 0; i < 16 && col0 + i < ep.ncols; ++i) dst[i] = v[i] * ep.scale;
+                for (int i = 0; i < 16; i += 4)
+                    *reinterpret_cast<float4*>(dst + i) =
+                        make_float4(v[i] * ep.scale, v[i + 1] * ep.scale, v[i + 2] * ep.scale, v[i + 3] * ep.scale);
+                continue;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+            if (rc0 + i >= ep.ncols) break;
+            const int j = (rc0 + i) >> 1;
+            const int x = ep.cols ? ep.cols[j] : ep.col0 + j;
+            const bool keep = !rbits || ((__ldg(rbits + (x >> 5)) >> (x & 31)) & 1u);
+            *reinterpret_cast<float2*>(orow + 2 * x) =
+                keep ? make_float2(v[i] * ep.scale, v[i + 1] * ep.scale) : make_float2(0.f, 0.f);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -232,19 +257,22 @@ k_dft_tc(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CU
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
 }
 
-// X (complex rows, [M][ld] complex) -> hi/lo bf16 [M][kp] (real view, zero
-// padded from 2n to kp columns).
-__global__ void k_split_rows(const float* __restrict__ x, long long ld, long long M, int n2, int kp,
-                             __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
-    const long long total = M * (long long)kp;
+// X (complex rows, [M][ld] complex) -> hi/lo bf16 [M][kp] (real view of the
+// nin gathered columns cols[a] or col0 + a, zero padded to kp reals).
+__global__ void k_split_rows(const float2* __restrict__ x, long long ld, long long M, int nin,
+                             const int* __restrict__ cols, int col0, int kp, __nv_bfloat162* __restrict__ hi,
+                             __nv_bfloat162* __restrict__ lo) {
+    const int kh = kp / 2;
+    const long long total = M * (long long)kh;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const long long m = i / kp;
-        const int k = (int)(i - m * kp);
-        const float v = k < n2 ? x[m * 2 * ld + k] : 0.f;
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        const long long m = i / kh;
+        const int a = (int)(i - m * kh);
+        const float2 v = a < nin ? x[m * ld + (cols ? __ldg(cols + a) : col0 + a)] : make_float2(0.f, 0.f);
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+        const float2 hf = __bfloat1622float2(h);
         hi[i] = h;
-        lo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+        lo[i] = __floats2bfloat162_rn(v.x - hf.x, v.y - hf.y);
     }
 }
 
@@ -291,19 +319,26 @@ static float bf16_float(uint16_t b) {
 int kpad(int n) { return (2 * n + BK - 1) / BK * BK; }
 int npad(int n) { return (2 * n + BN - 1) / BN * BN; }
 
-// B operand of the (centred) DFT of length n, sign -1 forward / +1 inverse:
-// hi and lo, each [npad][kpad] bf16 (B^T, K-major), built in FP64.
-void dft_matrix_split(int n, int sign, int centred, std::vector<uint16_t>* hi, std::vector<uint16_t>* lo) {
-    const int kp = kpad(n), np = npad(n);
+// B operand of the (centred) DFT of length n, sign -1 forward / +1 inverse,
+// from the input columns in_idx (empty: all n) to the output columns out_idx
+// (empty: all n): hi and lo, each [npad(nout)][kpad(nin)] bf16 (B^T,
+// K-major), built in FP64.
+void dft_matrix_split(int n, int sign, int centred, const std::vector<int>& in_idx, const std::vector<int>& out_idx,
+                      std::vector<uint16_t>* hi, std::vector<uint16_t>* lo) {
+    const int nin = in_idx.empty() ? n : (int)in_idx.size();
+    const int nout = out_idx.empty() ? n : (int)out_idx.size();
+    const int kp = kpad(nin), np = npad(nout);
     hi->assign((size_t)np * kp, 0);
     lo->assign((size_t)np * kp, 0);
     const long long h = n / 2;
     const double two_pi = 6.283185307179586476925286766559;
-    for (int j = 0; j < n; ++j)
-        for (int k = 0; k < n; ++k) {
+    for (int j = 0; j < nout; ++j) {
+        const long long jj = out_idx.empty() ? j : out_idx[j];
+        for (int k = 0; k < nin; ++k) {
+            const long long kk = in_idx.empty() ? k : in_idx[k];
             long long e;
-            if (centred) e = (((long long)(j - h) * (k - h)) % n + n) % n;   // fftshift o DFT o ifftshift
-            else e = ((long long)j * k) % n;
+            if (centred) e = (((jj - h) * (kk - h)) % n + n) % n;   // fftshift o DFT o ifftshift
+            else e = (jj * kk) % n;
             const double ang = two_pi * (double)e / n;
             const double c = std::cos(ang), s = sign * std::sin(ang);
             const double vals[4] = {c, -s, s, c};   // [2j][2k], [2j][2k+1], [2j+1][2k], [2j+1][2k+1]
@@ -316,38 +351,51 @@ void dft_matrix_split(int n, int sign, int centred, std::vector<uint16_t>* hi, s
                 (*lo)[idx[q]] = bf16_bits((float)((double)f - (double)bf16_float(bh)));
             }
         }
+    }
 }
 
 }  // namespace tc
 
 bool dft_tc_available() { return tc::encode_fn() != nullptr; }
 
-size_t dft_tc_scratch_bytes(long long M, int n) { return (size_t)M * tc::kpad(n) * 2 * 2; }
+size_t dft_tc_scratch_bytes(long long M, int nin) { return (size_t)M * tc::kpad(nin) * 2 * 2; }
 
-cudaError_t launch_dft_tc(const float2* in, long long ld_in, float2* out, long long ld_out, long long M, int n,
-                          const void* b_hi, const void* b_lo, void* scratch, float scale, int* err, cudaStream_t st) {
+cudaError_t launch_dft_tc(const DftTcArgs& a, cudaStream_t st) {
     using namespace tc;
-    const int kp = kpad(n), np = npad(n);
-    __nv_bfloat16* a_hi = static_cast<__nv_bfloat16*>(scratch);
-    __nv_bfloat16* a_lo = a_hi + (size_t)M * kp;
+    const int kp = kpad(a.nin), np = npad(a.nout);
+    __nv_bfloat16* a_hi = static_cast<__nv_bfloat16*>(a.scratch);
+    __nv_bfloat16* a_lo = a_hi + (size_t)a.M * kp;
     {
-        const long long total = M * (long long)kp;
+        const long long total = a.M * (long long)(kp / 2);
         const int threads = 256;
         const long long blocks = std::min<long long>((total + threads - 1) / threads, 148ll * 16);
-        k_split_rows<<<(unsigned)blocks, threads, 0, st>>>(reinterpret_cast<const float*>(in), ld_in, M, 2 * n, kp,
-                                                           a_hi, a_lo);
+        k_split_rows<<<(unsigned)blocks, threads, 0, st>>>(a.in, a.ld_in, a.M, a.nin, a.in_cols, a.in_col0, kp,
+                                                           reinterpret_cast<__nv_bfloat162*>(a_hi),
+                                                           reinterpret_cast<__nv_bfloat162*>(a_lo));
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     CUtensorMap m_ahi, m_alo, m_bhi, m_blo;
-    if (!make_map(&m_ahi, a_hi, M, kp, BM) || !make_map(&m_alo, a_lo, M, kp, BM) ||
-        !make_map(&m_bhi, b_hi, np, kp, BN) || !make_map(&m_blo, b_lo, np, kp, BN))
+    if (!make_map(&m_ahi, a_hi, a.M, kp, BM) || !make_map(&m_alo, a_lo, a.M, kp, BM) ||
+        !make_map(&m_bhi, a.b_hi, np, kp, BN) || !make_map(&m_blo, a.b_lo, np, kp, BN))
         return cudaErrorInvalidValue;
     e = cudaFuncSetAttribute(k_dft_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    Epilogue ep{reinterpret_cast<float*>(out), 2 * ld_out, M, 2 * n, scale};
-    dim3 grid((unsigned)(np / BN), (unsigned)((M + BM - 1) / BM));
-    k_dft_tc<<<grid, 128, SMEM_BYTES, st>>>(m_ahi, m_alo, m_bhi, m_blo, kp / BK, ep, err);
+    Epilogue ep{};
+    ep.out = reinterpret_cast<float*>(a.out);
+    ep.ld = 2 * a.ld_out;
+    ep.M = a.M;
+    ep.ncols = 2 * a.nout;
+    ep.scale = a.scale;
+    ep.cols = a.out_cols;
+    ep.col0 = a.out_col0;
+    ep.colbits = a.colbits;
+    ep.col_wstride = a.col_wstride;
+    ep.rows_per_prob = a.rows_per_prob > 0 ? a.rows_per_prob : 1;
+    ep.mask_offset = a.mask_offset;
+    ep.mask_mod = a.mask_mod > 0 ? a.mask_mod : 1;
+    dim3 grid((unsigned)(np / BN), (unsigned)((a.M + BM - 1) / BM));
+    k_dft_tc<<<grid, 128, SMEM_BYTES, st>>>(m_ahi, m_alo, m_bhi, m_blo, kp / BK, ep, a.err);
     return cudaGetLastError();
 }
 

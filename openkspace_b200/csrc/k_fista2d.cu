@@ -174,6 +174,66 @@ __global__ void k2d_row(Fista2dArgs a, FftPlan pl, const float2* __restrict__ gt
     }
 }
 
+// ------------------------------------------------ prox between row DFTs
+// The element-wise middle of the row pass when the two row transforms run
+// on the tensor cores (k_dft_tc.cu): W = F_x^H S is in global memory.  One
+// thread per 2x2 block, the same arithmetic as k2d_row above.
+__global__ void k2d_prox(Fista2dArgs a, const float2* __restrict__ W, int mode, int it) {
+    const int ny = a.ny, nx = a.nx, hx = nx / 2, hy = ny / 2;
+    const long long per = (long long)hy * hx;
+    const long long tot = a.nprob * per;
+    const float alpha = mode ? __ldg(a.alpha + it) : 0.f;
+    const float lam = a.lambda;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long p = q / per, b = q - p * per;
+        const int i = (int)(b / hx), j = (int)(b - (long long)i * hx);
+        const long long e0 = p * a.st_stride + (long long)(2 * i) * nx + 2 * j, e1 = e0 + nx;
+        const float4 h0 = *reinterpret_cast<const float4*>(W + e0);
+        const float4 h1 = *reinterpret_cast<const float4*>(W + e1);
+        if (mode == 0) {
+            *reinterpret_cast<float4*>(a.X + e0) = h0;
+            *reinterpret_cast<float4*>(a.X + e1) = h1;
+            *reinterpret_cast<float4*>(a.Z + e0) = h0;
+            *reinterpret_cast<float4*>(a.Z + e1) = h1;
+            continue;
+        }
+        const float4 za = *reinterpret_cast<const float4*>(a.Z + e0);
+        const float4 zd = *reinterpret_cast<const float4*>(a.Z + e1);
+        const float4 xo0 = *reinterpret_cast<const float4*>(a.X + e0);
+        const float4 xo1 = *reinterpret_cast<const float4*>(a.X + e1);
+        const float2 va = make_float2(za.x - h0.x, za.y - h0.y), vb = make_float2(za.z - h0.z, za.w - h0.w);
+        const float2 vd = make_float2(zd.x - h1.x, zd.y - h1.y), ve = make_float2(zd.z - h1.z, zd.w - h1.w);
+        const float2 s0 = va + vb, d0 = va - vb, s1 = vd + ve, d1 = vd - ve;
+        float2 pll = (s0 + s1) * 0.5f, phl = (d0 + d1) * 0.5f;
+        float2 plh = (s0 - s1) * 0.5f, phh = (d0 - d1) * 0.5f;
+        // phh is the LL band of the demodulated image: left untouched
+        pll = shrink2d(pll, lam);
+        phl = shrink2d(phl, lam);
+        plh = shrink2d(plh, lam);
+        const float2 t0 = pll + plh, t1 = phl + phh, t2 = pll - plh, t3 = phl - phh;
+        const float2 xa = (t0 + t1) * 0.5f, xb = (t0 - t1) * 0.5f;
+        const float2 xd = (t2 + t3) * 0.5f, xe = (t2 - t3) * 0.5f;
+        const float2 za2 = xa + (xa - make_float2(xo0.x, xo0.y)) * alpha;
+        const float2 zb2 = xb + (xb - make_float2(xo0.z, xo0.w)) * alpha;
+        const float2 zd2 = xd + (xd - make_float2(xo1.x, xo1.y)) * alpha;
+        const float2 ze2 = xe + (xe - make_float2(xo1.z, xo1.w)) * alpha;
+        *reinterpret_cast<float4*>(a.X + e0) = make_float4(xa.x, xa.y, xb.x, xb.y);
+        *reinterpret_cast<float4*>(a.X + e1) = make_float4(xd.x, xd.y, xe.x, xe.y);
+        *reinterpret_cast<float4*>(a.Z + e0) = make_float4(za2.x, za2.y, zb2.x, zb2.y);
+        *reinterpret_cast<float4*>(a.Z + e1) = make_float4(zd2.x, zd2.y, ze2.x, ze2.y);
+    }
+}
+
+cudaError_t launch_fista2d_prox(const Fista2dArgs& a, const float2* W, int mode, int it, cudaStream_t st) {
+    const long long tot = a.nprob * (long long)(a.ny / 2) * (a.nx / 2);
+    if (tot <= 0) return cudaSuccess;
+    long long blocks = (tot + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k2d_prox<<<(unsigned)blocks, 256, 0, st>>>(a, W, mode, it);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------- demodulated copy
 __global__ void k2d_demod(const float2* __restrict__ X, float2* __restrict__ out, long long nprob, int ny, int nx,
                           long long in_stride, long long out_stride) {

@@ -217,15 +217,43 @@ struct Staging {
 
 // Tensor-core (tcgen05, split 3xBF16) row DFT (k_dft_tc.cu).
 namespace tc {
-int kpad(int n);
-int npad(int n);
-void dft_matrix_split(int n, int sign, int centred, std::vector<uint16_t>* hi, std::vector<uint16_t>* lo);
+int kpad(int n);   // 2n reals rounded up to the K block
+int npad(int n);   // 2n reals rounded up to the N tile
+void dft_matrix_split(int n, int sign, int centred, const std::vector<int>& in_idx, const std::vector<int>& out_idx,
+                      std::vector<uint16_t>* hi, std::vector<uint16_t>* lo);
 }  // namespace tc
 bool dft_tc_available();
-size_t dft_tc_scratch_bytes(long long M, int n);
-// out[m] = scale * in[m] W for M rows (row strides in complex elements);
-// b_hi/b_lo from tc::dft_matrix_split; scratch of dft_tc_scratch_bytes.
-cudaError_t launch_dft_tc(const float2* in, long long ld_in, float2* out, long long ld_out, long long M, int n,
-                          const void* b_hi, const void* b_lo, void* scratch, float scale, int* err, cudaStream_t st);
+size_t dft_tc_scratch_bytes(long long M, int nin);
+// out[m][out col j] = scale * sum_k in[m][in col k] W[k][j] for M rows.
+struct DftTcArgs {
+    const float2* in;
+    long long ld_in;          // complex elements
+    int nin;                  // input columns: in_cols[k] (nullable) or in_col0 + k
+    const int* in_cols;
+    int in_col0;
+    float2* out;
+    long long ld_out;
+    int nout;                 // output columns: out_cols[j] (nullable) or out_col0 + j
+    const int* out_cols;
+    int out_col0;
+    long long M;
+    float scale;
+    // optional: output columns clear in the row's mask are stored as zero
+    // (row m is problem m / rows_per_prob, mask (problem + mask_offset) % mask_mod)
+    const uint32_t* colbits;
+    int col_wstride;
+    int rows_per_prob;
+    long long mask_offset;
+    int mask_mod;
+    const void* b_hi;         // tc::dft_matrix_split of (nin -> nout)
+    const void* b_lo;
+    void* scratch;            // dft_tc_scratch_bytes(M, nin)
+    int* err;                 // bounded-wait error flag
+};
+cudaError_t launch_dft_tc(const DftTcArgs& a, cudaStream_t st);
+// Haar prox + momentum between the two tensor-core transforms of the 2-D
+// engine's row pass (k_fista2d.cu): mode 0 sets X = Z = W; mode 1 forms
+// v = Z - W, shrinks its Haar details, X' = prox, Z' = X' + alpha (X' - X).
+cudaError_t launch_fista2d_prox(const Fista2dArgs& a, const float2* W, int mode, int it, cudaStream_t st);
 
 }  // namespace oks
