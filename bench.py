@@ -41,6 +41,16 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def tc_peak():
+    """Dense bf16 tensor peak in TFLOP/s: the sustained figure (the tensor-core
+    DFTs run inside a seconds-long step)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured (sustained)"
+    return 1400.0, "fallback (sustained)"
+
+
 # --------------------------------------------------------------- workloads
 class PlainWorkload:
     """8 coils, 256 x 256, R = 4 + 24 centre lines, lambda 0.01, 50 iterations."""
@@ -141,6 +151,14 @@ class PrecisionWorkload:
         # k2d_row per problem: the init pass reads S, writes X~, Z~, S (32 B
         # per pixel); every iteration reads S, Z~, X~ and writes X~, Z~, S (48 B)
         return (48.0 * self.iters + 32.0) * self.ny * self.nx * self.nc * self.nz
+
+    tc_flops_model = ("tensor-core row DFTs: per problem and row pass (iterations + init), F_x^H over the "
+                      "rec_x sampled kx columns and F_x back onto them, each 3 bf16 products of "
+                      "2 * ny * (2 rec_x) * (2 nx) FLOPs")
+
+    def tc_flops_per_step(self):
+        per_gemm = 3 * 2.0 * self.ny * (2 * self.vol.rec_x) * (2 * self.nx)
+        return 2 * per_gemm * (self.iters + 1) * self.nc * self.nz
 
     def prepare(self, ctx):
         import torch
@@ -253,18 +271,17 @@ WORKLOADS = {"plain": lambda: PlainWorkload(1), "volume": lambda: PlainWorkload(
              "precision_small": lambda: PrecisionWorkload(2, 4), "batched_small": lambda: BatchedWorkload(6)}
 
 
-def run_serving(args):
+def serving_measure(ctx, rates, seconds, max_requests):
     """Poisson arrivals of single-slice requests (the batched workload's size /
     coil / R / iteration distribution) at several rates through the request
     server, beside the plain per-slice drop-in (okscuda_cs_slice, one at a
-    time, host buffers).  Latency = submit -> result on the host."""
+    time, host buffers).  Latency = submit -> result on the host.  Returns
+    (served per rate, plain)."""
     import threading
 
     import torch
-    from openkspace_b200 import Context, OksError, _lib, synth
+    from openkspace_b200 import OksError, _lib, synth
     from openkspace_b200.server import Server
-    torch.cuda.set_device(0)
-    ctx = Context(0)
     pool = synth.uneven_requests(n=32, workload=3)
     pinned = [torch.from_numpy(r.kspace.view(np.float32)).pin_memory().numpy().view(np.complex64) for r in pool]
     masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in pool]
@@ -280,7 +297,6 @@ def run_serving(args):
     plain_rate = len(pool) / (time.perf_counter() - t0)
     plain = {"slices_per_s": plain_rate, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
              "p99_ms": 1e3 * float(np.percentile(lat, 99))}
-    rates = [float(x) for x in args.rates.split(",")]
     out = {}
     rng = np.random.default_rng(7)
     with Server(ctx, max_inflight=48, n_streams=12) as srv:
@@ -288,7 +304,7 @@ def run_serving(args):
             i, _ = srv.submit(pinned[rid0], masks[rid0], pool[rid0].iters, pool[rid0].lam)
             srv.wait(i, 120000)
         for rate in rates:
-            nreq = int(min(args.requests, max(40, rate * args.seconds)))
+            nreq = int(min(max_requests, max(40, rate * seconds)))
             arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
             outs = [np.empty(pool[i % len(pool)].kspace.shape[1:], np.float32) for i in range(nreq)]
             submitted, done = {}, {}
@@ -326,6 +342,18 @@ def run_serving(args):
             out[str(int(rate))] = {"requests": nreq, "slices_per_s": nreq / span,
                                    "p50_ms": 1e3 * float(np.percentile(lats, 50)),
                                    "p99_ms": 1e3 * float(np.percentile(lats, 99))}
+    return out, plain
+
+
+def run_serving(args):
+    """The serving workload alone: several Poisson rates, one JSON line."""
+    import torch
+    from openkspace_b200 import Context
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    rates = [float(x) for x in args.rates.split(",")]
+    out, plain = serving_measure(ctx, rates, args.seconds, args.requests)
+    plain_rate = plain["slices_per_s"]
     best = max(out.values(), key=lambda v: v["slices_per_s"])
     line = {"metric": "FISTA-CS slices/s + p50/p99 latency (served vs plain)", "value": best["slices_per_s"],
             "unit": "slices/s", "n_gpus": 1, "higher_is_better": True, "dtype": "c64", "data": "synthetic",
@@ -413,8 +441,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain", choices=sorted(WORKLOADS) + ["served"])
+    ap.add_argument("--workload", default="precision", choices=sorted(WORKLOADS) + ["served"])
+    ap.add_argument("--row-engine", default="simt", choices=["simt", "tc"],
+                    help="2-D-mask engine readout transforms: FP32 SIMT FFT or tcgen05 3xBF16 DFT")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="precision: skip the short tensor-core and serving side measurements")
     ap.add_argument("--rates", default="50,200,800", help="served: Poisson arrival rates (req/s)")
     ap.add_argument("--seconds", type=float, default=4.0, help="served: arrivals per rate x this many seconds")
     ap.add_argument("--requests", type=int, default=2000, help="served: at most this many requests per rate")
@@ -447,6 +479,7 @@ def main():
     ctx = Context(local)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
+    ctx.set_option("row_engine", 1 if args.row_engine == "tc" else 0)
     wl.prepare(ctx)
     flush = None
     if wl.input_bytes() < L2_BYTES:
@@ -492,15 +525,37 @@ def main():
     ms, prof = timed(wl.step_device, args.steps, profile=True)
     ms_e2e, _ = timed(wl.step_e2e, args.steps)
     clk = clocks.stop()
+    # precision workload: the other readout engine, a few steps, for the
+    # SIMT FFT vs tensor-core DFT comparison on the same configuration
+    other = None
+    if wl.name == "precision" and not args.no_extras:
+        other_engine = "simt" if args.row_engine == "tc" else "tc"
+        ctx.set_option("row_engine", 1 if other_engine == "tc" else 0)
+        wl.step_device()
+        k_other = 3
+        ms_o, prof_o = timed(wl.step_device, k_other, profile=True)
+        ctx.set_option("row_engine", 1 if args.row_engine == "tc" else 0)
+        other = {"row_engine": other_engine, "steps": k_other, "ms_per_step": ms_o / k_other,
+                 "value": wl.units * k_other * world / (ms_o / 1e3), "unit": "slices/s",
+                 "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof_o.items()}}
 
     units = wl.units * args.steps * world
     value = units / (ms / 1e3)
     e2e_value = units / (ms_e2e / 1e3)
     hbm, peak_kind = peaks()
+    bound, unit, peak, model = "hbm", "GB/s", hbm, wl.bytes_model
     dom_name = next((k for k in wl.dominant if k in prof), wl.dominant[0])
     dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
     # algorithmic bytes of the dominant kernel over the timed steps / its device time
     achieved = wl.dominant_bytes_per_step() * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    if wl.name == "precision" and args.row_engine == "tc":
+        # tensor-core row DFTs: the tcgen05 FLOPs they issue / their device time
+        dom_name = "k_dft_tc"
+        dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
+        bound, unit = "tensor", "TFLOP/s"
+        peak, peak_kind = tc_peak()
+        achieved = wl.tc_flops_per_step() * args.steps / (dom_ms / 1e3) / 1e12 if dom_ms > 0 else 0.0
+        model = wl.tc_flops_model
     launches = int(sum(n for _, n in prof.values()))
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "dram_traffic.json")   # per-launch ncu DRAM bytes, by workload
@@ -521,11 +576,27 @@ def main():
         "e2e": {"value": e2e_value, "unit": "slices/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof.items()},
-        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                     "model": wl.bytes_model},
+        "roofline": {"bound": bound, "kernel": dom_name, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": unit, "frac": achieved / peak, "traffic": traffic,
+                     "model": model},
         "clocks": clk,
     }
+    if wl.name == "precision":
+        line["config"]["row_engine"] = ("FP32 SIMT FFT" if args.row_engine == "simt"
+                                        else "tcgen05 split-3xBF16 DFT-as-GEMM, FP32 accumulation")
+    if other is not None:
+        line["other_row_engine"] = other
+    if wl.name == "precision" and not args.no_extras and world == 1:
+        # the metric's served-vs-plain half: Poisson arrivals at 800 req/s of
+        # the uneven request mix through the request server, beside the
+        # plain per-slice drop-in (host clock, submit -> result on the host)
+        sctx = Context(local)
+        served, plain = serving_measure(sctx, [800.0], 2.0, 400)
+        sctx.close()
+        line["serving"] = {"served": served, "plain": plain,
+                           "served_over_plain": served["800"]["slices_per_s"] / plain["slices_per_s"],
+                           "requests": "sizes {256^2,320^2,384^2,368x640}, coils U{8..32}, R {2,3,4,6}, "
+                                       "iters U{30..150}; --workload served for 50/200/800 req/s"}
     if not args.no_cpu_baseline:
         nthreads = 1
         dt, u, sample = wl.cpu_sample(nthreads)
