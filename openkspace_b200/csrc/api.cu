@@ -63,6 +63,8 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         ctx->mask_bits = value != 0;
     } else if (!std::strcmp(name, "occ2d")) {
         ctx->occ2d = value != 0;
+    } else if (!std::strcmp(name, "prefetch2d")) {
+        ctx->prefetch2d = value != 0;
     } else if (!std::strcmp(name, "row_engine")) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "row_engine: 0 SIMT FFT, 1 tensor-core DFT");
         ctx->row_engine = (int)value;
@@ -383,6 +385,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         a.mask_offset = p0 % nmask;
         a.persist = ctx->persist2d;
         a.occ = ctx->occ2d;
+        a.prefetch = ctx->prefetch2d;
         auto col = [&](int mode) {
             if (col_reg) {
                 ProfScope ps(ctx, "k2d_col_reg", st);

@@ -36,6 +36,7 @@ struct okscuda_ctx {
     int mask_bits = 1;                    // 2-D passes: separable masks read as row/column bits
     int occ2d = 1;                        // 2-D register passes: 1 = launch bounds for 12 warps per SM
     int fista2d_streams = 2;              // 2-D engine: chunks in flight at once (forked streams)
+    int prefetch2d = 1;                   // 2-D register column pass: pipelined loads (separable masks)
     oks::RegTables reg_tables;
     // tensor-core row DFT: split B operands per (n, sign, centred, column
     // sets), device column lists, error flag

@@ -26,6 +26,17 @@ namespace reg {
 
 __device__ __forceinline__ int padi(int i) { return i + (i >> 5); }
 
+// 8-byte asynchronous global -> shared copy; src_bytes 0 writes zeros (the
+// source address is then not read but must still be a valid pointer).
+__device__ __forceinline__ void cp_async8(float2* dst, const float2* src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 template <int SIGN, int R>
 __device__ __forceinline__ void bfly(float2* v, const float2* __restrict__ roots) {
     if constexpr (R == 2) bfly2<SIGN>(v);
@@ -513,6 +524,83 @@ k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float
     const int nx = a.nx, npairs = nx / 2;
     const bool live = t < TA;
     const float minv = a.minv, ysc = a.ysc;
+    if (a.prefetch && a.separable) {
+        // Software-pipelined form: while a unit's transforms run, the loads
+        // of the group's next sampled unit are in flight (cp.async into this
+        // thread's own shared-memory slots, so no barrier guards them).
+        float2* PS = RT + roots_total + G * 2 * P::SMEM_X + g * 2 * E * T;   // [E][T] S, then [E][T] y
+        float2* PY = PS + E * T;
+        const long long total = a.nprob * npairs, stride = (long long)gridDim.x * G;
+        auto next_unit = [&](long long u) {
+            for (; u < total; u += stride) {
+                const long long p = u / npairs;
+                const int x0 = 2 * (int)(u - p * npairs);
+                const long long mi = (p + a.mask_offset) % a.mask_mod;
+                if ((__ldg(a.colbits + mi * a.col_wstride + (x0 >> 5)) >> (x0 & 31)) & 3u) break;
+            }
+            return u;
+        };
+        auto issue = [&](long long u) {
+            const long long p = u / npairs;
+            const int x0 = 2 * (int)(u - p * npairs);
+            const long long mi = (p + a.mask_offset) % a.mask_mod;
+            const uint32_t cpair = (__ldg(a.colbits + mi * a.col_wstride + (x0 >> 5)) >> (x0 & 31)) & 3u;
+            const uint32_t* __restrict__ rb = a.rowbits + mi * a.row_wstride;
+            const float2* y = a.y + p * a.y_stride;
+            const float2* S = a.S + p * a.st_stride;
+            uint32_t mb = 0;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int q = t + TA * e;
+                const int r = q >> 1;
+                const long long off = (long long)r * nx + x0 + (q & 1);
+                const bool m = live && (((__ldg(rb + (r >> 5)) >> (r & 31)) & (cpair >> (q & 1)) & 1u) != 0);
+                if (m) mb |= 1u << e;
+                cp_async8(PY + e * T + t, m ? y + off : y, m ? 8u : 0u);
+                if (mode) cp_async8(PS + e * T + t, live ? S + off : S, live ? 8u : 0u);
+            }
+            cp_async_commit();
+            return mb;
+        };
+        long long u = next_unit((long long)blockIdx.x * G + g);
+        uint32_t mb_next = u < total ? issue(u) : 0u;
+        while (u < total) {
+            const long long cur = u;
+            const uint32_t mb = mb_next;
+            cp_async_wait_all();
+            const long long p = cur / npairs;
+            const int x0 = 2 * (int)(cur - p * npairs);
+            float2 w[E], yv[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int q = t + TA * e;
+                const int r = q >> 1, x = x0 + (q & 1);
+                yv[e] = PY[e * T + t] * (((r + x) & 1) ? -ysc : ysc);
+                w[e] = mode ? PS[e * T + t] : (((mb >> e) & 1u) ? yv[e] * minv : make_float2(0.f, 0.f));
+            }
+            u = next_unit(cur + stride);
+            if (u < total) mb_next = issue(u);   // in flight during the transforms below
+            group_sync<P>();                     // the previous unit's last stage has read A/B
+            if (mode) {
+                forward<P>(w, A, B, TW, RT, t);
+#pragma unroll
+                for (int e = 0; e < E; ++e)
+                    w[e] = ((mb >> e) & 1u) ? (w[e] - yv[e]) * minv : make_float2(0.f, 0.f);
+                group_sync<P>();
+            }
+            inverse<P>(w, A, B, TW, RT, t);
+            if (live) {
+                float2* __restrict__ S = a.S + p * a.st_stride;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int q = t + TA * e;
+                    S[(long long)(q >> 1) * nx + x0 + (q & 1)] = w[e];
+                }
+            }
+        }
+        cp_async_wait_all();
+        return;
+    }
     // persistent: the tables above are loaded once, units are grid-strided
     for (long long unit = (long long)blockIdx.x * G + g; unit < a.nprob * npairs;
          unit += (long long)gridDim.x * G) {
@@ -792,7 +880,9 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X);
+    // the pipelined column pass (separable masks) adds each group's prefetch slots
+    const int pf = (!row && a.prefetch && a.separable) ? 1 : 0;
+    const size_t smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X + (size_t)pf * G * 2 * P::E * P::T);
     if (row) e = cudaFuncSetAttribute(k2d_row_reg<P, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     else e = cudaFuncSetAttribute(k2d_col_reg<P, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -800,16 +890,16 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
     // persistent form: every resident CTA slot once, units grid-strided
     // (the kernels accept any grid)
     if (a.persist) {
-        static int per_sm[2] = {0, 0}, nsm = 0;
-        if (!per_sm[row]) {
+        static int per_sm[2][2] = {{0, 0}, {0, 0}}, nsm = 0;
+        if (!per_sm[row][pf]) {
             int dev = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            if (row) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k2d_row_reg<P, MINB>, P::T * G, smem);
-            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k2d_col_reg<P, MINB>, P::T * G, smem);
-            if (per_sm[row] < 1) per_sm[row] = 1;
+            if (row) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1][pf], k2d_row_reg<P, MINB>, P::T * G, smem);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0][pf], k2d_col_reg<P, MINB>, P::T * G, smem);
+            if (per_sm[row][pf] < 1) per_sm[row][pf] = 1;
         }
-        if (grid > (long long)per_sm[row] * nsm) grid = (long long)per_sm[row] * nsm;
+        if (grid > (long long)per_sm[row][pf] * nsm) grid = (long long)per_sm[row][pf] * nsm;
     }
     if (row)
         k2d_row_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, it, tw, rt, nrt);

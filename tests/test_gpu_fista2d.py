@@ -109,8 +109,9 @@ def ragged_row_mask(rng, ny, nx, frac=0.35):
 @pytest.mark.parametrize("ny,nx,iters", [(368, 640, 5), (256, 256, 6), (384, 320, 4)])
 def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
     """Separable masks read as row/column bits vs as bytes, the two register
-    budgets of the 2-D passes, persistent vs one-CTA-per-unit grids and one
-    vs two chunks in flight give the same result; a ragged (non-separable)
+    budgets of the 2-D passes, persistent vs one-CTA-per-unit grids, one vs
+    two chunks in flight and the pipelined vs plain column pass give the
+    same result; a ragged (non-separable)
     mask takes the byte path and matches FP64."""
     m = partial_row_mask(rng, ny, nx)
     k = np.where(m[None], crandn(rng, (5, ny, nx)), 0).astype(np.complex64)
@@ -118,8 +119,9 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
     forms = [dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2),
              dict(mask_bits=0, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2),
              dict(mask_bits=1, occ2d=0, persist2d=0, fista2d_streams=1, fista2d_chunk=2),
-             dict(mask_bits=1, occ2d=1, persist2d=0, fista2d_streams=3, fista2d_chunk=1)]
-    default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0)
+             dict(mask_bits=1, occ2d=1, persist2d=0, fista2d_streams=3, fista2d_chunk=1),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=0)]
+    default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0, prefetch2d=1)
     results = []
     try:
         for form in forms:
