@@ -74,9 +74,10 @@ const char* okscuda_version(void);
  *                   slot, units grid-strided; 0 = one CTA per unit
  *   "mask_bits"     2-D column pass: 1 = separable masks are read as row
  *                   and column bits instead of mask bytes
- *   "prefetch2d"    2-D register column pass with separable masks: 1
- *                   (default) = the next unit's loads are issued (cp.async)
- *                   before the current unit's transforms
+ *   "prefetch2d"    2-D register passes, the next unit's loads issued
+ *                   (cp.async) before the current unit's transforms: bit 0
+ *                   column pass with separable masks (default 1), bit 1 row
+ *                   pass
  *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
  *                   least 12 warps resident per SM, 0 = registers as needed
  * Any other name returns OKS_EINVAL. */

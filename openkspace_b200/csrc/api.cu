@@ -64,7 +64,8 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
     } else if (!std::strcmp(name, "occ2d")) {
         ctx->occ2d = value != 0;
     } else if (!std::strcmp(name, "prefetch2d")) {
-        ctx->prefetch2d = value != 0;
+        if (value < 0 || value > 3) return set_err(ctx, OKS_EINVAL, "prefetch2d: bit 0 column pass, bit 1 row pass");
+        ctx->prefetch2d = (int)value;
     } else if (!std::strcmp(name, "row_engine")) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "row_engine: 0 SIMT FFT, 1 tensor-core DFT");
         ctx->row_engine = (int)value;
@@ -292,7 +293,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     rc = stage_upload(ctx, up.data(), up.size(), &slot);
     if (rc) return rc;
     long long chunk = ctx->fista2d_chunk > 0 ? ctx->fista2d_chunk
-                                             : std::max<long long>(1, (64ll << 20) / (4 * N * 8));
+                                             : std::max<long long>(1, (96ll << 20) / (4 * N * 8));
     if (chunk > nprob) chunk = nprob;
     // independent chunks run concurrently on `ns` forked streams, each with
     // its own state, so that one chunk's launch tails overlap the other's

@@ -524,7 +524,7 @@ k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float
     const int nx = a.nx, npairs = nx / 2;
     const bool live = t < TA;
     const float minv = a.minv, ysc = a.ysc;
-    if (a.prefetch && a.separable) {
+    if ((a.prefetch & 1) && a.separable) {
         // Software-pipelined form: while a unit's transforms run, the loads
         // of the group's next sampled unit are in flight (cp.async into this
         // thread's own shared-memory slots, so no barrier guards them).
@@ -670,7 +670,36 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
     const float alpha = mode ? __ldg(a.alpha + it) : 0.f;
     const float lam = a.lambda;
     const bool b0 = (t & 1) != 0, b1 = (t & 2) != 0;
-    for (long long unit = (long long)blockIdx.x * G + g; unit < a.nprob * nrp; unit += (long long)gridDim.x * G) {
+    const long long total = a.nprob * nrp, stride = (long long)gridDim.x * G;
+    // pipelined form (a.prefetch bit 1): the next unit's S, Z~, X~ are copied
+    // (cp.async) into this thread's own shared-memory slots while the current
+    // unit's transforms run
+    float2* PF = RT + roots_total + G * 2 * P::SMEM_X + g * 3 * E * T;   // [E][T] S, Z~, X~
+    auto issue = [&](long long u) {
+        const long long p = u / nrp;
+        const int r0 = 2 * (int)(u - p * nrp);
+        const uint32_t* cb = a.colbits + ((p + a.mask_offset) % a.mask_mod) * a.col_wstride;
+        const long long base = p * a.st_stride + (long long)r0 * N;
+        const float2* S = a.S + base;
+        const float2* X = a.X + base;
+        const float2* Z = a.Z + base;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int q = t + TA * e;
+            const int x = q >> 1;
+            const long long off = (long long)(q & 1) * N + x;
+            const bool on = live && ((__ldg(cb + (x >> 5)) >> (x & 31)) & 1u);
+            cp_async8(PF + e * T + t, on ? S + off : S, on ? 8u : 0u);
+            if (mode) {
+                cp_async8(PF + (E + e) * T + t, live ? Z + off : Z, live ? 8u : 0u);
+                cp_async8(PF + (2 * E + e) * T + t, live ? X + off : X, live ? 8u : 0u);
+            }
+        }
+        cp_async_commit();
+    };
+    const bool pf = (a.prefetch & 2) != 0;
+    if (pf && (long long)blockIdx.x * G + g < total) issue((long long)blockIdx.x * G + g);
+    for (long long unit = (long long)blockIdx.x * G + g; unit < total; unit += stride) {
         const long long p = unit / nrp;
         const int r0 = 2 * (int)(unit - p * nrp);
         const long long mi = (p + a.mask_offset) % a.mask_mod;
@@ -682,16 +711,29 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
         // every global load of the unit is issued before any store
         float2 w[E], zo[E], xo[E];
         uint32_t cm = 0;                       // column sampled, per element
+        if (pf) {
+            cp_async_wait_all();
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int q = t + TA * e;
-            const int x = q >> 1;
-            const long long off = (long long)(q & 1) * N + x;
-            const bool on = live && ((cb[x >> 5] >> (x & 31)) & 1u);
-            if (on) cm |= 1u << e;
-            w[e] = on ? S[off] : make_float2(0.f, 0.f);
-            zo[e] = (mode && live) ? Z[off] : make_float2(0.f, 0.f);
-            xo[e] = (mode && live) ? X[off] : make_float2(0.f, 0.f);
+            for (int e = 0; e < E; ++e) {
+                const int x = (t + TA * e) >> 1;
+                if (live && ((__ldg(cb + (x >> 5)) >> (x & 31)) & 1u)) cm |= 1u << e;
+                w[e] = PF[e * T + t];
+                zo[e] = mode ? PF[(E + e) * T + t] : make_float2(0.f, 0.f);
+                xo[e] = mode ? PF[(2 * E + e) * T + t] : make_float2(0.f, 0.f);
+            }
+            if (unit + stride < total) issue(unit + stride);   // in flight during the transforms below
+        } else {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int q = t + TA * e;
+                const int x = q >> 1;
+                const long long off = (long long)(q & 1) * N + x;
+                const bool on = live && ((cb[x >> 5] >> (x & 31)) & 1u);
+                if (on) cm |= 1u << e;
+                w[e] = on ? S[off] : make_float2(0.f, 0.f);
+                zo[e] = (mode && live) ? Z[off] : make_float2(0.f, 0.f);
+                xo[e] = (mode && live) ? X[off] : make_float2(0.f, 0.f);
+            }
         }
         group_sync<P>();                       // the previous unit's last stage has read A/B
         inverse<P>(w, A, B, TW, RT, t);
@@ -741,6 +783,7 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
             }
         }
     }
+    if (pf) cp_async_wait_all();
 }
 
 // ------------------------------------------- SENSE mode, register form
@@ -881,8 +924,15 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
     // the pipelined column pass (separable masks) adds each group's prefetch slots
-    const int pf = (!row && a.prefetch && a.separable) ? 1 : 0;
-    const size_t smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X + (size_t)pf * G * 2 * P::E * P::T);
+    // and the pipelined row pass its three
+    // (left out where they would cost resident CTAs below MINB per SM)
+    Fista2dArgs b = a;
+    const size_t base_smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X);
+    const size_t pf_smem = sizeof(float2) * (size_t)G * (row ? 3 : 2) * P::E * P::T;
+    int pf = row ? ((a.prefetch & 2) ? 1 : 0) : ((a.separable && (a.prefetch & 1)) ? 1 : 0);
+    if (pf && MINB > 1 && (base_smem + pf_smem + 1024) * MINB > 220u * 1024u) pf = 0;
+    b.prefetch = pf;
+    const size_t smem = base_smem + (pf ? pf_smem : 0);
     if (row) e = cudaFuncSetAttribute(k2d_row_reg<P, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     else e = cudaFuncSetAttribute(k2d_col_reg<P, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -902,9 +952,9 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
         if (grid > (long long)per_sm[row][pf] * nsm) grid = (long long)per_sm[row][pf] * nsm;
     }
     if (row)
-        k2d_row_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, it, tw, rt, nrt);
+        k2d_row_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(b, mode, it, tw, rt, nrt);
     else
-        k2d_col_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(a, mode, tw, rt, nrt);
+        k2d_col_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(b, mode, tw, rt, nrt);
     return cudaGetLastError();
 }
 

@@ -144,7 +144,8 @@ struct Fista2dArgs {
     long long nprob;
     int persist;              // register passes: grid of resident CTAs, units grid-strided
     int occ;                  // register passes: 0 registers as needed, 1 at least 12 warps per SM
-    int prefetch;             // register column pass, separable masks: next unit's loads in flight (cp.async)
+    int prefetch;             // register passes: next unit's loads in flight (cp.async); bit 0 column
+                              // pass (separable masks), bit 1 row pass
 };
 cudaError_t launch_fista2d_col(const Fista2dArgs& a, const DevPlan& py, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_row(const Fista2dArgs& a, const DevPlan& px, int mode, int it, cudaStream_t st);
