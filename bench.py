@@ -123,8 +123,13 @@ class PrecisionWorkload:
     (FP64 noise fit, prewhitening, oversampling removal, placement, FISTA at
     the reference's 368 x 640 grid with partial-row masks, RSS, crop to 320)."""
     name = "precision"
-    dominant = ("k2d_row_reg", "k2d_row")
-    bytes_model = "row pass: 48 B per pixel per problem per iteration (read S, Z, X; write X, Z, S), 32 B init"
+    # the 2-D engine runs as one CUDA graph per call (all chunks and
+    # iterations); without graphs its row pass is the largest kernel
+    dominant = ("k2d_graph", "k2d_row_reg", "k2d_row")
+    bytes_model = ("2-D engine, column + row pass per problem and iteration: column pass reads S and writes S "
+                   "on the sampled kx columns (fraction f_c) and reads y on the sampled (ky, kx) points "
+                   "(f_c f_r); row pass reads S (f_c), Z~, X~ and writes X~, Z~, S (f_c): "
+                   "8 (6 f_c + 4 + f_c f_r) B per pixel; init passes and the demodulated copy added")
 
     def __init__(self, nz: int = 36, iters: int = 120):
         from openkspace_b200 import synth
@@ -147,10 +152,17 @@ class PrecisionWorkload:
     def input_bytes(self):
         return self.acqs.data.nbytes
 
-    def dominant_bytes_per_step(self):
+    def dominant_bytes_per_step(self, kernel=None):
+        npx = self.ny * self.nx * self.nc * self.nz
+        if kernel in (None, "k2d_graph"):
+            f_c = self.vol.rec_x / self.nx
+            f_r = len(self.vol.ky_index[0]) / self.ny
+            per_iter = 8.0 * (6 * f_c + 4 + f_c * f_r)
+            init = 8.0 * (2 * f_c + f_c * f_r) + 8.0 * (2 * f_c + 2)
+            return (per_iter * self.iters + init + 16.0) * npx
         # k2d_row per problem: the init pass reads S, writes X~, Z~, S (32 B
         # per pixel); every iteration reads S, Z~, X~ and writes X~, Z~, S (48 B)
-        return (48.0 * self.iters + 32.0) * self.ny * self.nx * self.nc * self.nz
+        return (48.0 * self.iters + 32.0) * npx
 
     tc_flops_model = ("tensor-core row DFTs: per problem and row pass (iterations + init), F_x^H over the "
                       "rec_x sampled kx columns and F_x back onto them, each 3 bf16 products of "
@@ -382,7 +394,7 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -547,7 +559,8 @@ def main():
     dom_name = next((k for k in wl.dominant if k in prof), wl.dominant[0])
     dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
     # algorithmic bytes of the dominant kernel over the timed steps / its device time
-    achieved = wl.dominant_bytes_per_step() * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    dbytes = wl.dominant_bytes_per_step(dom_name) if wl.name == "precision" else wl.dominant_bytes_per_step()
+    achieved = dbytes * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     if wl.name == "precision" and args.row_engine == "tc":
         # tensor-core row DFTs: the tcgen05 FLOPs they issue / their device time
         dom_name = "k_dft_tc"

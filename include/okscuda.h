@@ -80,8 +80,27 @@ const char* okscuda_version(void);
  *                   pass
  *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
  *                   least 12 warps resident per SM, 0 = registers as needed
+ *   "autotune_use"  1 (default): shapes in the autotune table use their
+ *                   tuned choices in place of the options above; 0: ignore
+ *                   the table
+ *   "autotune_clear" (any value) empties the autotune table
  * Any other name returns OKS_EINVAL. */
 int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value);
+/* Autotuner (no reference counterpart): times the plan and launch-shape
+ * candidates of the FISTA engine for one shape on seeded synthetic data on
+ * the device and keeps the fastest for that shape in the context's table.
+ * kind 0: ky-only masks (column engine: register plan variants, generic
+ * kernel; the choice applies to every nx).  kind 1: 2-D masks with partial
+ * rows (register budget, pipelined loads, chunks in flight, chunk size).  nc
+ * problems, `iters` iterations per timing call.  A JSON report of every
+ * candidate's time and the choice is written to report (may be NULL). */
+int okscuda_autotune(okscuda_ctx* ctx, int kind, int ny, int nx, int nc, int iters, char* report,
+                     size_t report_len);
+/* The table as text, one line per shape ("kind ny nx col_engine col_variant
+ * persist2d occ2d prefetch2d fista2d_streams fista2d_chunk"), and loading such
+ * text back (added to the table; OKS_EINVAL on a malformed line). */
+int okscuda_autotune_table(okscuda_ctx* ctx, char* buf, size_t len);
+int okscuda_autotune_load(okscuda_ctx* ctx, const char* text);
 
 /* ---------------------------------------------------------- device memory */
 int okscuda_malloc(okscuda_ctx* ctx, size_t bytes, void** d_ptr);

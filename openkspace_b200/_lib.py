@@ -42,6 +42,9 @@ SIGNATURES = {
     "okscuda_synchronize": (_i, [_vp]),
     "okscuda_version": (_c.c_char_p, []),
     "okscuda_set_option": (_i, [_vp, _c.c_char_p, _c.c_longlong]),
+    "okscuda_autotune": (_i, [_vp, _i, _i, _i, _i, _i, _c.c_char_p, _sz]),
+    "okscuda_autotune_table": (_i, [_vp, _c.c_char_p, _sz]),
+    "okscuda_autotune_load": (_i, [_vp, _c.c_char_p]),
     "okscuda_malloc": (_i, [_vp, _sz, _c.POINTER(_vp)]),
     "okscuda_free": (_i, [_vp, _vp]),
     "okscuda_upload": (_i, [_vp, _vp, _vp, _sz]),

@@ -43,6 +43,7 @@ void okscuda_destroy(okscuda_ctx* ctx) {
         cudaFree(kv.second.out_cols);
     }
     if (ctx->tc_err) cudaFree(ctx->tc_err);
+    for (auto& kv : ctx->g2d) free_graph2d(kv.second);
     for (auto& a : ctx->aux) { cudaStreamDestroy(a.stream); cudaEventDestroy(a.done); }
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -66,6 +67,17 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
     } else if (!std::strcmp(name, "prefetch2d")) {
         if (value < 0 || value > 3) return set_err(ctx, OKS_EINVAL, "prefetch2d: bit 0 column pass, bit 1 row pass");
         ctx->prefetch2d = (int)value;
+    } else if (!std::strcmp(name, "graph2d")) {
+        ctx->graph2d = value != 0;
+        if (!ctx->graph2d) {
+            cudaDeviceSynchronize();
+            for (auto& kv : ctx->g2d) free_graph2d(kv.second);
+            ctx->g2d.clear();
+        }
+    } else if (!std::strcmp(name, "autotune_use")) {
+        ctx->use_tuned = value != 0;
+    } else if (!std::strcmp(name, "autotune_clear")) {
+        ctx->tuned.clear();
     } else if (!std::strcmp(name, "row_engine")) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "row_engine: 0 SIMT FFT, 1 tensor-core DFT");
         ctx->row_engine = (int)value;
@@ -292,13 +304,14 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     oks::Staging::Slot* slot = nullptr;
     rc = stage_upload(ctx, up.data(), up.size(), &slot);
     if (rc) return rc;
-    long long chunk = ctx->fista2d_chunk > 0 ? ctx->fista2d_chunk
+    const TuneParams tp = tune_params(ctx, 1, ny, nx);
+    long long chunk = tp.fista2d_chunk > 0 ? tp.fista2d_chunk
                                              : std::max<long long>(1, (96ll << 20) / (4 * N * 8));
     if (chunk > nprob) chunk = nprob;
     // independent chunks run concurrently on `ns` forked streams, each with
     // its own state, so that one chunk's launch tails overlap the other's
     const long long nchunks = (nprob + chunk - 1) / chunk;
-    const int ns = (int)std::max<long long>(1, std::min<long long>(ctx->fista2d_streams, nchunks));
+    const int ns = (int)std::max<long long>(1, std::min<long long>(tp.fista2d_streams, nchunks));
     // row pass on the tensor cores (row_engine 1): F_x^H restricted to the kx
     // columns any mask samples, prox, F_x back onto those columns
     const bool use_tc = ctx->row_engine == 1;
@@ -328,136 +341,225 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         tc_split = (tc_split + 255) & ~size_t(255);
     }
     const size_t stream_bytes = ((sizeof(float2) * per_stream + 255) & ~size_t(255)) + tc_split;
-    void* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(&scratch, stream_bytes * ns, ctx->stream);
-    if (e != cudaSuccess) { stage_release(ctx, slot); return cuda_err(ctx, e, "cudaMallocAsync(fista2d)"); }
     const int hs = ((ny / 2) + (nx / 2)) & 1;
     // register-resident passes where a compile-time plan exists (col_engine 1
     // forces the generic shared-memory passes)
-    const bool col_reg = ctx->col_engine != 1 && oks::fista2d_reg_supported(ny);
-    const bool row_reg = ctx->col_engine != 1 && oks::fista2d_reg_supported(nx);
+    const bool col_reg = tp.col_engine != 1 && oks::fista2d_reg_supported(ny);
+    const bool row_reg = tp.col_engine != 1 && oks::fista2d_reg_supported(nx);
+    cudaError_t e = cudaSuccess;
     if ((col_reg || row_reg) && (e = oks::reg_tables_init(&ctx->reg_tables)) != cudaSuccess) {
-        cudaFreeAsync(scratch, ctx->stream);
         stage_release(ctx, slot);
         return cuda_err(ctx, e, "register tables");
     }
-    if (ns > 1) {
-        rc = ensure_aux_streams(ctx, ns);
-        if (!rc && (e = cudaEventRecord(ctx->fork_ev, ctx->stream)) != cudaSuccess) rc = cuda_err(ctx, e, "fork");
-        for (int k = 0; k < ns && !rc; ++k)
-            if ((e = cudaStreamWaitEvent(ctx->aux[k].stream, ctx->fork_ev, 0)) != cudaSuccess)
-                rc = cuda_err(ctx, e, "fork");
-        if (rc) {
-            cudaFreeAsync(scratch, ctx->stream);
-            stage_release(ctx, slot);
-            return rc;
-        }
+    if (ns > 1 && (rc = ensure_aux_streams(ctx, ns))) {
+        stage_release(ctx, slot);
+        return rc;
     }
-    long long ci = 0;
-    for (long long p0 = 0; p0 < nprob && e == cudaSuccess; p0 += chunk, ++ci) {
-        const int k = (int)(ci % ns);
-        cudaStream_t st = ns > 1 ? ctx->aux[k].stream : ctx->stream;
-        uint8_t* sbase = static_cast<uint8_t*>(scratch) + (size_t)k * stream_bytes;
-        float2* base = reinterpret_cast<float2*>(sbase);
-        float2* W = base + 3 * chunk * N;                                      // tensor-core mode only
-        void* split = sbase + ((sizeof(float2) * per_stream + 255) & ~size_t(255));
-        oks::Fista2dArgs a{};
-        a.nprob = std::min(chunk, nprob - p0);
-        a.y = reinterpret_cast<const float2*>(d_kspace) + p0 * N;
-        a.y_stride = N;
-        // problem p0 + i uses mask (p0 + i) % nmask (mask_offset = p0 % nmask)
-        a.mask_mod = nmask;
-        a.mask_stride = N;
-        a.mask = static_cast<const uint8_t*>(slot->dev);
-        a.colbits = reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(slot->dev) + cb_off);
-        a.col_wstride = cw;
-        a.rowbits = reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(slot->dev) + rb_off);
-        a.row_wstride = rw;
-        a.separable = separable && ctx->mask_bits != 0;
-        a.X = base + 2 * chunk * N;
-        a.Z = base;
-        a.S = a.Z + chunk * N;
-        a.st_stride = N;
-        a.ny = ny; a.nx = nx;
-        a.ysc = std::sqrt((float)ny * (float)nx) * (hs ? -1.f : 1.f);
-        a.minv = 1.0f / ((float)ny * (float)nx);
-        a.lambda = lambda;
-        a.alpha = alpha;
-        a.mask_offset = p0 % nmask;
-        a.persist = ctx->persist2d;
-        a.occ = ctx->occ2d;
-        a.prefetch = ctx->prefetch2d;
-        auto col = [&](int mode) {
-            if (col_reg) {
-                ProfScope ps(ctx, "k2d_col_reg", st);
-                return oks::launch_fista2d_col_reg(a, ctx->reg_tables, mode, st);
-            }
-            ProfScope ps(ctx, "k2d_col", st);
-            return oks::launch_fista2d_col(a, *py, mode, st);
-        };
-        auto row = [&](int mode, int it) {
-            if (use_tc) {
-                const bool contiguous = tcols.back() - tcols.front() + 1 == (int)tcols.size();
-                oks::DftTcArgs t{};
-                t.M = a.nprob * ny;
-                t.scale = 1.0f;
-                t.scratch = split;
-                t.err = ctx->tc_err;
-                // h = F_x^H S over the sampled columns
-                t.in = a.S; t.ld_in = nx; t.nin = (int)tcols.size();
-                t.in_cols = contiguous ? nullptr : m_inv->in_cols;
-                t.in_col0 = contiguous ? tcols.front() : 0;
-                t.out = W; t.ld_out = nx; t.nout = nx;
-                t.b_hi = m_inv->hi; t.b_lo = m_inv->lo;
-                cudaError_t e1;
-                {
+
+    // The whole launch sequence of one call: chunks round-robin over `ns`
+    // forked streams, every iteration's column and row pass, the demodulated
+    // copy out.  Inputs, outputs, masks and scratch are parameters so that the
+    // same sequence can be captured once into a CUDA graph over buffers the
+    // graph owns (below).
+    auto enqueue = [&](const float2* ysrc, float2* outdst, const uint8_t* mdev, void* scratch) -> cudaError_t {
+        cudaError_t err = cudaSuccess;
+        if (ns > 1) {
+            if ((err = cudaEventRecord(ctx->fork_ev, ctx->stream)) != cudaSuccess) return err;
+            for (int k = 0; k < ns; ++k)
+                if ((err = cudaStreamWaitEvent(ctx->aux[k].stream, ctx->fork_ev, 0)) != cudaSuccess) return err;
+        }
+        long long ci = 0;
+        for (long long p0 = 0; p0 < nprob && err == cudaSuccess; p0 += chunk, ++ci) {
+            const int k = (int)(ci % ns);
+            cudaStream_t st = ns > 1 ? ctx->aux[k].stream : ctx->stream;
+            uint8_t* sbase = static_cast<uint8_t*>(scratch) + (size_t)k * stream_bytes;
+            float2* base = reinterpret_cast<float2*>(sbase);
+            float2* W = base + 3 * chunk * N;                                      // tensor-core mode only
+            void* split = sbase + ((sizeof(float2) * per_stream + 255) & ~size_t(255));
+            oks::Fista2dArgs a{};
+            a.nprob = std::min(chunk, nprob - p0);
+            a.y = ysrc + p0 * N;
+            a.y_stride = N;
+            // problem p0 + i uses mask (p0 + i) % nmask (mask_offset = p0 % nmask)
+            a.mask_mod = nmask;
+            a.mask_stride = N;
+            a.mask = mdev;
+            a.colbits = reinterpret_cast<const uint32_t*>(mdev + cb_off);
+            a.col_wstride = cw;
+            a.rowbits = reinterpret_cast<const uint32_t*>(mdev + rb_off);
+            a.row_wstride = rw;
+            a.separable = separable && ctx->mask_bits != 0;
+            a.X = base + 2 * chunk * N;
+            a.Z = base;
+            a.S = a.Z + chunk * N;
+            a.st_stride = N;
+            a.ny = ny; a.nx = nx;
+            a.ysc = std::sqrt((float)ny * (float)nx) * (hs ? -1.f : 1.f);
+            a.minv = 1.0f / ((float)ny * (float)nx);
+            a.lambda = lambda;
+            a.alpha = alpha;
+            a.mask_offset = p0 % nmask;
+            a.persist = tp.persist2d;
+            a.occ = tp.occ2d;
+            a.prefetch = tp.prefetch2d;
+            auto col = [&](int mode) {
+                if (col_reg) {
+                    ProfScope ps(ctx, "k2d_col_reg", st);
+                    return oks::launch_fista2d_col_reg(a, ctx->reg_tables, mode, st);
+                }
+                ProfScope ps(ctx, "k2d_col", st);
+                return oks::launch_fista2d_col(a, *py, mode, st);
+            };
+            auto row = [&](int mode, int it) {
+                if (use_tc) {
+                    const bool contiguous = tcols.back() - tcols.front() + 1 == (int)tcols.size();
+                    oks::DftTcArgs t{};
+                    t.M = a.nprob * ny;
+                    t.scale = 1.0f;
+                    t.scratch = split;
+                    t.err = ctx->tc_err;
+                    // h = F_x^H S over the sampled columns
+                    t.in = a.S; t.ld_in = nx; t.nin = (int)tcols.size();
+                    t.in_cols = contiguous ? nullptr : m_inv->in_cols;
+                    t.in_col0 = contiguous ? tcols.front() : 0;
+                    t.out = W; t.ld_out = nx; t.nout = nx;
+                    t.b_hi = m_inv->hi; t.b_lo = m_inv->lo;
+                    cudaError_t e1;
+                    {
+                        ProfScope ps(ctx, "k_dft_tc", st);
+                        e1 = oks::launch_dft_tc(t, st);
+                    }
+                    if (e1 != cudaSuccess) return e1;
+                    {
+                        ProfScope ps(ctx, "k2d_prox", st);
+                        e1 = oks::launch_fista2d_prox(a, W, mode, it, st);
+                    }
+                    if (e1 != cudaSuccess) return e1;
+                    // S = F_x z~' on the sampled columns, zero where the row's mask is clear
+                    oks::DftTcArgs f = t;
+                    f.in = a.Z; f.nin = nx; f.in_cols = nullptr; f.in_col0 = 0;
+                    f.out = a.S; f.nout = (int)tcols.size();
+                    f.out_cols = contiguous ? nullptr : m_fwd->out_cols;
+                    f.out_col0 = contiguous ? tcols.front() : 0;
+                    f.colbits = a.colbits; f.col_wstride = cw; f.rows_per_prob = ny;
+                    f.mask_offset = a.mask_offset; f.mask_mod = nmask;
+                    f.b_hi = m_fwd->hi; f.b_lo = m_fwd->lo;
                     ProfScope ps(ctx, "k_dft_tc", st);
-                    e1 = oks::launch_dft_tc(t, st);
+                    return oks::launch_dft_tc(f, st);
                 }
-                if (e1 != cudaSuccess) return e1;
-                {
-                    ProfScope ps(ctx, "k2d_prox", st);
-                    e1 = oks::launch_fista2d_prox(a, W, mode, it, st);
+                if (row_reg) {
+                    ProfScope ps(ctx, "k2d_row_reg", st);
+                    return oks::launch_fista2d_row_reg(a, ctx->reg_tables, mode, it, st);
                 }
-                if (e1 != cudaSuccess) return e1;
-                // S = F_x z~' on the sampled columns, zero where the row's mask is clear
-                oks::DftTcArgs f = t;
-                f.in = a.Z; f.nin = nx; f.in_cols = nullptr; f.in_col0 = 0;
-                f.out = a.S; f.nout = (int)tcols.size();
-                f.out_cols = contiguous ? nullptr : m_fwd->out_cols;
-                f.out_col0 = contiguous ? tcols.front() : 0;
-                f.colbits = a.colbits; f.col_wstride = cw; f.rows_per_prob = ny;
-                f.mask_offset = a.mask_offset; f.mask_mod = nmask;
-                f.b_hi = m_fwd->hi; f.b_lo = m_fwd->lo;
-                ProfScope ps(ctx, "k_dft_tc", st);
-                return oks::launch_dft_tc(f, st);
+                ProfScope ps(ctx, "k2d_row", st);
+                return oks::launch_fista2d_row(a, *px, mode, it, st);
+            };
+            // the tensor-core row pass reads every sampled column of S, also
+            // those of column pairs the column pass skips for this problem's mask
+            if (use_tc) err = cudaMemsetAsync(a.S, 0, sizeof(float2) * a.nprob * N, st);
+            if (err == cudaSuccess) err = col(0);
+            if (err == cudaSuccess) err = row(0, 0);
+            for (int it = 0; it < iters && err == cudaSuccess; ++it) {
+                err = col(1);
+                if (err == cudaSuccess) err = row(1, it);
             }
-            if (row_reg) {
-                ProfScope ps(ctx, "k2d_row_reg", st);
-                return oks::launch_fista2d_row_reg(a, ctx->reg_tables, mode, it, st);
+            if (err == cudaSuccess) {
+                ProfScope ps(ctx, "k2d_demod", st);
+                err = oks::launch_fista2d_demod(a.X, outdst + p0 * N, a.nprob, ny, nx, N, N, st);
             }
-            ProfScope ps(ctx, "k2d_row", st);
-            return oks::launch_fista2d_row(a, *px, mode, it, st);
-        };
-        // the tensor-core row pass reads every sampled column of S, also
-        // those of column pairs the column pass skips for this problem's mask
-        if (use_tc) e = cudaMemsetAsync(a.S, 0, sizeof(float2) * a.nprob * N, st);
-        if (e == cudaSuccess) e = col(0);
-        if (e == cudaSuccess) e = row(0, 0);
-        for (int it = 0; it < iters && e == cudaSuccess; ++it) {
-            e = col(1);
-            if (e == cudaSuccess) e = row(1, it);
         }
-        if (e == cudaSuccess) {
-            ProfScope ps(ctx, "k2d_demod", st);
-            e = oks::launch_fista2d_demod(a.X, reinterpret_cast<float2*>(d_out) + p0 * N, a.nprob, ny, nx, N, N, st);
+        // join (also after a launch error)
+        for (int k = 0; k < ns && ns > 1; ++k) {
+            cudaEventRecord(ctx->aux[k].done, ctx->aux[k].stream);
+            cudaStreamWaitEvent(ctx->stream, ctx->aux[k].done, 0);
+        }
+        return err;
+    };
+
+    // CUDA-graph form (graph2d, SIMT row engine): the second call with the
+    // same shape, iterations, lambda and choices captures the launch sequence
+    // over buffers owned by the cache entry; every later call copies its
+    // k-space and masks in, replays the graph (one launch for all chunks and
+    // iterations) and copies the coil images out.  The first call runs the
+    // launches directly, which also creates every table the capture needs.
+    const size_t data_bytes = sizeof(float2) * (size_t)nprob * N;
+    if (ctx->graph2d && !use_tc) {
+        char kb[320];
+        std::snprintf(kb, sizeof kb, "%d/%d/%lld/%d/%d/%08x/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%zu/%d", ny, nx, nprob, nmask, iters,
+                      [&] { uint32_t u; std::memcpy(&u, &lambda, 4); return u; }(), chunk, ns, (int)col_reg,
+                      (int)row_reg, tp.persist2d, tp.occ2d, tp.prefetch2d, (int)separable, ctx->mask_bits, up.size(),
+                      ctx->device);
+        const std::string key(kb);
+        auto it = ctx->g2d.find(key);
+        if (it == ctx->g2d.end()) {
+            ctx->g2d.emplace(key, okscuda_ctx::Graph2d{});   // seen once: run directly this time
+        } else if (!it->second.failed) {
+            okscuda_ctx::Graph2d& g = it->second;
+            g.last_use = ++ctx->g2d_clock;
+            if (!g.exec) {
+                // evict the least recently used entry beyond the cache size
+                if (ctx->g2d.size() > 4) {
+                    auto victim = ctx->g2d.end();
+                    for (auto v = ctx->g2d.begin(); v != ctx->g2d.end(); ++v)
+                        if (v != it && (victim == ctx->g2d.end() || v->second.last_use < victim->second.last_use))
+                            victim = v;
+                    if (victim != ctx->g2d.end()) {
+                        cudaDeviceSynchronize();
+                        free_graph2d(victim->second);
+                        ctx->g2d.erase(victim);
+                    }
+                }
+                cudaError_t ge = cudaMalloc(&g.y, data_bytes);
+                if (ge == cudaSuccess) ge = cudaMalloc(&g.out, data_bytes);
+                if (ge == cudaSuccess) ge = cudaMalloc(&g.masks, up.size());
+                if (ge == cudaSuccess) ge = cudaMalloc(&g.scratch, stream_bytes * ns);
+                if (ge == cudaSuccess) ge = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
+                if (ge == cudaSuccess) {
+                    const bool prof = ctx->prof_on;
+                    ctx->prof_on = false;
+                    cudaGraph_t graph = nullptr;
+                    ge = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+                    if (ge == cudaSuccess) {
+                        cudaError_t le = enqueue(static_cast<const float2*>(g.y), static_cast<float2*>(g.out),
+                                                 static_cast<const uint8_t*>(g.masks), g.scratch);
+                        ge = cudaStreamEndCapture(ctx->stream, &graph);
+                        if (le != cudaSuccess) ge = le;
+                    }
+                    if (ge == cudaSuccess) ge = cudaGraphInstantiate(&g.exec, graph, 0);
+                    if (graph) cudaGraphDestroy(graph);
+                    ctx->prof_on = prof;
+                }
+                if (ge != cudaSuccess) {
+                    (void)cudaGetLastError();
+                    free_graph2d(g);
+                    g.failed = true;   // this shape keeps the direct launches
+                }
+            }
+            if (g.exec) {
+                cudaError_t ge = cudaStreamWaitEvent(ctx->stream, g.done, 0);   // the previous replay is done
+                if (ge == cudaSuccess)
+                    ge = cudaMemcpyAsync(g.masks, slot->dev, up.size(), cudaMemcpyDeviceToDevice, ctx->stream);
+                if (ge == cudaSuccess)
+                    ge = cudaMemcpyAsync(g.y, d_kspace, data_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+                if (ge == cudaSuccess) {
+                    ProfScope ps(ctx, "k2d_graph");
+                    ge = cudaGraphLaunch(g.exec, ctx->stream);
+                }
+                if (ge == cudaSuccess)
+                    ge = cudaMemcpyAsync(d_out, g.out, data_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+                if (ge == cudaSuccess) ge = cudaEventRecord(g.done, ctx->stream);
+                stage_release(ctx, slot);
+                if (ge != cudaSuccess) return cuda_err(ctx, ge, "fista2d graph replay");
+                return OKS_OK;
+            }
         }
     }
-    // join (also after a launch error: the scratch is freed on ctx->stream)
-    for (int k = 0; k < ns && ns > 1; ++k) {
-        cudaEventRecord(ctx->aux[k].done, ctx->aux[k].stream);
-        cudaStreamWaitEvent(ctx->stream, ctx->aux[k].done, 0);
-    }
+
+    void* scratch = nullptr;
+    e = cudaMallocAsync(&scratch, stream_bytes * ns, ctx->stream);
+    if (e != cudaSuccess) { stage_release(ctx, slot); return cuda_err(ctx, e, "cudaMallocAsync(fista2d)"); }
+    e = enqueue(reinterpret_cast<const float2*>(d_kspace), reinterpret_cast<float2*>(d_out),
+                static_cast<const uint8_t*>(slot->dev), scratch);
     cudaFreeAsync(scratch, ctx->stream);
     stage_release(ctx, slot);
     if (e != cudaSuccess) return cuda_err(ctx, e, "fista2d launch");
@@ -514,8 +616,9 @@ int oks_fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t*
         fa.xout = out; fa.out_stride = (long long)ny * nx;
         fa.ny = ny; fa.nx = nx; fa.iters = iters; fa.lambda = lambda; fa.alpha = alpha;
         fa.nprob = nprob;
-        fa.variant = ctx->col_variant;
-        const bool use_reg = ctx->col_engine != 1 && oks::fista_col_reg_supported(ny);
+        const TuneParams tp = tune_params(ctx, 0, ny, nx);
+        fa.variant = tp.col_variant;
+        const bool use_reg = tp.col_engine != 1 && oks::fista_col_reg_supported(ny);
         if (use_reg) e = oks::reg_tables_init(&ctx->reg_tables);
         if (e == cudaSuccess && use_reg) {
             ProfScope ps(ctx, "k_fista_col_reg");

@@ -47,7 +47,7 @@ extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs,
                 if ((m[x] != 0) != on) { sep = false; break; }
             if (on) words[(size_t)i * wstride + (y >> 5)] |= 1u << (y & 31);
         }
-        batched[i] = sep && oks::fista_col_reg_supported(r.ny) && ctx->col_engine != 1;
+        batched[i] = sep && oks::fista_col_reg_supported(r.ny) && tune_params(ctx, 0, r.ny, 0).col_engine != 1;
     }
     void* scratch = nullptr;
     if (scratch_elems) OKS_CUDA(cudaMallocAsync(&scratch, sizeof(float2) * scratch_elems, ctx->stream));
@@ -139,7 +139,7 @@ extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs,
             fa.probs = static_cast<const oks::ColProblem*>(tslot->dev) + spans[k].first;
             fa.nprob = (long long)(spans[k].second - spans[k].first);
             fa.nunits = nunits[k];
-            fa.variant = ctx->col_variant;
+            fa.variant = tune_params(ctx, 0, g.first, 0).col_variant;
             fa.nx = 2;   // unused in the batched form; keeps the launch guard open
             {
                 ProfScope ps(ctx, "k_fista_col_reg", s);

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -17,6 +18,18 @@
 #include "plan.h"
 
 using oks::DevPlan;
+
+// Plan and launch-shape choices of the FISTA engines for one shape (set by
+// okscuda_set_option globally, or per shape by okscuda_autotune).
+struct TuneParams {
+    int col_engine;
+    int col_variant;
+    int persist2d;
+    int occ2d;
+    int prefetch2d;
+    int fista2d_streams;
+    long long fista2d_chunk;
+};
 
 struct okscuda_ctx {
     int device = 0;
@@ -37,6 +50,25 @@ struct okscuda_ctx {
     int occ2d = 1;                        // 2-D register passes: 1 = launch bounds for 12 warps per SM
     int fista2d_streams = 2;              // 2-D engine: chunks in flight at once (forked streams)
     int prefetch2d = 1;                   // 2-D register column pass: pipelined loads (separable masks)
+    // per-shape choices found by okscuda_autotune: key (kind, ny, nx), kind 0
+    // = ky-only masks (column engine, nx = 0), kind 1 = 2-D masks
+    std::map<std::tuple<int, int, int>, TuneParams> tuned;
+    int use_tuned = 1;
+    // 2-D engine CUDA graphs: key -> instantiated launch sequence over the
+    // entry's own buffers (k-space in, coil images out, masks, scratch)
+    struct Graph2d {
+        cudaGraphExec_t exec = nullptr;
+        void* y = nullptr;
+        void* out = nullptr;
+        void* masks = nullptr;
+        void* scratch = nullptr;
+        cudaEvent_t done = nullptr;
+        bool failed = false;
+        unsigned long long last_use = 0;
+    };
+    std::map<std::string, Graph2d> g2d;
+    unsigned long long g2d_clock = 0;
+    int graph2d = 1;                      // 2-D engine: replay captured launch sequences
     oks::RegTables reg_tables;
     // tensor-core row DFT: split B operands per (n, sign, centred, column
     // sets), device column lists, error flag
@@ -83,6 +115,29 @@ inline int cuda_err(okscuda_ctx* c, cudaError_t e, const char* where) {
         cudaError_t e0_ = cudaSetDevice(ctx->device);                    \
         if (e0_ != cudaSuccess) return cuda_err(ctx, e0_, "cudaSetDevice"); \
     } while (0)
+
+inline void free_graph2d(okscuda_ctx::Graph2d& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    cudaFree(g.y);
+    cudaFree(g.out);
+    cudaFree(g.masks);
+    cudaFree(g.scratch);
+    if (g.done) cudaEventDestroy(g.done);
+    g.exec = nullptr;
+    g.y = g.out = g.masks = g.scratch = nullptr;
+    g.done = nullptr;
+}
+
+// The choices in force for a shape: the autotuned entry when there is one
+// (and lookups are on), else the context-wide options.
+inline TuneParams tune_params(const okscuda_ctx* ctx, int kind, int ny, int nx) {
+    if (ctx->use_tuned) {
+        auto it = ctx->tuned.find(std::make_tuple(kind, ny, kind == 0 ? 0 : nx));
+        if (it != ctx->tuned.end()) return it->second;
+    }
+    return TuneParams{ctx->col_engine, ctx->col_variant, ctx->persist2d, ctx->occ2d,
+                      ctx->prefetch2d, ctx->fista2d_streams, ctx->fista2d_chunk};
+}
 
 inline int ensure_scratch(okscuda_ctx* ctx, size_t bytes) {
     if (bytes <= ctx->scratch_bytes) return OKS_OK;

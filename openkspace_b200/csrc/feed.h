@@ -20,7 +20,10 @@ struct PlaceEntry {
 
 cudaError_t launch_noise_fit(const float2* noise, int nc, long long ns, double denom, double2* partial_scratch,
                              int max_parts, float2* W, double2* W64, int* status, cudaStream_t st);
-cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st);
+// status (nullable): device result word of the noise fit; when it is not 0
+// the kernel leaves the data unchanged (no host round trip to decide)
+cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st,
+                                   const int* status = nullptr);
 cudaError_t launch_os_remove(const float2* in, float2* out, long long nlines, const DevPlan& pe, const DevPlan& pr,
                              cudaStream_t st);
 cudaError_t launch_place(const float2* src, int nc_src, int ns, const PlaceEntry* tab, long long nent, float2* kspace,

@@ -147,7 +147,10 @@ __global__ void k_chol_inv(const double2* __restrict__ partial, int nparts, int 
 // data [nacq][nc][ns]: every sample column s -> W s (lower triangular).
 template <int NCMAX>
 __global__ void k_prewhiten_apply(float2* __restrict__ data, const float2* __restrict__ Wg, long long nacq, int nc,
-                                  int ns) {
+                                  int ns, const int* __restrict__ status) {
+    // status (optional): the noise fit's result word; anything but 0 means
+    // the fit returned None (prewhiten.rs:161) and the data stay as they are
+    if (status && *status != 0) return;
     __shared__ float2 W[NCMAX * NCMAX];
     for (int q = threadIdx.x; q < nc * nc; q += blockDim.x) W[(q / nc) * NCMAX + q % nc] = Wg[q];
     __syncthreads();
@@ -171,15 +174,16 @@ __global__ void k_prewhiten_apply(float2* __restrict__ data, const float2* __res
     }
 }
 
-cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st) {
+cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st,
+                                   const int* status) {
     const long long total = nacq * ns;
     if (total <= 0 || nc <= 0) return cudaSuccess;
     long long blocks = (total + 255) / 256;
     if (blocks > 148 * 8) blocks = 148 * 8;
-    if (nc <= 8) k_prewhiten_apply<8><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns);
-    else if (nc <= 16) k_prewhiten_apply<16><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns);
-    else if (nc <= 32) k_prewhiten_apply<32><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns);
-    else if (nc <= 64) k_prewhiten_apply<64><<<(unsigned)blocks, 128, 0, st>>>(data, W, nacq, nc, ns);
+    if (nc <= 8) k_prewhiten_apply<8><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns, status);
+    else if (nc <= 16) k_prewhiten_apply<16><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns, status);
+    else if (nc <= 32) k_prewhiten_apply<32><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns, status);
+    else if (nc <= 64) k_prewhiten_apply<64><<<(unsigned)blocks, 128, 0, st>>>(data, W, nacq, nc, ns, status);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }

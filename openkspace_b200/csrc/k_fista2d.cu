@@ -257,7 +257,7 @@ cudaError_t launch_fista2d_col(const Fista2dArgs& a, const DevPlan& py, int mode
     if ((size_t)3 * tc * n * sizeof(float2) > 150 * 1024) tc = 1;
     size_t smem = sizeof(float2) * ((size_t)3 * tc * n + py.plan.tw_total + py.roots_total) +
                   sizeof(float) * (size_t)tc * n;
-    cudaError_t e = cudaFuncSetAttribute(k2d_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = set_smem_attr(reinterpret_cast<const void*>(k2d_col), smem);
     if (e != cudaSuccess) return e;
     int nthr = rup(tc * n / 4, 32);
     nthr = nthr < 64 ? 64 : (nthr > 256 ? 256 : nthr);
@@ -271,7 +271,7 @@ cudaError_t launch_fista2d_row(const Fista2dArgs& a, const DevPlan& px, int mode
     int rpc = 4;
     if ((size_t)2 * rpc * n * sizeof(float2) > 150 * 1024) rpc = 2;
     size_t smem = sizeof(float2) * ((size_t)2 * rpc * n + px.plan.tw_total + px.roots_total);
-    cudaError_t e = cudaFuncSetAttribute(k2d_row, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = set_smem_attr(reinterpret_cast<const void*>(k2d_row), smem);
     if (e != cudaSuccess) return e;
     int nthr = rup(rpc * n / 4, 32);
     nthr = nthr < 64 ? 64 : (nthr > 256 ? 256 : nthr);

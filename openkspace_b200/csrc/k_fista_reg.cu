@@ -933,8 +933,8 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
     if (pf && MINB > 1 && (base_smem + pf_smem + 1024) * MINB > 220u * 1024u) pf = 0;
     b.prefetch = pf;
     const size_t smem = base_smem + (pf ? pf_smem : 0);
-    if (row) e = cudaFuncSetAttribute(k2d_row_reg<P, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    else e = cudaFuncSetAttribute(k2d_col_reg<P, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (row) e = set_smem_attr(reinterpret_cast<const void*>(k2d_row_reg<P, MINB>), smem);
+    else e = set_smem_attr(reinterpret_cast<const void*>(k2d_col_reg<P, MINB>), smem);
     if (e != cudaSuccess) return e;
     long long grid = (units + G - 1) / G;
     // persistent form: every resident CTA slot once, units grid-strided
@@ -1007,7 +1007,7 @@ static cudaError_t launch_p(const FistaColArgs& a, cudaStream_t st) {
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
     const size_t smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X);
-    e = cudaFuncSetAttribute(k_fista_col_reg<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = set_smem_attr(reinterpret_cast<const void*>(k_fista_col_reg<P>), smem);
     if (e != cudaSuccess) return e;
     const long long units = a.probs ? a.nunits : a.nprob * (long long)(a.nx / 2);
     const long long grid = (units + G - 1) / G;

@@ -3,11 +3,31 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "fft_dev.cuh"
 
 namespace oks {
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per (kernel, device,
+// size) instead of before every launch: the 2-D engine issues thousands of
+// launches per call, and the host's launch rate can bound it.
+inline cudaError_t set_smem_attr(const void* fn, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& v = done[{fn, dev}];
+    if (v >= smem) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) v = smem;
+    return e;
+}
 
 // Device copy of one FFT length's plan: the FftPlan (by value) plus its
 // twiddle and root tables in global memory.

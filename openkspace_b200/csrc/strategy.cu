@@ -45,12 +45,11 @@ struct DevBuf {
 
 }  // namespace
 
-extern "C" {
-
-// ------------------------------------------------------- feeding stages
-int okscuda_prewhiten_fit(okscuda_ctx* ctx, const okscuda_c64* d_noise, int nc, long long ns,
-                          long long total_samples, okscuda_c64* d_W) {
-    OKS_CHECK_CTX();
+// The noise fit's launches (FP64 covariance, Cholesky, inverse); the result
+// word (0 ok, 1 / 2 not positive definite) is left in d_status on the device.
+// Errors the host can decide (sizes) are returned here.
+static int prewhiten_fit_launch(okscuda_ctx* ctx, const okscuda_c64* d_noise, int nc, long long ns,
+                                long long total_samples, okscuda_c64* d_W, int* d_status) {
     if (!d_W || nc <= 0 || ns < 0) return set_err(ctx, OKS_EINVAL, "prewhiten_fit: bad arguments");
     if (nc > 128) return set_err(ctx, OKS_ENOTSUP, "prewhiten_fit: nc=%d above 128", nc);
     const long long total = total_samples > 0 ? total_samples : ns;
@@ -59,17 +58,26 @@ int okscuda_prewhiten_fit(okscuda_ctx* ctx, const okscuda_c64* d_noise, int nc, 
     if (ns > 0 && !d_noise) return set_err(ctx, OKS_EINVAL, "prewhiten_fit: null noise");
     const int max_parts = 148 * 4;
     const size_t npair = (size_t)nc * (nc + 1) / 2;
-    DevBuf part(ctx), st(ctx);
+    DevBuf part(ctx);   // released stream-ordered, after the kernels that use it
     OKS_CUDA(part.alloc(sizeof(double2) * npair * max_parts));
-    OKS_CUDA(st.alloc(sizeof(int)));
     // prewhiten.rs:98: denominator (total - 1).max(1)
     const double denom = std::max((double)total - 1.0, 1.0);
-    {
-        ProfScope ps(ctx, "k_noise_fit");
-        OKS_CUDA(oks::launch_noise_fit(reinterpret_cast<const float2*>(d_noise), nc, ns, denom,
-                                       part.as<double2>(), max_parts, reinterpret_cast<float2*>(d_W), nullptr,
-                                       st.as<int>(), ctx->stream));
-    }
+    ProfScope ps(ctx, "k_noise_fit");
+    OKS_CUDA(oks::launch_noise_fit(reinterpret_cast<const float2*>(d_noise), nc, ns, denom, part.as<double2>(),
+                                   max_parts, reinterpret_cast<float2*>(d_W), nullptr, d_status, ctx->stream));
+    return OKS_OK;
+}
+
+extern "C" {
+
+// ------------------------------------------------------- feeding stages
+int okscuda_prewhiten_fit(okscuda_ctx* ctx, const okscuda_c64* d_noise, int nc, long long ns,
+                          long long total_samples, okscuda_c64* d_W) {
+    OKS_CHECK_CTX();
+    DevBuf st(ctx);
+    OKS_CUDA(st.alloc(sizeof(int)));
+    int rc = prewhiten_fit_launch(ctx, d_noise, nc, ns, total_samples, d_W, st.as<int>());
+    if (rc) return rc;
     int status = -1;
     OKS_CUDA(cudaMemcpyAsync(&status, st.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     OKS_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -191,7 +199,7 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
     // --- 1. calibration: noise scans -> W (strategy.rs:783-798) -------------
     bool have_w = false;
     int w_nc = 0;
-    DevBuf dW(ctx);
+    DevBuf dW(ctx), dWstat(ctx);
     if (cfg->prewhiten) {
         std::vector<long long> noise;
         for (long long a = 0; a < nacq; ++a)
@@ -217,10 +225,13 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
                     col += ns;
                 }
                 OKS_CUDA(dW.alloc(sizeof(float2) * (size_t)nc * nc));
-                int rc = okscuda_prewhiten_fit(ctx, reinterpret_cast<const okscuda_c64*>(dn.p), nc, match, total,
-                                               dW.as<okscuda_c64>());
+                OKS_CUDA(dWstat.alloc(sizeof(int)));
+                // no host round trip: a fit that fails (None, prewhiten.rs:161)
+                // leaves its status word set and the apply kernel skips
+                int rc = prewhiten_fit_launch(ctx, reinterpret_cast<const okscuda_c64*>(dn.p), nc, match, total,
+                                              dW.as<okscuda_c64>(), dWstat.as<int>());
                 if (rc == OKS_OK) { have_w = true; w_nc = nc; }
-                else if (rc != OKS_ENOTPD && rc != OKS_ESKIP) return rc;   // None -> skip prewhitening
+                else if (rc != OKS_ESKIP) return rc;
             }
         }
     }
@@ -294,8 +305,10 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
         }
         // preprocess: W s (prewhiten.rs:118-124 skips other channel counts), then OS removal
         if (have_w && gnc == w_nc) {
-            int rc = okscuda_prewhiten_apply(ctx, dW.as<okscuda_c64>(), raw.as<okscuda_c64>(), ng, gnc, gns);
-            if (rc) return rc;
+            if (gnc > 64) return set_err(ctx, OKS_ENOTSUP, "prewhiten_apply: nc=%d above 64", gnc);
+            ProfScope ps(ctx, "k_prewhiten_apply");
+            OKS_CUDA(oks::launch_prewhiten_apply(raw.as<float2>(), dW.as<float2>(), ng, gnc, gns, ctx->stream,
+                                                 dWstat.as<int>()));
         }
         int pns = gns;
         DevBuf os(ctx);

@@ -267,6 +267,24 @@ class Context:
     def set_option(self, name: str, value: int):
         self.check(self.lib.okscuda_set_option(self.handle, name.encode(), int(value)))
 
+    def autotune(self, kind: int, ny: int, nx: int, nc: int = 8, iters: int = 20) -> dict:
+        """Times the engine's plan/launch-shape candidates for one shape and
+        keeps the fastest (kind 0: ky-only masks, 1: 2-D masks); returns the
+        report (every candidate's time and the choice)."""
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self.check(self.lib.okscuda_autotune(self.handle, int(kind), int(ny), int(nx), int(nc), int(iters), buf,
+                                             len(buf)))
+        return json.loads(buf.value.decode())
+
+    def autotune_table(self) -> str:
+        buf = ctypes.create_string_buffer(1 << 16)
+        self.check(self.lib.okscuda_autotune_table(self.handle, buf, len(buf)))
+        return buf.value.decode()
+
+    def autotune_load(self, text: str):
+        self.check(self.lib.okscuda_autotune_load(self.handle, text.encode()))
+
     # -- profiling ----------------------------------------------------------
     def profile(self, on: bool = True):
         self.check(self.lib.okscuda_profile_enable(self.handle, int(on)))
