@@ -297,7 +297,7 @@ def serving_measure(ctx, rates, seconds, max_requests):
     pool = synth.uneven_requests(n=32, workload=3)
     pinned = [torch.from_numpy(r.kspace.view(np.float32)).pin_memory().numpy().view(np.complex64) for r in pool]
     masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in pool]
-    for k, m, r in zip(pinned[:4], masks[:4], pool[:4]):       # warm-up: plans, tables, pools
+    for k, m, r in zip(pinned, masks, pool):                 # warm-up: every size, iteration count (plans, tables)
         ctx.cs_slice(k, m, r.iters, r.lam)
     # plain per-slice drop-in
     lat = []

@@ -137,6 +137,70 @@ struct Tw {
     static constexpr int total() { return inv(P::S); }
 };
 
+// cos and sin of 2 pi m / R for compile-time m and R (Taylor series of the
+// angle reduced to [-pi, pi], 30 terms: below double rounding there), so the
+// odd-radix butterflies below multiply by immediates instead of loading a
+// table of roots.
+constexpr double cx_sin(double x) {
+    double term = x, sum = x;
+    for (int n = 1; n < 30; ++n) {
+        term *= -x * x / ((2.0 * n) * (2.0 * n + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+constexpr double cx_cos(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int n = 1; n < 30; ++n) {
+        term *= -x * x / ((2.0 * n - 1.0) * (2.0 * n));
+        sum += term;
+    }
+    return sum;
+}
+template <int R, int M>
+struct RootRM {
+    static constexpr double ang = 6.283185307179586476925286766559 * (double)(2 * M <= R ? M : M - R) / (double)R;
+    static constexpr float c = (float)cx_cos(ang);
+    static constexpr float s = (float)cx_sin(ang);
+};
+
+// re += sum_j a_j cos(2 pi j Q / R), im += sum_j b_j sin(2 pi j Q / R), j = J..H
+template <int R, int Q, int J>
+__device__ __forceinline__ void odd_acc(const float2* a, const float2* b, float2& re, float2& im) {
+    if constexpr (J <= (R - 1) / 2) {
+        constexpr int M = (J * Q) % R;
+        re.x = fmaf(a[J - 1].x, RootRM<R, M>::c, re.x);
+        re.y = fmaf(a[J - 1].y, RootRM<R, M>::c, re.y);
+        im.x = fmaf(b[J - 1].x, RootRM<R, M>::s, im.x);
+        im.y = fmaf(b[J - 1].y, RootRM<R, M>::s, im.y);
+        odd_acc<R, Q, J + 1>(a, b, re, im);
+    }
+}
+
+// Output pairs Q, Q + NS, ... of an odd-radix butterfly in symmetric form.
+template <int SIGN, int R, int NS, int Q>
+__device__ __forceinline__ void odd_pairs(const float2* a, const float2* b, float2 x0, float2* dst, int ob, int p,
+                                          int c) {
+    if constexpr (Q <= (R - 1) / 2) {
+        float2 re = x0, im = make_float2(0.f, 0.f);
+        odd_acc<R, Q, 1>(a, b, re, im);
+        const float2 si = mul_si<SIGN>(im);
+        dst[padi(2 * (ob + Q * p) + c)] = re + si;
+        dst[padi(2 * (ob + (R - Q) * p) + c)] = re - si;
+        odd_pairs<SIGN, R, NS, Q + NS>(a, b, x0, dst, ob, p, c);
+    }
+}
+
+// Thread s of a butterfly's NS threads forms the pairs q = s+1, s+1+NS, ...
+template <int SIGN, int R, int NS, int S0>
+__device__ __forceinline__ void odd_pairs_for(int s, const float2* a, const float2* b, float2 x0, float2* dst, int ob,
+                                              int p, int c) {
+    if constexpr (S0 < NS) {
+        if (s == S0) odd_pairs<SIGN, R, NS, S0 + 1>(a, b, x0, dst, ob, p, c);
+        else odd_pairs_for<SIGN, R, NS, S0 + 1>(s, a, b, x0, dst, ob, p, c);
+    }
+}
+
 // One stage over smem for intermediate stages: items f = t + TA*b, both
 // columns, any radix.  src/dst are padded exchange buffers.
 template <class P, int SIGN, int R, int p>
@@ -174,21 +238,9 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
             y0 = y0 + a[j - 1];
         }
         if (s == 0) dst[padi(2 * ob + c)] = y0;
-        for (int q = s + 1; q <= H; q += NS) {
-            float2 re = x0, im = make_float2(0.f, 0.f);
-            int m = 0;                                   // j q mod R
-#pragma unroll
-            for (int j = 1; j <= H; ++j) {
-                m += q;
-                if (m >= R) m -= R;
-                const float2 w = roots[m];
-                re.x += a[j - 1].x * w.x; re.y += a[j - 1].y * w.x;
-                im.x += b[j - 1].x * w.y; im.y += b[j - 1].y * w.y;
-            }
-            const float2 si = mul_si<SIGN>(im);
-            dst[padi(2 * (ob + q * p) + c)] = re + si;
-            dst[padi(2 * (ob + (R - q) * p) + c)] = re - si;
-        }
+        // output pairs with compile-time q: the roots are immediates
+        odd_pairs_for<SIGN, R, NS, 0>(s, a, b, x0, dst, ob, p, c);
+        (void)roots;
         return;
     }
     if (P::TA != P::T && t >= P::TA) return;   // padding lanes own no element
