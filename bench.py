@@ -1,14 +1,21 @@
 """FISTA-CS benchmark (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload plain|volume|precision]
+                    [--workload precision|plain|volume|batched|served] [--row-engine simt|tc]
 
 A step is one pass of the hot path over one batch of synthetic input:
-  plain      one 8-coil 256 x 256 slice (R = 4 + 24 centre lines, 50 iterations,
-             lambda 0.01) through okscuda_cs_slice
-  volume     the same slice size, 36 slices per step in one batched launch
+  precision  (default) 36 slices x 15 coils, 640 (2x oversampled) x 368, R = 4 with an
+             8 % centre, correlated noise, 120 iterations, lambda 0.005: the whole
+             CsRss pipeline (noise fit, prewhitening, oversampling removal,
+             placement, FISTA on the 368 x 640 grid, RSS, crop); the line also
+             carries a short run with the other readout engine and a served-vs-plain
+             measurement
+  plain      one 8-coil 256 x 256 slice (R = 4 + 24 centre lines, 50 iterations)
+  volume     36 slices of the plain size in one batched launch
+  batched    64 slices of uneven size, coils, R and iterations in one okscuda_cs_batch
+  served     Poisson arrivals through the request server beside the plain drop-in
 value = slices/s with inputs resident in HBM; e2e = the same through the
-public API with pinned host buffers copied in and the RSS copied out inside
+public API with pinned host buffers copied in and the result copied out inside
 the timed region.  Multi-GPU: one process per GPU, every rank solves its own
 slices (no data-path collective; weak scaling).  ``--impl reference`` times
 the CPU restatement of the reference (oracle/cs_ref.c; the Rust reference
