@@ -16,6 +16,20 @@ int okscuda_create(int device, okscuda_ctx** out) {
     if (device < 0 || device >= ndev) return OKS_EINVAL;
     e = cudaSetDevice(device);
     if (e != cudaSuccess) return OKS_ECUDA;
+    // The engines take their scratch stream-ordered (cudaMallocAsync).  With
+    // the pool's default release threshold of 0, every host synchronisation
+    // returns that memory to the driver and the next call maps it again
+    // (hundreds of ms for the GB-sized scratch of a volume); keep up to
+    // 16 GiB cached in the device's default pool instead.
+    {
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess && pool) {
+            uint64_t keep = 16ull << 30, cur = 0;
+            if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur < keep)
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        (void)cudaGetLastError();
+    }
     auto* c = new okscuda_ctx();
     c->device = device;
     e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
