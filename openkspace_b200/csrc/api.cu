@@ -70,7 +70,7 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "col_engine: 0 auto, 1 generic, 2 register");
         ctx->col_engine = (int)value;
     } else if (!std::strcmp(name, "col_variant")) {
-        if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "col_variant: 0 or 1");
+        if (value < -1 || value > 1) return set_err(ctx, OKS_EINVAL, "col_variant: -1 (per length), 0 or 1");
         ctx->col_variant = (int)value;
     } else if (!std::strcmp(name, "persist2d")) {
         ctx->persist2d = value != 0;

@@ -62,8 +62,8 @@ extern "C" int okscuda_autotune(okscuda_ctx* ctx, int kind, int ny, int nx, int 
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { cudaFreeAsync(d, ctx->stream); return cuda_err(ctx, e, "autotune data"); }
 
-    const TuneParams base{ctx->col_engine, ctx->col_variant, ctx->persist2d, ctx->occ2d,
-                          ctx->prefetch2d, ctx->fista2d_streams, ctx->fista2d_chunk};
+    TuneParams base{ctx->col_engine, ctx->col_variant < 0 ? 0 : ctx->col_variant, ctx->persist2d, ctx->occ2d,
+                    ctx->prefetch2d, ctx->fista2d_streams, ctx->fista2d_chunk};
     std::vector<TuneParams> cands;
     if (kind == 0) {
         TuneParams p = base;

@@ -44,7 +44,7 @@ struct okscuda_ctx {
     oks::Staging staging;
     long long fista2d_chunk = 0;          // problems per 2-D-mask chunk (0 = auto)
     int col_engine = 0;                   // ky-only masks: 0 auto, 1 generic smem, 2 register-resident
-    int col_variant = 0;                  // register column engine plan variant
+    int col_variant = -1;                 // register column engine plan variant (-1: per-length default)
     int persist2d = 1;                    // 2-D register passes: persistent grid
     int mask_bits = 1;                    // 2-D passes: separable masks read as row/column bits
     int occ2d = 1;                        // 2-D register passes: 1 = launch bounds for 12 warps per SM
@@ -135,7 +135,10 @@ inline TuneParams tune_params(const okscuda_ctx* ctx, int kind, int ny, int nx) 
         auto it = ctx->tuned.find(std::make_tuple(kind, ny, kind == 0 ? 0 : nx));
         if (it != ctx->tuned.end()) return it->second;
     }
-    return TuneParams{ctx->col_engine, ctx->col_variant, ctx->persist2d, ctx->occ2d,
+    // built-in plan variants, from okscuda_autotune runs on B200: the E = 8
+    // alternative plan is faster for column lengths 256, 384 and 512
+    const int variant = ctx->col_variant >= 0 ? ctx->col_variant : (ny == 256 || ny == 384 || ny == 512) ? 1 : 0;
+    return TuneParams{ctx->col_engine, variant, ctx->persist2d, ctx->occ2d,
                       ctx->prefetch2d, ctx->fista2d_streams, ctx->fista2d_chunk};
 }
 
