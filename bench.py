@@ -284,8 +284,79 @@ class BatchedWorkload:
         return dt, self.units * sample / work, f"{ncoil} coils of the lightest slice, scaled by coil-iteration-pixels"
 
 
+class Volume3dWorkload:
+    """32 coils, 256 x 256 x 192 (kz) 3-D Cartesian, ky-only R = 6 with 24
+    centre lines (every kz partition), 80 iterations, lambda 0.01: the CsRss
+    3-D path -- placement, centred IFFT along kz, then 192 x 32 per-slice
+    FISTA solves through the column engine, RSS, crop."""
+    name = "volume3d"
+    dominant = ("k_fista_col_reg", "k_fista_col")
+    bytes_model = "state model: 40 B per pixel per coil per iteration (read z, x, y; write x', z')"
+
+    def __init__(self, nz: int = 192, nc: int = 32, iters: int = 80):
+        from openkspace_b200 import synth
+        from openkspace_b200.strategy import CsRss, cartesian3d_acquisitions
+        self.k, self.mask_rows = synth.volume_3d(nc=nc, nz=nz)
+        self.acqs = cartesian3d_acquisitions(self.k, self.mask_rows)
+        self.strategy = CsRss(iters=iters, lambda_=0.01)
+        self.nc, self.nz, self.ny, self.nx = self.k.shape
+        self.iters = iters
+        self.units = nz
+
+    def config(self):
+        return {"workload": f"cartesian3d_{self.nc}c_{self.ny}x{self.nx}x{self.nz}_R6_I{self.iters}",
+                "coils": self.nc, "slices_per_step": self.nz, "ny": self.ny, "nx": self.nx, "nz": self.nz,
+                "iters": self.iters, "lambda": 0.01, "mask": "ky-only R=6 + 24 centre lines, all kz",
+                "pipeline": "CsRss 3-D (strategy.rs:782-891: kz IFFT fft.rs:52-84, per-slice FISTA, RSS)"}
+
+    def input_bytes(self):
+        return self.acqs.data.nbytes
+
+    def dominant_bytes_per_step(self):
+        return 40.0 * self.ny * self.nx * self.nc * self.nz * self.iters
+
+    def prepare(self, ctx):
+        import torch
+        self.ctx = ctx
+        self.d_data = ctx.to_device(self.acqs.data)
+        self.shape = self.strategy.output_shape(ctx, self.acqs)
+        self.d_out = ctx.empty(self.shape, np.float32)
+        pinned = torch.from_numpy(self.acqs.data.view(np.float32)).pin_memory()
+        self._pinned = pinned
+        self.acqs.data = pinned.numpy().view(np.complex64)
+        self.h_out = torch.empty(self.shape, dtype=torch.float32).pin_memory().numpy()
+        self.k_cpu = np.ascontiguousarray(self.k[:2])   # the one-core CPU sample needs two coils
+        del self.k   # the acquisition set holds the samples from here on
+
+    def step_device(self):
+        self.strategy.reconstruct(self.ctx, self.acqs, device_data=self.d_data, out=self.d_out)
+
+    def step_e2e(self):
+        self.strategy.reconstruct(self.ctx, self.acqs, out=self.h_out)
+
+    def e2e_bytes(self):
+        return self.acqs.data.nbytes, int(np.prod(self.shape)) * 4
+
+    def cpu_sample(self, nthreads):
+        """The FP32 C restatement on one kz-decoupled slice: `ncoil` coils of
+        the placed k-space, centred IFFT along kz, FISTA + RSS (scaled to 32)."""
+        from oracle import csref
+        k = getattr(self, "k", None)
+        if k is None:
+            k = self.k_cpu
+        m = self.mask_rows
+        ncoil = max(1, min(k.shape[0], nthreads if nthreads > 1 else 2))
+        t = time.perf_counter()
+        kz = csref.ifft1_axis(k[:ncoil], 1)[:, :1]                           # [ncoil, 1, ny, nx]
+        mask = np.repeat(m[:, None], self.nx, 1)[None]
+        csref.csrss(np.ascontiguousarray(kz), mask, self.iters, 0.01, nthreads=nthreads)
+        dt = time.perf_counter() - t
+        return dt, ncoil / self.nc, f"1 slice: kz IFFT of {ncoil} of {self.nc} coils + FISTA + RSS (scaled)"
+
+
 WORKLOADS = {"plain": lambda: PlainWorkload(1), "volume": lambda: PlainWorkload(36),
              "precision": lambda: PrecisionWorkload(36), "batched": lambda: BatchedWorkload(64),
+             "volume3d": lambda: Volume3dWorkload(),
              # reduced sizes of the same kernels, for profiler captures only
              "precision_small": lambda: PrecisionWorkload(2, 4), "batched_small": lambda: BatchedWorkload(6)}
 

@@ -91,6 +91,20 @@ def oversampled_acquisitions(vol) -> AcquisitionSet:
     return AcquisitionSet.build(acqs, (ex, vol.ny, 1), (vol.rec_x, vol.ny, 1), vol.ny // 2)
 
 
+def cartesian3d_acquisitions(kspace: np.ndarray, mask_rows: np.ndarray) -> AcquisitionSet:
+    """An AcquisitionSet of 3-D Cartesian k-space [nc, nz, ny, nx]: every
+    sampled ky line of every kz partition (``kspace_encode_step_2`` = kz), no
+    noise scan, no readout oversampling."""
+    nc, nz, ny, nx = kspace.shape
+    rows = np.flatnonzero(mask_rows)
+    acqs = []
+    for z in range(nz):
+        for r in rows:
+            acqs.append(({"kspace_encode_step_1": int(r), "kspace_encode_step_2": z, "center_sample": nx // 2},
+                         kspace[:, z, r, :]))
+    return AcquisitionSet.build(acqs, (nx, ny, nz), (nx, ny, nz), ny // 2, nz // 2)
+
+
 @dataclasses.dataclass
 class ImageVolume:
     """strategy.rs:26-34."""
