@@ -13,6 +13,8 @@ A step is one pass of the hot path over one batch of synthetic input:
   plain      one 8-coil 256 x 256 slice (R = 4 + 24 centre lines, 50 iterations)
   volume     36 slices of the plain size in one batched launch
   batched    64 slices of uneven size, coils, R and iterations in one okscuda_cs_batch
+  volume3d   32 coils, 256 x 256 x 192 3-D Cartesian, R = 6, 80 iterations: the
+             CsRss 3-D path (kz IFFT, 192 x 32 slice solves, RSS)
   served     Poisson arrivals through the request server beside the plain drop-in
 value = slices/s with inputs resident in HBM; e2e = the same through the
 public API with pinned host buffers copied in and the result copied out inside
