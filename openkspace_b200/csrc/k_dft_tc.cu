@@ -11,15 +11,18 @@
 // is accumulated in FP32 in tensor memory (the lo*lo term is below the FP32
 // rounding of the sum).
 //
-// Kernel (one CTA per 128 x 256 output tile, 128 threads):
+// Kernel (persistent, one CTA per SM looping over 128 x 256 output tiles,
+// 192 threads):
 //   * warp 0 lane 0: TMA producer.  A (X_hi, X_lo) and B (B_hi, B_lo) tiles
 //     of 64 bf16 along K (128 B = one 128-byte swizzle row) go to a 2-stage
 //     shared-memory ring, completion on an mbarrier per stage;
 //   * warp 1 lane 0: MMA issuer.  tcgen05.mma kind::f16 (bf16 in, f32
 //     accumulate), M = 128, N = 256, K = 16 per instruction, 3 products per
-//     K step; tcgen05.commit frees the stage and finally signals the epilogue;
-//   * all four warps: epilogue.  tcgen05.ld of the warp's 32 TMEM lanes
-//     (= output rows), scale, store.
+//     K step, into one of two accumulators in tensor memory (all 512
+//     columns); tcgen05.commit frees each stage and signals a finished tile;
+//   * warps 2-5: epilogue.  tcgen05.ld of the warp's 32 TMEM lanes (= output
+//     rows), scale, store, then hand the accumulator back -- so a tile's
+//     epilogue overlaps the next tile's MMAs.
 // Every wait is bounded (about two seconds); on time-out the kernel records
 // an error in *err, lets what it issued drain, frees its tensor memory and
 // returns (okscuda_tc_status reads and clears the flag).
@@ -45,6 +48,8 @@ constexpr int A_BYTES = BM * BK * 2;                    // 16 KB
 constexpr int B_BYTES = BN * BK * 2;                    // 32 KB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
 constexpr int SMEM_BYTES = NST * STAGE_BYTES + 1024 + 128;
+constexpr int kThreads = 192;                          // producer warp, MMA warp, 4 epilogue warps
+constexpr int kEpiThreads = 128;
 constexpr long long kWaitCycles = 4000000000ll;         // ~2 s at 1.9 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -147,23 +152,37 @@ struct Epilogue {
     int mask_mod;
 };
 
-__global__ void __launch_bounds__(128, 1)
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Persistent: CTA b takes tiles b, b + grid, ...; tile t = (m_tile, n_tile) =
+// (t / n_tiles, t % n_tiles).  Two accumulators in tensor memory (2 x BN
+// columns, all 512): the epilogue of one tile overlaps the MMAs of the next.
+__global__ void __launch_bounds__(kThreads, 1)
 k_dft_tc(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
          const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo, int nk,
-         Epilogue ep, int* err) {
+         int m_tiles, int n_tiles, Epilogue ep, int* err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte aligned tile area (the 128-byte swizzle repeats every 1024 B)
     uint8_t* tiles = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(tiles + NST * STAGE_BYTES);   // full[NST], empty[NST], done
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * NST + 1);
+    // full[NST], empty[NST], tfull[2], tempty[2], done
+    uint64_t* bars = reinterpret_cast<uint64_t*>(tiles + NST * STAGE_BYTES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * NST + 5);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n_tile = blockIdx.x, m_tile = blockIdx.y;
-    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + NST), done = smem_u32(bars + 2 * NST);
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + NST);
+    const uint32_t tfull0 = smem_u32(bars + 2 * NST), tempty0 = smem_u32(bars + 2 * NST + 2);
+    const uint32_t done = smem_u32(bars + 2 * NST + 4);
+    const int ntiles = m_tiles * n_tiles;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < NST; ++s) {
             mbar_init(full0 + 8 * s, 1);
             mbar_init(empty0 + 8 * s, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(tfull0 + 8 * b, 1);
+            mbar_init(tempty0 + 8 * b, kEpiThreads);
         }
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -171,7 +190,7 @@ k_dft_tc(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CU
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"((uint32_t)BN));
+                     "r"((uint32_t)(2 * BN)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -180,81 +199,113 @@ k_dft_tc(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CU
     const uint32_t tmem = *tmem_slot;
 
     if (threadIdx.x == 0) {
-        // ---- TMA producer
-        int issued = 0;
-        for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % NST;
-            if (kb >= NST && !mbar_wait(empty0 + 8 * s, ((kb / NST) & 1) ^ 1, err, 1)) break;
-            uint8_t* st = tiles + s * STAGE_BYTES;
-            const uint32_t fb = full0 + 8 * s;
-            mbar_expect_tx(fb, STAGE_BYTES);
-            tma_load_2d(smem_u32(st), &map_ahi, fb, kb * BK, m_tile * BM);
-            tma_load_2d(smem_u32(st + A_BYTES), &map_alo, fb, kb * BK, m_tile * BM);
-            tma_load_2d(smem_u32(st + 2 * A_BYTES), &map_bhi, fb, kb * BK, n_tile * BN);
-            tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &map_blo, fb, kb * BK, n_tile * BN);
-            issued = kb + 1;
+        // ---- TMA producer: the K blocks of every tile through the ring
+        long long g = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            const int m_tile = t / n_tiles, n_tile = t - m_tile * n_tiles;
+            for (int kb = 0; kb < nk; ++kb, ++g) {
+                const int s = (int)(g % NST);
+                if (g >= NST && !mbar_wait(empty0 + 8 * s, (uint32_t)((g / NST) & 1) ^ 1u, err, 1)) {
+                    ok = false;
+                    break;
+                }
+                uint8_t* st = tiles + s * STAGE_BYTES;
+                const uint32_t fb = full0 + 8 * s;
+                mbar_expect_tx(fb, STAGE_BYTES);
+                tma_load_2d(smem_u32(st), &map_ahi, fb, kb * BK, m_tile * BM);
+                tma_load_2d(smem_u32(st + A_BYTES), &map_alo, fb, kb * BK, m_tile * BM);
+                tma_load_2d(smem_u32(st + 2 * A_BYTES), &map_bhi, fb, kb * BK, n_tile * BN);
+                tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &map_blo, fb, kb * BK, n_tile * BN);
+            }
         }
         // copies still in flight complete before the CTA may exit
-        for (int kb = issued - NST < 0 ? 0 : issued - NST; kb < issued; ++kb)
-            mbar_wait(full0 + 8 * (kb % NST), (kb / NST) & 1, err, 2);
+        for (long long q = g - NST < 0 ? 0 : g - NST; q < g; ++q)
+            mbar_wait(full0 + 8 * (int)(q % NST), (uint32_t)((q / NST) & 1), err, 2);
     } else if (threadIdx.x == 32) {
         // ---- MMA issuer
-        for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % NST;
-            if (!mbar_wait(full0 + 8 * s, (kb / NST) & 1, err, 3)) break;
+        long long g = 0;
+        int li = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++li) {
+            const int ab = li & 1;
+            // the epilogue has drained this accumulator (two tiles ago)
+            if (li >= 2 && !mbar_wait(tempty0 + 8 * ab, (uint32_t)((li >> 1) & 1) ^ 1u, err, 3)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a_hi = smem_u32(tiles + s * STAGE_BYTES);
-            const uint32_t a_lo = a_hi + A_BYTES, b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
+            const uint32_t acc = tmem + (uint32_t)(ab * BN);
+            for (int kb = 0; kb < nk; ++kb, ++g) {
+                const int s = (int)(g % NST);
+                if (!mbar_wait(full0 + 8 * s, (uint32_t)((g / NST) & 1), err, 4)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_hi = smem_u32(tiles + s * STAGE_BYTES);
+                const uint32_t a_lo = a_hi + A_BYTES, b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
 #pragma unroll
-            for (int kk = 0; kk < BK / 16; ++kk) {
-                const uint32_t o = kk * 32;   // 16 bf16 along K inside the 128-byte row
-                mma_bf16(tmem, sw128_desc(a_hi + o), sw128_desc(b_hi + o), (kb | kk) != 0);
-                mma_bf16(tmem, sw128_desc(a_hi + o), sw128_desc(b_lo + o), 1u);
-                mma_bf16(tmem, sw128_desc(a_lo + o), sw128_desc(b_hi + o), 1u);
+                for (int kk = 0; kk < BK / 16; ++kk) {
+                    const uint32_t o = kk * 32;   // 16 bf16 along K inside the 128-byte row
+                    mma_bf16(acc, sw128_desc(a_hi + o), sw128_desc(b_hi + o), (kb | kk) != 0);
+                    mma_bf16(acc, sw128_desc(a_hi + o), sw128_desc(b_lo + o), 1u);
+                    mma_bf16(acc, sw128_desc(a_lo + o), sw128_desc(b_hi + o), 1u);
+                }
+                mma_commit(empty0 + 8 * s);   // the stage is free once these MMAs have read it
             }
-            mma_commit(empty0 + 8 * s);   // the stage is free once these MMAs have read it
+            if (ok) mma_commit(tfull0 + 8 * ab);   // the tile's accumulator is complete
         }
-        mma_commit(done);                 // every MMA issued above has completed
+        mma_commit(done);                          // every MMA issued above has completed
+    } else if (warp >= 2) {
+        // ---- epilogue: warp w owns TMEM lanes (= tile rows) 32 (w % 4) .. +31
+        const int q = warp & 3;
+        int li = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++li) {
+            const int ab = li & 1;
+            const int m_tile = t / n_tiles, n_tile = t - m_tile * n_tiles;
+            const bool ok = mbar_wait(tfull0 + 8 * ab, (uint32_t)((li >> 1) & 1), err, 5);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const long long row = (long long)m_tile * BM + q * 32 + lane;
+            const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * BN);
+            const uint32_t* rbits = nullptr;
+            if (ep.colbits && row < ep.M)
+                rbits = ep.colbits + ((row / ep.rows_per_prob + ep.mask_offset) % ep.mask_mod) * ep.col_wstride;
+            float* orow = ep.out + row * ep.ld;
+            for (int c = 0; c < BN; c += 16) {
+                float v[16];
+                tmem_ld16(tl + (uint32_t)c, v);
+                const int rc0 = n_tile * BN + c;   // real output column of v[0]
+                if (!ok || row >= ep.M || rc0 >= ep.ncols) continue;
+                if (!ep.cols && !rbits && rc0 + 16 <= ep.ncols && ((ep.ld | ep.col0) % 2) == 0) {
+                    float* dst = orow + 2 * ep.col0 + rc0;
+                    if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+#pragma unroll
+                        for (int i = 0; i < 16; i += 4)
+                            *reinterpret_cast<float4*>(dst + i) = make_float4(v[i] * ep.scale, v[i + 1] * ep.scale,
+                                                                             v[i + 2] * ep.scale, v[i + 3] * ep.scale);
+                        continue;
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 16; i += 2) {
+                    if (rc0 + i >= ep.ncols) break;
+                    const int j = (rc0 + i) >> 1;
+                    const int x = ep.cols ? ep.cols[j] : ep.col0 + j;
+                    const bool keep = !rbits || ((__ldg(rbits + (x >> 5)) >> (x & 31)) & 1u);
+                    *reinterpret_cast<float2*>(orow + 2 * x) =
+                        keep ? make_float2(v[i] * ep.scale, v[i + 1] * ep.scale) : make_float2(0.f, 0.f);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(tempty0 + 8 * ab);           // this accumulator may be reused
+            if (!ok) break;
+        }
     }
     __syncwarp();
-
-    // ---- epilogue: warp w owns TMEM lanes (= tile rows) 32w .. 32w+31
-    const bool ok = mbar_wait(done, 0, err, 4);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const long long row = (long long)m_tile * BM + warp * 32 + lane;
-    const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
-    const uint32_t* rbits = nullptr;
-    if (ep.colbits && row < ep.M)
-        rbits = ep.colbits + ((row / ep.rows_per_prob + ep.mask_offset) % ep.mask_mod) * ep.col_wstride;
-    float* orow = ep.out + row * ep.ld;
-    for (int c = 0; c < BN; c += 16) {
-        float v[16];
-        tmem_ld16(tl + (uint32_t)c, v);
-        const int rc0 = n_tile * BN + c;   // real output column of v[0]
-        if (!ok || row >= ep.M || rc0 >= ep.ncols) continue;
-        if (!ep.cols && !rbits && rc0 + 16 <= ep.ncols && ((ep.ld | ep.col0) % 2) == 0) {
-            float* dst = orow + 2 * ep.col0 + rc0;
-            if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
-#pragma unroll
-                for (int i = 0; i < 16; i += 4)
-                    *reinterpret_cast<float4*>(dst + i) =
-                        make_float4(v[i] * ep.scale, v[i + 1] * ep.scale, v[i + 2] * ep.scale, v[i + 3] * ep.scale);
-                continue;
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < 16; i += 2) {
-            if (rc0 + i >= ep.ncols) break;
-            const int j = (rc0 + i) >> 1;
-            const int x = ep.cols ? ep.cols[j] : ep.col0 + j;
-            const bool keep = !rbits || ((__ldg(rbits + (x >> 5)) >> (x & 31)) & 1u);
-            *reinterpret_cast<float2*>(orow + 2 * x) =
-                keep ? make_float2(v[i] * ep.scale, v[i + 1] * ep.scale) : make_float2(0.f, 0.f);
-        }
-    }
+    // every MMA has completed before the tensor memory is released
+    mbar_wait(done, 0, err, 6);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * BN)));
 }
 
 // X (complex rows, [M][ld] complex) -> hi/lo bf16 [M][kp] (real view of the
@@ -394,8 +445,17 @@ cudaError_t launch_dft_tc(const DftTcArgs& a, cudaStream_t st) {
     ep.rows_per_prob = a.rows_per_prob > 0 ? a.rows_per_prob : 1;
     ep.mask_offset = a.mask_offset;
     ep.mask_mod = a.mask_mod > 0 ? a.mask_mod : 1;
-    dim3 grid((unsigned)(np / BN), (unsigned)((a.M + BM - 1) / BM));
-    k_dft_tc<<<grid, 128, SMEM_BYTES, st>>>(m_ahi, m_alo, m_bhi, m_blo, kp / BK, ep, a.err);
+    const int n_tiles = np / BN, m_tiles = (int)((a.M + BM - 1) / BM);
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (nsm < 1) nsm = 148;
+    }
+    // persistent: one CTA per SM (its shared memory and all 512 TMEM columns)
+    const int grid = std::min(n_tiles * m_tiles, nsm);
+    k_dft_tc<<<grid, kThreads, SMEM_BYTES, st>>>(m_ahi, m_alo, m_bhi, m_blo, kp / BK, m_tiles, n_tiles, ep, a.err);
     return cudaGetLastError();
 }
 
