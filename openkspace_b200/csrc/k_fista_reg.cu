@@ -446,8 +446,17 @@ __device__ __forceinline__ float2 shrink_c(float2 c, float lam) {
     return c * ((m - lam) / m);
 }
 
+// Resident CTAs per SM the column engine is compiled for: at least 12 warps
+// (the register budget per thread follows from it), except for the E = 16
+// plans, whose 16 elements per thread would spill under that budget.
 template <class P>
-__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1))
+constexpr int col_min_blocks() {
+    constexpr int threads = P::T * (P::T == 32 ? 4 : 1);
+    return P::E >= 16 ? 1 : (12 * 32 + threads - 1) / threads;
+}
+
+template <class P>
+__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1), col_min_blocks<P>())
 k_fista_col_reg(FistaColArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
     constexpr int N = P::N, E = P::E, TA = P::TA, T = P::T;
     constexpr int G = (T == 32) ? 4 : 1;                 // groups (column pairs) per CTA
