@@ -330,7 +330,9 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
 /* No reference counterpart (the reference has no timing hooks).  When
  * enabled, every kernel launch of this context is bracketed by CUDA events
  * on the context stream; okscuda_profile_read aggregates per kernel name the
- * summed device time (ms) and the launch count.  Enabling clears the log. */
+ * summed device time (ms) and the launch count.  A replayed CUDA graph of the
+ * 2-D engine is one entry, "k2d_graph", whose count is the kernel nodes it
+ * ran.  Enabling clears the log. */
 int okscuda_profile_enable(okscuda_ctx* ctx, int on);
 int okscuda_profile_read(okscuda_ctx* ctx, char* names, int name_len, double* total_ms,
                          long long* launches, int nslots, int* nfound);

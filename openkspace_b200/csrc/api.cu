@@ -539,7 +539,21 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
                         ge = cudaStreamEndCapture(ctx->stream, &graph);
                         if (le != cudaSuccess) ge = le;
                     }
-                    if (ge == cudaSuccess) ge = cudaGraphInstantiate(&g.exec, graph, 0);
+                    if (ge == cudaSuccess) {
+                        // count the kernel nodes, so profiling reports the kernels a replay runs
+                        size_t nn = 0;
+                        if (cudaGraphGetNodes(graph, nullptr, &nn) == cudaSuccess && nn > 0) {
+                            std::vector<cudaGraphNode_t> nodes(nn);
+                            if (cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess)
+                                for (size_t q = 0; q < nn; ++q) {
+                                    cudaGraphNodeType ty;
+                                    if (cudaGraphNodeGetType(nodes[q], &ty) == cudaSuccess &&
+                                        ty == cudaGraphNodeTypeKernel)
+                                        ++g.kernels;
+                                }
+                        }
+                        ge = cudaGraphInstantiate(&g.exec, graph, 0);
+                    }
                     if (graph) cudaGraphDestroy(graph);
                     ctx->prof_on = prof;
                 }
@@ -556,7 +570,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
                 if (ge == cudaSuccess)
                     ge = cudaMemcpyAsync(g.y, d_kspace, data_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
                 if (ge == cudaSuccess) {
-                    ProfScope ps(ctx, "k2d_graph");
+                    ProfScope ps(ctx, "k2d_graph", nullptr, g.kernels > 0 ? g.kernels : 1);
                     ge = cudaGraphLaunch(g.exec, ctx->stream);
                 }
                 if (ge == cudaSuccess)
@@ -714,7 +728,7 @@ int okscuda_profile_read(okscuda_ctx* ctx, char* names, int name_len, double* to
             if (keys[k] == r.name) break;
         if (k == keys.size()) { keys.push_back(r.name); ms.push_back(0.0); cnt.push_back(0); }
         ms[k] += t;
-        cnt[k] += 1;
+        cnt[k] += r.kernels;
     }
     *nfound = (int)keys.size();
     for (int k = 0; k < (int)keys.size() && k < nslots; ++k) {

@@ -65,6 +65,7 @@ struct okscuda_ctx {
         cudaEvent_t done = nullptr;
         bool failed = false;
         unsigned long long last_use = 0;
+        long long kernels = 0;            // kernel nodes in the graph
     };
     std::map<std::string, Graph2d> g2d;
     unsigned long long g2d_clock = 0;
@@ -81,7 +82,8 @@ struct okscuda_ctx {
     cudaEvent_t fork_ev = nullptr;
     // per-launch CUDA-event profiling (okscuda_profile_*)
     bool prof_on = false;
-    struct ProfRec { const char* name; cudaEvent_t a, b; };
+    // kernels = kernel launches inside the bracket (the node count of a replayed graph)
+    struct ProfRec { const char* name; cudaEvent_t a, b; long long kernels; };
     std::vector<ProfRec> prof;
     std::vector<cudaEvent_t> ev_pool;
 };
@@ -220,14 +222,17 @@ inline cudaEvent_t prof_event(okscuda_ctx* ctx) {
     return e;
 }
 
-// Records CUDA events around one kernel launch when profiling is on.
+// Records CUDA events around one kernel launch (or one graph of `kernels`
+// kernel launches) when profiling is on.
 struct ProfScope {
     okscuda_ctx* ctx;
     cudaStream_t st;
     okscuda_ctx::ProfRec rec{};
-    ProfScope(okscuda_ctx* c, const char* name, cudaStream_t s = nullptr) : ctx(c), st(s ? s : c->stream) {
+    ProfScope(okscuda_ctx* c, const char* name, cudaStream_t s = nullptr, long long kernels = 1)
+        : ctx(c), st(s ? s : c->stream) {
         if (!ctx->prof_on) return;
         rec.name = name;
+        rec.kernels = kernels;
         rec.a = prof_event(ctx);
         rec.b = prof_event(ctx);
         cudaEventRecord(rec.a, st);
