@@ -95,6 +95,13 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
     } else if (!std::strcmp(name, "row_engine")) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "row_engine: 0 SIMT FFT, 1 tensor-core DFT");
         ctx->row_engine = (int)value;
+    } else if (!std::strcmp(name, "xform_engine")) {
+        if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "xform_engine: 0 shared-memory, 1 register");
+        ctx->xform_reg = (int)value;
+    } else if (!std::strcmp(name, "xform_tile")) {
+        if (value != 0 && value != 2 && value != 4 && value != 8)
+            return set_err(ctx, OKS_EINVAL, "xform_tile: 0 (by length), 2, 4 or 8 column pairs");
+        ctx->xform_tile = (int)value;
     } else if (!std::strcmp(name, "fista2d_streams")) {
         if (value < 1 || value > 8) return set_err(ctx, OKS_EINVAL, "fista2d_streams: 1 to 8");
         ctx->fista2d_streams = (int)value;
@@ -187,6 +194,7 @@ int okscuda_centred_fft2(okscuda_ctx* ctx, okscuda_c64* d_data, int batch, int n
     if (rc) return rc;
     float2* d = reinterpret_cast<float2*>(d_data);
     oks::RowXformArgs ra{};
+    ra.reg = ctx->xform_reg;
     ra.in = d; ra.out = d; ra.nrows = (long long)batch * ny; ra.ld_in = nx; ra.ld_out = nx;
     ra.sign = inverse ? +1 : -1; ra.centred = 1; ra.scale = 1.0f; ra.rows_per_prob = ny;
     {
@@ -194,6 +202,7 @@ int okscuda_centred_fft2(okscuda_ctx* ctx, okscuda_c64* d_data, int batch, int n
         OKS_CUDA(oks::launch_row_xform(ra, *px, ctx->stream));
     }
     oks::ColXformArgs ca{};
+    ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile;
     ca.data = d; ca.nprob = batch; ca.ny = ny; ca.nx = nx; ca.prob_stride = (long long)ny * nx;
     ca.sign = inverse ? +1 : -1; ca.centred = 1;
     ca.scale = 1.0f / std::sqrt((float)ny * (float)nx);
@@ -623,6 +632,7 @@ int oks_fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t*
     // y' = sqrt(ny) (-1)^{ny/2} (-1)^r * centred unitary row-IDFT of y
     float2* out = reinterpret_cast<float2*>(d_out);
     oks::RowXformArgs ra{};
+    ra.reg = ctx->xform_reg;
     ra.in = reinterpret_cast<const float2*>(d_kspace);
     ra.out = out;
     ra.nrows = nprob * ny;

@@ -76,6 +76,7 @@ extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs,
         const DevPlan* px;
         if ((rc = get_plan(ctx, r.nx, &px))) break;
         oks::RowXformArgs ra{};
+        ra.reg = ctx->xform_reg;
         ra.in = reinterpret_cast<const float2*>(r.d_kspace);
         ra.out = coils[i];
         ra.nrows = (long long)r.nc * r.ny;

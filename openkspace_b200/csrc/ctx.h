@@ -77,6 +77,8 @@ struct okscuda_ctx {
     std::map<std::string, TcMat> tc_mats;
     int* tc_err = nullptr;
     int row_engine = 0;                   // 2-D engine row pass: 0 SIMT FFT, 1 tensor-core DFT
+    int xform_reg = 1;                    // row/column transforms: 1 register kernels where a plan exists
+    int xform_tile = 0;                   // column pairs per CTA of the register column transform (0: by length)
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)
     cudaEvent_t fork_ev = nullptr;

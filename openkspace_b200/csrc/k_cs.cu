@@ -71,6 +71,7 @@ static int round_up(int v, int m) { return (v + m - 1) / m * m; }
 cudaError_t launch_row_xform(const RowXformArgs& a, const DevPlan& pl, cudaStream_t st) {
     const int n = pl.plan.n;
     if (a.nrows <= 0) return cudaSuccess;
+    if (a.reg && xform_reg_supported(n)) return launch_row_xform_reg(a, n, st);
     int rpc = 16384 / (2 * n);       // two ping-pong buffers within ~128 KB
     if (rpc < 1) rpc = 1;
     if (rpc > 32) rpc = 32;
@@ -122,6 +123,10 @@ __global__ void k_col_xform(ColXformArgs a, FftPlan pl, const float2* __restrict
 cudaError_t launch_col_xform(const ColXformArgs& a, const DevPlan& pl, cudaStream_t st) {
     const int n = pl.plan.n;
     if (a.nprob <= 0 || a.nx <= 0) return cudaSuccess;
+    // the register kernel moves 16-byte chunks of two columns
+    if (a.reg && xform_reg_supported(n) && (a.nx & 1) == 0 && (a.prob_stride & 1) == 0 &&
+        (reinterpret_cast<uintptr_t>(a.data) & 15) == 0)
+        return launch_col_xform_reg(a, st);
     int tc = 4096 / n;
     if (tc > 16) tc = 16;
     if (tc < 1) tc = 1;

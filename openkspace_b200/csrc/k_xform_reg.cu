@@ -1,0 +1,333 @@
+// Standalone centred transforms along rows and columns, register form (sm_100a).
+//
+// The centred DFT of cs.rs:141-218 (ifftshift -> DFT -> fftshift, shift.rs:11-26)
+// for an even length n is a plain DFT between two sign modulations:
+//   out[k] = (-1)^(k + n/2) * sum_m (-1)^m x[m] w^(m k),   w = e^(-+2 pi i / n),
+// since rotating the input by n/2 multiplies the DFT by (-1)^k and rotating
+// the output by n/2 turns (-1)^m into a half-period shift.  The shifts are
+// therefore sign flips on load and store, and the transform itself is one
+// register-resident Stockham plan (reg_fft.cuh) per pair of lines.
+//
+// Rows (k_row_xform_reg): one thread group per row pair.  The next pair is
+// copied (cp.async, 16-byte chunks, L2 only) into the group's staging buffer
+// while the current pair is transformed, so HBM reads overlap the FFT.
+//
+// Columns (k_col_xform_reg): one CTA per tile of 2G columns x n rows, a column
+// pair per thread group.  The tile arrives through the same kind of staging
+// buffer in whole 2G * 8-byte row segments (16-byte chunks XOR-swizzled by row
+// so the groups' column reads are conflict-free); results go back through the
+// groups' exchange buffers so that the CTA writes whole row segments too.
+#include "reg_fft.cuh"
+
+namespace oks {
+namespace reg {
+
+// 16-byte asynchronous global -> shared copy, cached in L2 only; src_bytes 0
+// writes zeros (the source pointer must still be valid).
+__device__ __forceinline__ void cp_async16(float2* dst, const float2* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+// Exchange buffer of one group: the XOR swizzle of padi stays inside aligned
+// blocks of 16, so 2N rounded up to 16 entries suffice.
+template <class P>
+constexpr int xbuf() { return (2 * P::N + 15) / 16 * 16; }
+
+// Groups per CTA of the row kernel (warp-sized groups share a CTA).
+template <class P>
+constexpr int row_groups() { return P::T == 32 ? 4 : 1; }
+
+// Register budget per thread: 64 (32 resident warps), 128 for plans with a
+// large odd radix, whose symmetric butterfly keeps 2 (R - 1) values live.
+template <class P>
+constexpr int xform_regs() {
+    for (int s = 0; s < P::S; ++s)
+        if (P::R[s] % 2 == 1 && P::R[s] > 5) return 128;
+    return 64;
+}
+// Minimum resident CTAs per SM the transform kernels are compiled for.
+template <class P, int THREADS>
+constexpr int xform_min_blocks() {
+    return 65536 / (THREADS * xform_regs<P>()) < 1 ? 1 : 65536 / (THREADS * xform_regs<P>());
+}
+
+template <class P>
+__global__ void __launch_bounds__(P::T * row_groups<P>(), xform_min_blocks<P, P::T * row_groups<P>()>())
+k_row_xform_reg(RowXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
+    constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
+    constexpr int G = row_groups<P>();
+    constexpr int XB = xbuf<P>();
+    constexpr int NTW = Tw<P>::total();
+    extern __shared__ __align__(16) float2 sm[];
+    const int g = threadIdx.x / T, t = threadIdx.x % T;
+    float2* ST = sm + g * 2 * N;                    // [2][N]: the next row pair
+    float2* A = sm + G * 2 * N + g * 2 * XB;
+    float2* B = A + XB;
+    float2* TW = sm + G * 2 * (N + XB);
+    float2* RT = TW + NTW;
+    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    __syncthreads();
+
+    const long long npairs = (a.nrows + 1) >> 1, stride = (long long)gridDim.x * G;
+    const bool live = t < TA, vec = a.vec16 != 0;
+    const int cs = t & 1;                            // row of the pair this thread holds
+    auto row_kept = [&](long long row) {
+        if (row >= a.nrows) return false;
+        return !a.use_keep || row_on(a.keep, row / a.rows_per_prob, (int)(row % a.rows_per_prob));
+    };
+    auto issue = [&](long long u) {
+        const bool k0 = row_kept(2 * u), k1 = row_kept(2 * u + 1);
+        const float2* r0 = a.in + (2 * u) * a.ld_in;
+        const float2* r1 = r0 + a.ld_in;
+        if (vec) {
+#pragma unroll
+            for (int k = t; k < N; k += T) {         // N chunks of two elements
+                const int c = k >= N / 2, x = 2 * (k - c * (N / 2));
+                const bool on = c ? k1 : k0;
+                cp_async16(ST + c * N + x, on ? (c ? r1 : r0) + x : a.in, on ? 16u : 0u);
+            }
+        } else {
+#pragma unroll
+            for (int k = t; k < 2 * N; k += T) {
+                const int c = k >= N, x = k - c * N;
+                const bool on = c ? k1 : k0;
+                cp_async8(ST + c * N + x, on ? (c ? r1 : r0) + x : a.in, on ? 8u : 0u);
+            }
+        }
+        cp_async_commit();
+    };
+    const float sc_n2 = (a.centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    long long u = (long long)blockIdx.x * G + g;
+    if (u < npairs) issue(u);
+    for (; u < npairs; u += stride) {
+        cp_async_wait_all();
+        group_sync<P>();                             // the pair is in ST; A/B are free
+        float2 w[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int x = (t + TA * e) >> 1;
+            float2 v = live ? ST[cs * N + x] : make_float2(0.f, 0.f);
+            if (a.centred && (x & 1)) v = make_float2(-v.x, -v.y);
+            w[e] = v;
+        }
+        group_sync<P>();                             // ST has been read: refill it
+        if (u + stride < npairs) issue(u + stride);
+        if (a.sign < 0) forward<P>(w, A, B, TW, RT, t);
+        else inverse<P>(w, A, B, TW, RT, t);
+        const long long row = 2 * u + cs;
+        if (live && row < a.nrows) {
+            float s = sc_n2;
+            if (a.rowsign && ((row % a.rows_per_prob) & 1)) s = -s;
+            float2* o = a.out + row * a.ld_out;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int k = (t + TA * e) >> 1;
+                o[k] = w[e] * ((a.centred && (k & 1)) ? -s : s);
+            }
+        }
+    }
+    cp_async_wait_all();
+}
+
+template <class P, int G>
+__global__ void __launch_bounds__(P::T * G, xform_min_blocks<P, P::T * G>())
+k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
+    constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
+    constexpr int TC = 2 * G;                        // columns per tile
+    constexpr int KS = G >= 8 ? 0 : G == 4 ? 1 : 2;  // row bits below the swizzle key
+    constexpr int XB = xbuf<P>();
+    constexpr int NTW = Tw<P>::total();
+    static_assert(G == 2 || G == 4 || G == 8, "2, 4 or 8 column pairs per tile");
+    extern __shared__ __align__(16) float2 sm[];
+    const int g = threadIdx.x / T, t = threadIdx.x % T;
+    float2* ST = sm;                                 // [N][TC] staging, 16-byte chunks swizzled
+    float2* AB = sm + N * TC;                        // per group: A, B
+    float2* A = AB + g * 2 * XB;
+    float2* B = A + XB;
+    float2* TW = AB + G * 2 * XB;
+    float2* RT = TW + NTW;
+    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    // chunk j (columns 2j, 2j+1) of row r sits at slot j ^ key(r): the eight
+    // rows a warp's column reads touch then cover all 16 bank pairs
+    auto slot = [](int r, int j) { return r * TC + 2 * (j ^ ((r >> KS) & (G - 1))); };
+    const int ntx = (a.nx + TC - 1) / TC;
+    const long long total = a.nprob * ntx;
+    auto issue = [&](long long u) {
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * TC;
+        const float2* base = a.data + p * a.prob_stride + x0;
+#pragma unroll 4
+        for (int k = threadIdx.x; k < N * G; k += T * G) {
+            const int r = k / G, j = k % G;
+            const bool on = x0 + 2 * j < a.nx;       // nx is even: chunks are whole
+            cp_async16(ST + slot(r, j), on ? base + (long long)r * a.nx + 2 * j : a.data, on ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    const bool live = t < TA;
+    const float sc_n2 = (a.centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    long long u = blockIdx.x;
+    if (u < total) issue(u);
+    for (; u < total; u += gridDim.x) {
+        cp_async_wait_all();
+        __syncthreads();                             // tile in ST; the last tile's stores have read A
+        float2 w[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int q = t + TA * e, r = q >> 1;
+            float2 v = live ? ST[slot(r, g) + (q & 1)] : make_float2(0.f, 0.f);
+            if (a.centred && (r & 1)) v = make_float2(-v.x, -v.y);
+            w[e] = v;
+        }
+        __syncthreads();                             // every group has read ST: refill it
+        if (u + gridDim.x < total) issue(u + gridDim.x);
+        if (a.sign < 0) forward<P>(w, A, B, TW, RT, t);
+        else inverse<P>(w, A, B, TW, RT, t);
+        group_sync<P>();                             // the last stage has read A and B
+        if (live) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int q = t + TA * e, k = q >> 1;
+                A[padi(q) ^ (2 * g)] = w[e] * ((a.centred && (k & 1)) ? -sc_n2 : sc_n2);
+            }
+        }
+        __syncthreads();
+        // whole row segments out: chunk (r, j) is element (r, 0) and (r, 1) of
+        // group j, at padi(2r) ^ 2j and that index ^ 1
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * TC;
+        float2* base = a.data + p * a.prob_stride + x0;
+#pragma unroll 4
+        for (int k = threadIdx.x; k < N * G; k += T * G) {
+            const int r = k / G, j = k % G;
+            if (x0 + 2 * j >= a.nx) continue;
+            const int i0 = padi(2 * r) ^ (2 * j);
+            const float4 v = *reinterpret_cast<const float4*>(AB + j * 2 * XB + (i0 & ~1));
+            *reinterpret_cast<float4*>(base + (long long)r * a.nx + 2 * j) =
+                (i0 & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
+        }
+    }
+    cp_async_wait_all();
+}
+
+// Resident CTAs per SM of a kernel at a dynamic shared-memory size, queried
+// once per (kernel, size) and device.
+static int ctas_per_sm(const void* fn, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, size_t>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair(fn, smem + ((size_t)dev << 40));
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem) != cudaSuccess || n < 1) n = 1;
+    cache[key] = n;
+    return n;
+}
+
+static int sm_count() {
+    static int n[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!n[dev]) cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev);
+    return n[dev] > 0 ? n[dev] : 148;
+}
+
+template <class P>
+static cudaError_t row_p(const RowXformArgs& a, cudaStream_t st) {
+    constexpr int G = row_groups<P>();
+    const float2 *tw, *rt;
+    int nrt;
+    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)G * 2 * (P::N + xbuf<P>()) + Tw<P>::total() + nrt);
+    const void* fn = reinterpret_cast<const void*>(k_row_xform_reg<P>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long units = (a.nrows + 1) / 2;
+    long long grid = (units + G - 1) / G;
+    const long long cap = (long long)ctas_per_sm(fn, P::T * G, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    RowXformArgs b = a;
+    b.vec16 = ((reinterpret_cast<uintptr_t>(a.in) & 15) == 0 && (a.ld_in & 1) == 0) ? 1 : 0;
+    k_row_xform_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(b, tw, rt, nrt);
+    return cudaGetLastError();
+}
+
+template <class P, int G>
+static cudaError_t col_pg(const ColXformArgs& a, cudaStream_t st) {
+    const float2 *tw, *rt;
+    int nrt;
+    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)P::N * 2 * G + (size_t)G * 2 * xbuf<P>() + Tw<P>::total() + nrt);
+    const void* fn = reinterpret_cast<const void*>(k_col_xform_reg<P, G>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = a.nprob * ((a.nx + 2 * G - 1) / (2 * G));
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, P::T * G, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    k_col_xform_reg<P, G><<<(unsigned)grid, P::T * G, smem, st>>>(a, tw, rt, nrt);
+    return cudaGetLastError();
+}
+
+// Column pairs per tile: 8 (128-byte row segments) where the staging and
+// exchange buffers of 8 groups fit one SM's shared memory and 8 groups get
+// the plan's register budget, else 4.
+template <class P>
+static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
+    constexpr bool g8 = P::N <= 512 && P::T * 8 * xform_regs<P>() <= 65536;
+    int g = a.tile > 0 ? a.tile : (g8 ? 8 : 4);
+    if (g >= 8 && P::N > 512) g = 4;
+    if (g >= 8) return col_pg<P, 8>(a, st);
+    if (g >= 4) return col_pg<P, 4>(a, st);
+    return col_pg<P, 2>(a, st);
+}
+
+}  // namespace reg
+
+bool xform_reg_supported(int n) {
+    switch (n) {
+        case 128: case 192: case 256: case 320: case 368: case 384: case 512: case 640: return true;
+        default: return false;
+    }
+}
+
+cudaError_t launch_row_xform_reg(const RowXformArgs& a, int n, cudaStream_t st) {
+    if (a.nrows <= 0) return cudaSuccess;
+    switch (n) {
+        case 128: return reg::row_p<reg::S128>(a, st);
+        case 192: return reg::row_p<reg::S192>(a, st);
+        case 256: return reg::row_p<reg::S256>(a, st);
+        case 320: return reg::row_p<reg::S320>(a, st);
+        case 368: return reg::row_p<reg::S368>(a, st);
+        case 384: return reg::row_p<reg::S384>(a, st);
+        case 512: return reg::row_p<reg::S512>(a, st);
+        case 640: return reg::row_p<reg::P640>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_col_xform_reg(const ColXformArgs& a, cudaStream_t st) {
+    if (a.nprob <= 0 || a.nx <= 0) return cudaSuccess;
+    switch (a.ny) {
+        case 128: return reg::col_p<reg::S128>(a, st);
+        case 192: return reg::col_p<reg::S192>(a, st);
+        case 256: return reg::col_p<reg::S256>(a, st);
+        case 320: return reg::col_p<reg::S320>(a, st);
+        case 368: return reg::col_p<reg::S368>(a, st);
+        case 384: return reg::col_p<reg::S384>(a, st);
+        case 512: return reg::col_p<reg::S512>(a, st);
+        case 640: return reg::col_p<reg::P640>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace oks

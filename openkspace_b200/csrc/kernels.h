@@ -63,6 +63,8 @@ struct RowXformArgs {
     int rowsign;         // multiply row r by (-1)^r
     int use_keep;        // rows outside the problem's row mask are zero
     RowMasks keep;
+    int reg = 1;         // register-resident kernel where a plan of length n exists
+    int vec16 = 0;       // set by the launcher: rows start on 16-byte boundaries
 };
 cudaError_t launch_row_xform(const RowXformArgs& a, const DevPlan& pl, cudaStream_t st);
 
@@ -74,8 +76,16 @@ struct ColXformArgs {
     long long prob_stride;
     int sign, centred;
     float scale;
+    int reg = 1;         // register-resident kernel where a plan of length ny exists
+    int tile = 0;        // column pairs per CTA of that kernel (0: by length; 2, 4, 8)
 };
 cudaError_t launch_col_xform(const ColXformArgs& a, const DevPlan& pl, cudaStream_t st);
+
+// Register-resident centred transforms (k_xform_reg.cu) for the lengths with
+// a register plan; even lengths only, the shifts folded into sign flips.
+bool xform_reg_supported(int n);
+cudaError_t launch_row_xform_reg(const RowXformArgs& a, int n, cudaStream_t st);
+cudaError_t launch_col_xform_reg(const ColXformArgs& a, cudaStream_t st);
 
 // One problem (one coil of one slice) of a batched launch with per-problem
 // width, iteration count, lambda and mask (FistaColArgs::probs).

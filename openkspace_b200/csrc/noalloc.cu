@@ -115,6 +115,7 @@ extern "C" int okscuda_cs_slice_noalloc(okscuda_ctx* ctx, const okscuda_c64* d_k
     float2* coils = reinterpret_cast<float2*>(base + kTableBytes);
     const oks::RowMasks rm{reinterpret_cast<const uint32_t*>(base + o_mask), wstride, 1};
     oks::RowXformArgs ra{};
+    ra.reg = ctx->xform_reg;
     ra.in = reinterpret_cast<const float2*>(d_kspace);
     ra.out = coils;
     ra.nrows = (long long)nc * ny;

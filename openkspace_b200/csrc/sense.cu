@@ -125,6 +125,7 @@ extern "C" int okscuda_sense_cs(okscuda_ctx* ctx, const okscuda_c64* d_kspace, c
     if (h_lipschitz) *h_lipschitz = L;
     // 4. y'_c for every coil (row IDFT of the masked data, as the per-coil path)
     oks::RowXformArgs ra{};
+    ra.reg = ctx->xform_reg;
     ra.in = reinterpret_cast<const float2*>(d_kspace);
     ra.out = work;
     ra.nrows = (long long)nc * ny;

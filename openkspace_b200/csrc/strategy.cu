@@ -125,6 +125,7 @@ int okscuda_ifft1_kz(okscuda_ctx* ctx, okscuda_c64* d_data, int nc, int nz, int 
     int rc = get_plan(ctx, nz, &pz);
     if (rc) return rc;
     oks::ColXformArgs ca{};
+    ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile;
     ca.data = reinterpret_cast<float2*>(d_data);
     ca.nprob = nc;
     ca.ny = nz;
@@ -149,6 +150,7 @@ int okscuda_ifft2(okscuda_ctx* ctx, okscuda_c64* d_data, long long batch, int ny
         int rc = get_plan(ctx, ny, &py);
         if (rc) return rc;
         oks::ColXformArgs ca{};
+        ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile;
         ca.data = d; ca.nprob = batch; ca.ny = ny; ca.nx = nx; ca.prob_stride = (long long)ny * nx;
         ca.sign = +1; ca.centred = 1; ca.scale = 1.0f / (float)ny;
         ProfScope ps(ctx, "k_col_xform");
@@ -159,6 +161,7 @@ int okscuda_ifft2(okscuda_ctx* ctx, okscuda_c64* d_data, long long batch, int ny
         int rc = get_plan(ctx, nx, &px);
         if (rc) return rc;
         oks::RowXformArgs ra{};
+        ra.reg = ctx->xform_reg;
         ra.in = d; ra.out = d; ra.nrows = batch * ny; ra.ld_in = nx; ra.ld_out = nx;
         ra.sign = +1; ra.centred = 1; ra.scale = 1.0f / (float)nx; ra.rows_per_prob = ny;
         ProfScope ps(ctx, "k_row_xform");
