@@ -16,6 +16,8 @@ A step is one pass of the hot path over one batch of synthetic input:
   volume3d   32 coils, 256 x 256 x 192 3-D Cartesian, R = 6, 80 iterations: the
              CsRss 3-D path (kz IFFT, 192 x 32 slice solves, RSS)
   served     Poisson arrivals through the request server beside the plain drop-in
+  fft        the centred 2-D FFT alone: 1024 coil planes of 368 x 640 in place
+             (the row and column transform kernels; metric planes/s)
 value = slices/s with inputs resident in HBM; e2e = the same through the
 public API with pinned host buffers copied in and the result copied out inside
 the timed region.  Multi-GPU: one process per GPU, every rank solves its own
@@ -356,11 +358,104 @@ class Volume3dWorkload:
         return dt, ncoil / self.nc, f"1 slice: kz IFFT of {ncoil} of {self.nc} coils + FISTA + RSS (scaled)"
 
 
+class FftWorkload:
+    """The centred 2-D FFT of cs.rs:141-178 on a batch of coil planes of the
+    precision configuration's encoded size (368 ky x 640 readout), in place:
+    one register-resident row pass (length 640) and one column pass (length
+    368), each reading and writing every plane once."""
+    name = "fft"
+    metric = "centred 2-D FFT coil planes/s (relative L2 <= 1e-5 vs FP64)"
+    unit = "planes/s"
+    data = "synthetic (seeded complex Gaussian planes)"
+    dominant = ("k_col_xform", "k_row_xform")
+    bytes_model = "16 B per pixel per pass (read + write complex64)"
+
+    def __init__(self, nplanes: int = 1024, ny: int = 368, nx: int = 640):
+        self.nplanes, self.ny, self.nx = nplanes, ny, nx
+        self.units = nplanes
+
+    def config(self):
+        return {"workload": f"centred_fft2_{self.nplanes}x{self.ny}x{self.nx}", "planes_per_step": self.nplanes,
+                "ny": self.ny, "nx": self.nx, "direction": "forward, in place",
+                "unit": "one coil plane of the precision configuration's encoded size"}
+
+    def input_bytes(self):
+        return self.nplanes * self.ny * self.nx * 8
+
+    def dominant_bytes_per_step(self, kernel=None):
+        return 16.0 * self.nplanes * self.ny * self.nx
+
+    def prepare(self, ctx):
+        import torch
+        self.ctx = ctx
+        g = torch.Generator(device="cuda").manual_seed(7)
+        self.d = torch.randn((self.nplanes, self.ny, self.nx), dtype=torch.complex64, device="cuda", generator=g)
+        self.h_in = self.d.cpu().pin_memory()
+        self.h_out = torch.empty_like(self.h_in).pin_memory()
+        torch.cuda.synchronize()
+
+    def step_device(self):
+        c = self.ctx
+        c.check(c.lib.okscuda_centred_fft2(c.handle, self.d.data_ptr(), self.nplanes, self.ny, self.nx, 0))
+
+    def step_e2e(self):
+        c = self.ctx
+        nb = self.input_bytes()
+        c.check(c.lib.okscuda_upload(c.handle, self.d.data_ptr(), self.h_in.data_ptr(), nb))
+        self.step_device()
+        c.check(c.lib.okscuda_download(c.handle, self.h_out.data_ptr(), self.d.data_ptr(), nb))
+
+    def e2e_bytes(self):
+        return self.input_bytes(), self.input_bytes()
+
+    def cpu_sample(self, nthreads):
+        """The oracle's FP32 centred 2-D FFT (oracle/cs_ref.c) on a few planes."""
+        from oracle import csref
+        n = 8
+        rng = np.random.default_rng(7)
+        x = (rng.standard_normal((n, self.ny, self.nx)) + 1j * rng.standard_normal((n, self.ny, self.nx)))
+        x = x.astype(np.complex64)
+        t = time.perf_counter()
+        csref.centred_fft2(x)
+        return time.perf_counter() - t, n, f"{n} planes through the oracle's centred FFT2"
+
+
+def fft_stages(ctx, shapes=((368, 640), (256, 256), (320, 320), (384, 384), (512, 512)), target=1 << 30, reps=5):
+    """HBM rate of the row and column passes of the centred 2-D FFT (in place,
+    about 1 GiB of planes per shape, above L2): algorithmic 16 B per pixel per
+    pass over the device time of each pass's launches."""
+    import torch
+    hbm, kind = peaks()
+    out = {"peak_gbs": hbm, "peak_kind": kind, "bytes_model": "16 B per pixel per pass"}
+    for ny, nx in shapes:
+        batch = max(1, target // (ny * nx * 8))
+        d = torch.zeros((batch, ny, nx), dtype=torch.complex64, device="cuda")
+        torch.cuda.synchronize()
+        for _ in range(2):
+            ctx.check(ctx.lib.okscuda_centred_fft2(ctx.handle, d.data_ptr(), batch, ny, nx, 0))
+        ctx.profile(True)
+        for _ in range(reps):
+            ctx.check(ctx.lib.okscuda_centred_fft2(ctx.handle, d.data_ptr(), batch, ny, nx, 0))
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        rec = {"planes": batch}
+        for k, length in (("k_row_xform", nx), ("k_col_xform", ny)):
+            ms, n = prof[k]
+            gbs = 16.0 * batch * ny * nx / (ms / n / 1e3) / 1e9
+            rec[k] = {"length": length, "us_per_launch": 1e3 * ms / n, "achieved_gbs": gbs, "frac": gbs / hbm}
+        out[f"{ny}x{nx}"] = rec
+        del d
+    torch.cuda.synchronize()
+    return out
+
+
 WORKLOADS = {"plain": lambda: PlainWorkload(1), "volume": lambda: PlainWorkload(36),
              "precision": lambda: PrecisionWorkload(36), "batched": lambda: BatchedWorkload(64),
              "volume3d": lambda: Volume3dWorkload(),
              # reduced sizes of the same kernels, for profiler captures only
-             "precision_small": lambda: PrecisionWorkload(2, 4), "batched_small": lambda: BatchedWorkload(6)}
+             "fft": lambda: FftWorkload(),
+             "precision_small": lambda: PrecisionWorkload(2, 4), "batched_small": lambda: BatchedWorkload(6),
+             "fft_small": lambda: FftWorkload(96)}
 
 
 def serving_measure(ctx, rates, seconds, max_requests):
@@ -517,13 +612,15 @@ def run_reference(args, wl, rank):
             units += u
     total = sum(times)
     value = units / total
-    line = {"impl": "reference", "metric": "FISTA-CS slices/s (CPU restatement of the reference)",
-            "value": value, "unit": "slices/s", "n_gpus": args.gpus, "steps": args.steps,
+    vunit = getattr(wl, "unit", "slices/s")
+    metric = getattr(wl, "metric", "FISTA-CS slices/s at NRMSE<=1e-4 vs FP64")
+    line = {"impl": "reference", "metric": metric, "arm": "CPU restatement of the reference",
+            "value": value, "unit": vunit, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
             "dtype": "c64", "data": "synthetic", "config": wl.config(),
-            "cpu_baseline": {"value": value, "unit": "slices/s", "cores": nthreads, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": vunit, "cores": nthreads, "kind": "port",
                              "sample": sample},
-            "e2e": {"value": value, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": vunit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -639,7 +736,8 @@ def main():
     dom_name = next((k for k in wl.dominant if k in prof), wl.dominant[0])
     dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
     # algorithmic bytes of the dominant kernel over the timed steps / its device time
-    dbytes = wl.dominant_bytes_per_step(dom_name) if wl.name == "precision" else wl.dominant_bytes_per_step()
+    dbytes = (wl.dominant_bytes_per_step(dom_name) if wl.name in ("precision", "fft")
+              else wl.dominant_bytes_per_step())
     achieved = dbytes * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     if wl.name == "precision" and args.row_engine == "tc":
         # tensor-core row DFTs: the tcgen05 FLOPs they issue / their device time
@@ -659,14 +757,16 @@ def main():
     if rank != 0:
         return
     h2d, d2h = wl.e2e_bytes()
+    metric = getattr(wl, "metric", "FISTA-CS slices/s at NRMSE<=1e-4 vs FP64")
+    vunit = getattr(wl, "unit", "slices/s")
     line = {
-        "metric": "FISTA-CS slices/s at NRMSE<=1e-4 vs FP64",
-        "value": value, "unit": "slices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": metric,
+        "value": value, "unit": vunit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "c64", "data": "synthetic (seeded phantom/coils/noise/masks)",
+        "dtype": "c64", "data": getattr(wl, "data", "synthetic (seeded phantom/coils/noise/masks)"),
         "config": {**wl.config(), "parallelism": f"replicas x{world} (slices sharded, no collective)",
                    "l2": "flushed between steps" if flush is not None else "inputs larger than L2"},
-        "e2e": {"value": e2e_value, "unit": "slices/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_value, "unit": vunit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof.items()},
         "roofline": {"bound": bound, "kernel": dom_name, "achieved": achieved, "peak": peak,
@@ -690,10 +790,14 @@ def main():
                            "served_over_plain": served["800"]["slices_per_s"] / plain["slices_per_s"],
                            "requests": "sizes {256^2,320^2,384^2,368x640}, coils U{8..32}, R {2,3,4,6}, "
                                        "iters U{30..150}; --workload served for 50/200/800 req/s"}
+    if wl.name == "precision" and not args.no_extras:
+        # the FFT stages on their own: row and column passes of the centred
+        # 2-D FFT at the configuration's lengths, against the HBM roofline
+        line["fft_stages"] = fft_stages(ctx)
     if not args.no_cpu_baseline:
         nthreads = 1
         dt, u, sample = wl.cpu_sample(nthreads)
-        line["cpu_baseline"] = {"value": u / dt, "unit": "slices/s", "cores": nthreads, "kind": "port",
+        line["cpu_baseline"] = {"value": u / dt, "unit": vunit, "cores": nthreads, "kind": "port",
                                 "sample": sample}
     print(json.dumps(line), flush=True)
     if dist is not None:

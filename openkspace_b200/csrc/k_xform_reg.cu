@@ -14,8 +14,7 @@
 //
 // Columns (k_col_xform_reg): one CTA per tile of 2G columns x n rows, a column
 // pair per thread group.  The tile arrives through the same kind of staging
-// buffer in whole 2G * 8-byte row segments (16-byte chunks XOR-swizzled by row
-// so the groups' column reads are conflict-free); results go back through the
+// buffer in whole 2G * 8-byte row segments; results go back through the
 // groups' exchange buffers so that the CTA writes whole row segments too.
 #include "reg_fft.cuh"
 
@@ -40,22 +39,22 @@ constexpr int xbuf() { return (2 * P::N + 15) / 16 * 16; }
 template <class P>
 constexpr int row_groups() { return P::T == 32 ? 4 : 1; }
 
-// Register budget per thread: 64 (32 resident warps), 128 for plans with a
-// large odd radix, whose symmetric butterfly keeps 2 (R - 1) values live.
+// Register budget per thread: 64 (32 resident warps), more for plans with a
+// large odd radix, whose symmetric butterfly keeps 2 (R - 1) values live:
+// 128 in the row kernel, 168 in the column kernel (its groups' exchange
+// buffers sit at a runtime offset, which costs address registers).
 template <class P>
-constexpr int xform_regs() {
+constexpr bool big_odd_plan() {
     for (int s = 0; s < P::S; ++s)
-        if (P::R[s] % 2 == 1 && P::R[s] > 5) return 128;
-    return 64;
+        if (P::R[s] % 2 == 1 && P::R[s] > 5) return true;
+    return false;
 }
-// Minimum resident CTAs per SM the transform kernels are compiled for.
-template <class P, int THREADS>
-constexpr int xform_min_blocks() {
-    return 65536 / (THREADS * xform_regs<P>()) < 1 ? 1 : 65536 / (THREADS * xform_regs<P>());
-}
+// Minimum resident CTAs per SM for a register budget.
+template <int THREADS, int REGS>
+constexpr int xform_min_blocks() { return 65536 / (THREADS * REGS) < 1 ? 1 : 65536 / (THREADS * REGS); }
 
 template <class P>
-__global__ void __launch_bounds__(P::T * row_groups<P>(), xform_min_blocks<P, P::T * row_groups<P>()>())
+__global__ void __launch_bounds__(P::T * row_groups<P>(), xform_min_blocks<P::T * row_groups<P>(), big_odd_plan<P>() ? 128 : 64>())
 k_row_xform_reg(RowXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
     constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
     constexpr int G = row_groups<P>();
@@ -134,38 +133,38 @@ k_row_xform_reg(RowXformArgs a, const float2* __restrict__ gtw, const float2* __
 }
 
 template <class P, int G>
-__global__ void __launch_bounds__(P::T * G, xform_min_blocks<P, P::T * G>())
+__global__ void __launch_bounds__(P::T * G, xform_min_blocks<P::T * G, big_odd_plan<P>() ? 168 : 64>())
 k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
     constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
     constexpr int TC = 2 * G;                        // columns per tile
-    constexpr int KS = G >= 8 ? 0 : G == 4 ? 1 : 2;  // row bits below the swizzle key
-    constexpr int XB = xbuf<P>();
+    constexpr int SS = TC + 2;                       // staging row stride (float2)
+    constexpr int GS = 2 * xbuf<P>() + 2;            // per-group stride of the A, B buffers
     constexpr int NTW = Tw<P>::total();
     static_assert(G == 2 || G == 4 || G == 8, "2, 4 or 8 column pairs per tile");
     extern __shared__ __align__(16) float2 sm[];
     const int g = threadIdx.x / T, t = threadIdx.x % T;
-    float2* ST = sm;                                 // [N][TC] staging, 16-byte chunks swizzled
-    float2* AB = sm + N * TC;                        // per group: A, B
-    float2* A = AB + g * 2 * XB;
-    float2* B = A + XB;
-    float2* TW = AB + G * 2 * XB;
+    // The strides are padded by one 16-byte chunk, so that consecutive rows
+    // (staging) and consecutive groups (A) start on different bank pairs:
+    // a group's column reads and the CTA's row-segment reads are then
+    // conflict-free, with indices linear in the element number.
+    float2* ST = sm;                                 // [N][SS] staging of the next tile
+    float2* AB = sm + N * SS;
+    float2* A = AB + g * GS;
+    float2* B = A + xbuf<P>();
+    float2* TW = AB + G * GS;
     float2* RT = TW + NTW;
     for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
-    // chunk j (columns 2j, 2j+1) of row r sits at slot j ^ key(r): the eight
-    // rows a warp's column reads touch then cover all 16 bank pairs
-    auto slot = [](int r, int j) { return r * TC + 2 * (j ^ ((r >> KS) & (G - 1))); };
     const int ntx = (a.nx + TC - 1) / TC;
     const long long total = a.nprob * ntx;
     auto issue = [&](long long u) {
         const long long p = u / ntx;
         const int x0 = (int)(u - p * ntx) * TC;
         const float2* base = a.data + p * a.prob_stride + x0;
-#pragma unroll 4
         for (int k = threadIdx.x; k < N * G; k += T * G) {
             const int r = k / G, j = k % G;
             const bool on = x0 + 2 * j < a.nx;       // nx is even: chunks are whole
-            cp_async16(ST + slot(r, j), on ? base + (long long)r * a.nx + 2 * j : a.data, on ? 16u : 0u);
+            cp_async16(ST + r * SS + 2 * j, on ? base + (long long)r * a.nx + 2 * j : a.data, on ? 16u : 0u);
         }
         cp_async_commit();
     };
@@ -180,7 +179,7 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int q = t + TA * e, r = q >> 1;
-            float2 v = live ? ST[slot(r, g) + (q & 1)] : make_float2(0.f, 0.f);
+            float2 v = live ? ST[r * SS + 2 * g + (q & 1)] : make_float2(0.f, 0.f);
             if (a.centred && (r & 1)) v = make_float2(-v.x, -v.y);
             w[e] = v;
         }
@@ -193,23 +192,19 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int q = t + TA * e, k = q >> 1;
-                A[padi(q) ^ (2 * g)] = w[e] * ((a.centred && (k & 1)) ? -sc_n2 : sc_n2);
+                A[q] = w[e] * ((a.centred && (k & 1)) ? -sc_n2 : sc_n2);
             }
         }
         __syncthreads();
-        // whole row segments out: chunk (r, j) is element (r, 0) and (r, 1) of
-        // group j, at padi(2r) ^ 2j and that index ^ 1
+        // whole row segments out: chunk (r, j) is A_j[2r], A_j[2r + 1]
         const long long p = u / ntx;
         const int x0 = (int)(u - p * ntx) * TC;
         float2* base = a.data + p * a.prob_stride + x0;
-#pragma unroll 4
         for (int k = threadIdx.x; k < N * G; k += T * G) {
             const int r = k / G, j = k % G;
             if (x0 + 2 * j >= a.nx) continue;
-            const int i0 = padi(2 * r) ^ (2 * j);
-            const float4 v = *reinterpret_cast<const float4*>(AB + j * 2 * XB + (i0 & ~1));
             *reinterpret_cast<float4*>(base + (long long)r * a.nx + 2 * j) =
-                (i0 & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
+                *reinterpret_cast<const float4*>(AB + j * GS + 2 * r);
         }
     }
     cp_async_wait_all();
@@ -267,7 +262,7 @@ static cudaError_t col_pg(const ColXformArgs& a, cudaStream_t st) {
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(float2) * ((size_t)P::N * 2 * G + (size_t)G * 2 * xbuf<P>() + Tw<P>::total() + nrt);
+    const size_t smem = sizeof(float2) * ((size_t)P::N * (2 * G + 2) + (size_t)G * (2 * xbuf<P>() + 2) + Tw<P>::total() + nrt);
     const void* fn = reinterpret_cast<const void*>(k_col_xform_reg<P, G>);
     if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
     const long long tiles = a.nprob * ((a.nx + 2 * G - 1) / (2 * G));
@@ -278,12 +273,11 @@ static cudaError_t col_pg(const ColXformArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// Column pairs per tile: 8 (128-byte row segments) where the staging and
-// exchange buffers of 8 groups fit one SM's shared memory and 8 groups get
-// the plan's register budget, else 4.
+// Column pairs per tile: 8 (128-byte row segments) where 8 groups fit one
+// CTA (1024 threads, 64 registers each) and one SM's shared memory, else 4.
 template <class P>
 static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
-    constexpr bool g8 = P::N <= 512 && P::T * 8 * xform_regs<P>() <= 65536;
+    constexpr bool g8 = P::N <= 512 && P::T * 8 <= 1024 && !big_odd_plan<P>();
     int g = a.tile > 0 ? a.tile : (g8 ? 8 : 4);
     if (g >= 8 && P::N > 512) g = 4;
     if (g >= 8) return col_pg<P, 8>(a, st);
