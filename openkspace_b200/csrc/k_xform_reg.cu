@@ -53,21 +53,46 @@ constexpr bool big_odd_plan() {
 template <int THREADS, int REGS>
 constexpr int xform_min_blocks() { return 65536 / (THREADS * REGS) < 1 ? 1 : 65536 / (THREADS * REGS); }
 
+// A launch runs one direction, so shared memory holds only that direction's
+// twiddles: forward entries [0, NF), inverse entries [NF, total).
 template <class P>
+constexpr int tw_half() {
+    constexpr int nf = Tw<P>::fwd(P::S), ni = Tw<P>::total() - Tw<P>::fwd(P::S);
+    return nf > ni ? nf : ni;
+}
+
+// Copies direction SIGN's twiddles to TWs and returns the base pointer the
+// drivers index with the full table's offsets (TWs minus the skipped part, a
+// compile-time offset; it stays inside the CTA's buffers, which precede TWs).
+template <class P, int SIGN>
+__device__ __forceinline__ const float2* load_twiddles(float2* TWs, const float2* __restrict__ gtw) {
+    constexpr int NF = Tw<P>::fwd(P::S);
+    constexpr int off = SIGN > 0 ? NF : 0, n = SIGN > 0 ? Tw<P>::total() - NF : NF;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) TWs[q] = gtw[off + q];
+    return TWs - off;
+}
+
+// The transform of direction SIGN (-1 forward, +1 unnormalised inverse).
+template <class P, int SIGN, bool NB = false>
+__device__ __forceinline__ void transform(float2* w, float2* A, float2* B, const float2* TW, const float2* RT, int t) {
+    if constexpr (SIGN < 0) forward<P, NB>(w, A, B, TW, RT, t);
+    else inverse<P, NB>(w, A, B, TW, RT, t);
+}
+
+template <class P, int SIGN>
 __global__ void __launch_bounds__(P::T * row_groups<P>(), xform_min_blocks<P::T * row_groups<P>(), big_odd_plan<P>() ? 128 : 64>())
 k_row_xform_reg(RowXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
     constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
     constexpr int G = row_groups<P>();
     constexpr int XB = xbuf<P>();
-    constexpr int NTW = Tw<P>::total();
     extern __shared__ __align__(16) float2 sm[];
     const int g = threadIdx.x / T, t = threadIdx.x % T;
     float2* ST = sm + g * 2 * N;                    // [2][N]: the next row pair
     float2* A = sm + G * 2 * N + g * 2 * XB;
     float2* B = A + XB;
-    float2* TW = sm + G * 2 * (N + XB);
-    float2* RT = TW + NTW;
-    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    float2* TWs = sm + G * 2 * (N + XB);
+    float2* RT = TWs + tw_half<P>();
+    const float2* TW = load_twiddles<P, SIGN>(TWs, gtw);
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
     __syncthreads();
 
@@ -115,8 +140,7 @@ k_row_xform_reg(RowXformArgs a, const float2* __restrict__ gtw, const float2* __
         }
         group_sync<P>();                             // ST has been read: refill it
         if (u + stride < npairs) issue(u + stride);
-        if (a.sign < 0) forward<P>(w, A, B, TW, RT, t);
-        else inverse<P>(w, A, B, TW, RT, t);
+        transform<P, SIGN>(w, A, B, TW, RT, t);
         const long long row = 2 * u + cs;
         if (live && row < a.nrows) {
             float s = sc_n2;
@@ -132,14 +156,13 @@ k_row_xform_reg(RowXformArgs a, const float2* __restrict__ gtw, const float2* __
     cp_async_wait_all();
 }
 
-template <class P, int G>
+template <class P, int G, int SIGN>
 __global__ void __launch_bounds__(P::T * G, xform_min_blocks<P::T * G, big_odd_plan<P>() ? 168 : 64>())
 k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
     constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
     constexpr int TC = 2 * G;                        // columns per tile
     constexpr int SS = TC + 2;                       // staging row stride (float2)
     constexpr int GS = 2 * xbuf<P>() + 2;            // per-group stride of the A, B buffers
-    constexpr int NTW = Tw<P>::total();
     static_assert(G == 2 || G == 4 || G == 8, "2, 4 or 8 column pairs per tile");
     extern __shared__ __align__(16) float2 sm[];
     const int g = threadIdx.x / T, t = threadIdx.x % T;
@@ -151,9 +174,9 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
     float2* AB = sm + N * SS;
     float2* A = AB + g * GS;
     float2* B = A + xbuf<P>();
-    float2* TW = AB + G * GS;
-    float2* RT = TW + NTW;
-    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    float2* TWs = AB + G * GS;
+    float2* RT = TWs + tw_half<P>();
+    const float2* TW = load_twiddles<P, SIGN>(TWs, gtw);
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
     const int ntx = (a.nx + TC - 1) / TC;
     const long long total = a.nprob * ntx;
@@ -185,9 +208,8 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
         }
         __syncthreads();                             // every group has read ST: refill it
         if (u + gridDim.x < total) issue(u + gridDim.x);
-        if (a.sign < 0) forward<P>(w, A, B, TW, RT, t);
-        else inverse<P>(w, A, B, TW, RT, t);
-        group_sync<P>();                             // the last stage has read A and B
+        transform<P, SIGN, true>(w, A, B, TW, RT, t);
+        group_sync<P, true>();                       // the last stage has read A and B
         if (live) {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
@@ -243,8 +265,9 @@ static cudaError_t row_p(const RowXformArgs& a, cudaStream_t st) {
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(float2) * ((size_t)G * 2 * (P::N + xbuf<P>()) + Tw<P>::total() + nrt);
-    const void* fn = reinterpret_cast<const void*>(k_row_xform_reg<P>);
+    const size_t smem = sizeof(float2) * ((size_t)G * 2 * (P::N + xbuf<P>()) + tw_half<P>() + nrt);
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_row_xform_reg<P, -1>)
+                                : reinterpret_cast<const void*>(k_row_xform_reg<P, +1>);
     if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
     const long long units = (a.nrows + 1) / 2;
     long long grid = (units + G - 1) / G;
@@ -252,7 +275,8 @@ static cudaError_t row_p(const RowXformArgs& a, cudaStream_t st) {
     if (grid > cap) grid = cap;
     RowXformArgs b = a;
     b.vec16 = ((reinterpret_cast<uintptr_t>(a.in) & 15) == 0 && (a.ld_in & 1) == 0) ? 1 : 0;
-    k_row_xform_reg<P><<<(unsigned)grid, P::T * G, smem, st>>>(b, tw, rt, nrt);
+    if (a.sign < 0) k_row_xform_reg<P, -1><<<(unsigned)grid, P::T * G, smem, st>>>(b, tw, rt, nrt);
+    else k_row_xform_reg<P, +1><<<(unsigned)grid, P::T * G, smem, st>>>(b, tw, rt, nrt);
     return cudaGetLastError();
 }
 
@@ -262,14 +286,17 @@ static cudaError_t col_pg(const ColXformArgs& a, cudaStream_t st) {
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(float2) * ((size_t)P::N * (2 * G + 2) + (size_t)G * (2 * xbuf<P>() + 2) + Tw<P>::total() + nrt);
-    const void* fn = reinterpret_cast<const void*>(k_col_xform_reg<P, G>);
+    const size_t smem =
+        sizeof(float2) * ((size_t)P::N * (2 * G + 2) + (size_t)G * (2 * xbuf<P>() + 2) + tw_half<P>() + nrt);
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_col_xform_reg<P, G, -1>)
+                                : reinterpret_cast<const void*>(k_col_xform_reg<P, G, +1>);
     if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
     const long long tiles = a.nprob * ((a.nx + 2 * G - 1) / (2 * G));
     long long grid = tiles;
     const long long cap = (long long)ctas_per_sm(fn, P::T * G, smem) * sm_count();
     if (grid > cap) grid = cap;
-    k_col_xform_reg<P, G><<<(unsigned)grid, P::T * G, smem, st>>>(a, tw, rt, nrt);
+    if (a.sign < 0) k_col_xform_reg<P, G, -1><<<(unsigned)grid, P::T * G, smem, st>>>(a, tw, rt, nrt);
+    else k_col_xform_reg<P, G, +1><<<(unsigned)grid, P::T * G, smem, st>>>(a, tw, rt, nrt);
     return cudaGetLastError();
 }
 

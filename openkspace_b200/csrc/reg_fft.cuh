@@ -357,15 +357,23 @@ __device__ __forceinline__ void stage_to_reg(const float2* __restrict__ src, flo
     }
 }
 
-template <class P>
+// Barrier of one thread group.  NB (named barriers): groups of T >= 64
+// threads that share a CTA wait on barrier 1 + group index only, so the
+// groups do not hold each other up stage by stage.
+template <class P, bool NB = false>
 __device__ __forceinline__ void group_sync() {
-    if constexpr (P::T == 32) __syncwarp();
-    else __syncthreads();
+    if constexpr (P::T == 32) {
+        __syncwarp();
+    } else if constexpr (NB) {
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / P::T)), "n"(P::T) : "memory");
+    } else {
+        __syncthreads();
+    }
 }
 
 // Forward transform: registers (state layout) -> registers (mid layout of
 // the last radix).  Stages 0..S-2 go through smem buffers A/B.
-template <class P, int s>
+template <class P, int s, bool NB = false>
 __device__ __forceinline__ void fwd_rest(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
                                          int t) {
     if constexpr (s < P::S) {
@@ -378,13 +386,13 @@ __device__ __forceinline__ void fwd_rest(float2* w, float2* A, float2* B, const 
             stage_to_reg<P, -1, R, p>(src, w, tw + off, roots, t);
         } else {
             stage_smem<P, -1, R, p>(src, dst, tw + off, roots, t);
-            group_sync<P>();
-            fwd_rest<P, s + 1>(w, A, B, tw, roots, t);
+            group_sync<P, NB>();
+            fwd_rest<P, s + 1, NB>(w, A, B, tw, roots, t);
         }
     }
 }
 
-template <class P>
+template <class P, bool NB = false>
 __device__ __forceinline__ void forward(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
                                         int t) {
     constexpr int R0 = P::R[0];
@@ -392,13 +400,13 @@ __device__ __forceinline__ void forward(float2* w, float2* A, float2* B, const f
         stage_reg<P, -1, R0, 1>(w, nullptr, tw, roots, t);
     } else {
         stage_reg<P, -1, R0, 1>(w, A, tw, roots, t);   // outputs to A
-        group_sync<P>();
-        fwd_rest<P, 1>(w, A, B, tw, roots, t);
+        group_sync<P, NB>();
+        fwd_rest<P, 1, NB>(w, A, B, tw, roots, t);
     }
 }
 
 // Inverse transform: registers (mid layout of R[S-1]) -> registers (state).
-template <class P, int s>
+template <class P, int s, bool NB = false>
 __device__ __forceinline__ void inv_rest(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
                                          int t) {
     if constexpr (s < P::S) {
@@ -411,13 +419,13 @@ __device__ __forceinline__ void inv_rest(float2* w, float2* A, float2* B, const 
             stage_to_reg<P, +1, R, p>(src, w, tw + off, roots, t);
         } else {
             stage_smem<P, +1, R, p>(src, dst, tw + off, roots, t);
-            group_sync<P>();
-            inv_rest<P, s + 1>(w, A, B, tw, roots, t);
+            group_sync<P, NB>();
+            inv_rest<P, s + 1, NB>(w, A, B, tw, roots, t);
         }
     }
 }
 
-template <class P>
+template <class P, bool NB = false>
 __device__ __forceinline__ void inverse(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
                                         int t) {
     constexpr int R0 = P::R[P::S - 1];
@@ -425,8 +433,8 @@ __device__ __forceinline__ void inverse(float2* w, float2* A, float2* B, const f
         stage_reg<P, +1, R0, 1>(w, nullptr, tw + Tw<P>::inv(0), roots, t);
     } else {
         stage_reg<P, +1, R0, 1>(w, A, tw + Tw<P>::inv(0), roots, t);
-        group_sync<P>();
-        inv_rest<P, 1>(w, A, B, tw, roots, t);
+        group_sync<P, NB>();
+        inv_rest<P, 1, NB>(w, A, B, tw, roots, t);
     }
 }
 
