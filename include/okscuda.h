@@ -80,11 +80,20 @@ const char* okscuda_version(void);
  *                   column pass with separable masks (default 1), bit 1 row
  *                   pass
  *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
- *                   least 12 warps resident per SM, 0 = registers as needed
+ *                   least 12 warps resident per SM, 2 = at least 18,
+ *                   0 = registers as needed
  *   "autotune_use"  1 (default): shapes in the autotune table use their
  *                   tuned choices in place of the options above; 0: ignore
  *                   the table
  *   "autotune_clear" (any value) empties the autotune table
+ *   "xform_engine"  centred row / column transforms (okscuda_centred_fft2,
+ *                   okscuda_ifft2, okscuda_ifft1_kz, okscuda_dft_rows engine 0
+ *                   and the column engine's readout pass): 1 (default)
+ *                   register-resident kernels for the lengths with a compile-
+ *                   time plan (128, 192, 256, 320, 368, 384, 512, 640), 0 the
+ *                   shared-memory mixed-radix kernels for every length
+ *   "xform_tile"    register column transform: column pairs per CTA, 0
+ *                   (default: 8, or 4 where 8 do not fit), 2, 4 or 8
  * Any other name returns OKS_EINVAL. */
 int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value);
 /* Autotuner (no reference counterpart): times the plan and launch-shape
@@ -283,6 +292,7 @@ typedef struct {
     uint16_t kspace_encode_step_1;
     uint16_t kspace_encode_step_2;
     uint16_t slice;
+    uint16_t segment;               /* idx.segment: echo of a train (navigator bins) */
     long long data_offset;          /* in complex samples                          */
 } okscuda_acq_header;
 
@@ -313,6 +323,10 @@ typedef struct {
 void okscuda_csrss_default(okscuda_csrss_cfg* cfg);
 /* "cs" (strategy.rs:778-780) */
 const char* okscuda_csrss_name(void);
+/* sizeof(okscuda_acq_header) and sizeof(okscuda_acq_set), for bindings that
+ * mirror the two structs (host only, no device needed). */
+size_t okscuda_acq_header_size(void);
+size_t okscuda_acq_set_size(void);
 /* CsRss::reconstruct (strategy.rs:782-891): calibration, prewhitening,
  * oversampling removal, placement (reader.rs:225-468), kz decoupling,
  * odd-size fallback, per-slice per-coil FISTA, RSS, crop.  Writes the
@@ -320,9 +334,11 @@ const char* okscuda_csrss_name(void);
  * out_cap floats) and its shape to out_dims[3]; h_out == NULL queries the
  * shape only.  When acqs->data_on_device is set, h_out is a device buffer
  * too and the call returns without waiting for the GPU.  OKS_EINVAL mirrors
- * IoError::MissingField (no image acquisitions / zero channels);
- * OKS_ENOTSUP when phase_correct is set and navigator scans are present
- * (navigator phase correction is not part of this library). */
+ * IoError::MissingField (no image acquisitions / zero channels).  With
+ * phase_correct set, phase-correction scans (ACQ_IS_PHASECORR_DATA) are
+ * binned by (slice, segment) and every image line is multiplied by its bin's
+ * unit phasor after prewhitening and before oversampling removal
+ * (phasecorr.rs:61-169, strategy.rs:807-815). */
 int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, const okscuda_acq_set* acqs,
                               float* h_out, long long out_cap, int* out_dims);
 

@@ -79,6 +79,8 @@ SIGNATURES = {
     "okscuda_ifft2": (_i, [_vp, _vp, _c.c_longlong, _i, _i]),
     "okscuda_csrss_default": (None, [_vp]),
     "okscuda_csrss_name": (_c.c_char_p, []),
+    "okscuda_acq_header_size": (_c.c_size_t, []),
+    "okscuda_acq_set_size": (_c.c_size_t, []),
     "okscuda_csrss_reconstruct": (_i, [_vp, _vp, _vp, _vp, _c.c_longlong, _c.POINTER(_i)]),
     "okscuda_profile_enable": (_i, [_vp, _i]),
     "okscuda_profile_read": (_i, [_vp, _c.c_char_p, _i, _c.POINTER(_c.c_double),

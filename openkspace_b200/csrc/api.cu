@@ -77,7 +77,8 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
     } else if (!std::strcmp(name, "mask_bits")) {
         ctx->mask_bits = value != 0;
     } else if (!std::strcmp(name, "occ2d")) {
-        ctx->occ2d = value != 0;
+        if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "occ2d: 0 (1 CTA), 1 (12 warps), 2 (18 warps)");
+        ctx->occ2d = (int)value;
     } else if (!std::strcmp(name, "prefetch2d")) {
         if (value < 0 || value > 3) return set_err(ctx, OKS_EINVAL, "prefetch2d: bit 0 column pass, bit 1 row pass");
         ctx->prefetch2d = (int)value;

@@ -75,7 +75,7 @@ extern "C" int okscuda_autotune(okscuda_ctx* ctx, int kind, int ny, int nx, int 
     } else {
         const long long autochunk = std::max<long long>(1, (96ll << 20) / (4 * N * 8));
         const int chunk_mult[3] = {1, 2, 0};   // x1, x1/2, x1.5 (0 encodes 3/2)
-        for (int occ : {1, 0})
+        for (int occ : {1, 0, 2})
             for (int pf : {1, 0, 3})
                 for (int ns : {2, 3, 1})
                     for (int cm : chunk_mult) {

@@ -47,7 +47,7 @@ struct okscuda_ctx {
     int col_variant = -1;                 // register column engine plan variant (-1: per-length default)
     int persist2d = 1;                    // 2-D register passes: persistent grid
     int mask_bits = 1;                    // 2-D passes: separable masks read as row/column bits
-    int occ2d = 1;                        // 2-D register passes: 1 = launch bounds for 12 warps per SM
+    int occ2d = 1;                        // 2-D register passes: launch bounds for 12 (1) or 18 (2) warps per SM
     int fista2d_streams = 2;              // 2-D engine: chunks in flight at once (forked streams)
     int prefetch2d = 1;                   // 2-D register column pass: pipelined loads (separable masks)
     // per-shape choices found by okscuda_autotune: key (kind, ny, nx), kind 0

@@ -29,4 +29,24 @@ cudaError_t launch_os_remove(const float2* in, float2* out, long long nlines, co
 cudaError_t launch_place(const float2* src, int nc_src, int ns, const PlaceEntry* tab, long long nent, float2* kspace,
                          int nz, int ny, int nx, cudaStream_t st);
 
+// Navigator phase correction (phasecorr.rs:61-169).  A bin is the
+// navigators of one (slice, segment); its scans are entries [first, first +
+// count) of the scan list, each [nc][ns] samples at nav + off.
+struct PcBin {
+    int ns;               // samples per navigator of this bin
+    int first, count;
+    int pad;
+    long long corr;       // offset of the bin's correction vector (ns entries)
+};
+struct PcScan {
+    long long off;
+    int nc, pad;
+};
+// c(k) = conj(avg_k) / |avg_k| of the coil-summed navigators of each bin
+cudaError_t launch_phasecorr_fit(const float2* nav, const PcScan* scans, const PcBin* bins, int nbins, int max_ns,
+                                 float2* corr, cudaStream_t st);
+// data[a][c][k] *= c_bin(a)(k) for k < min(ns, bin ns); scan_bin[a] < 0: untouched
+cudaError_t launch_phasecorr_apply(float2* data, long long nacq, int nc, int ns, const int* scan_bin,
+                                   const PcBin* bins, const float2* corr, cudaStream_t st);
+
 }  // namespace oks

@@ -6,6 +6,8 @@
 //   oversampling.rs:103-155 centred IFFT/crop/FFT          -> k_os_remove
 //   reader.rs:332-457     line placement (first-wins, reverse, centring decided on the host)
 //                                                          -> k_place
+//   phasecorr.rs:61-169   navigator correction vectors / per-line phasor
+//                                                          -> k_phasecorr_fit, k_phasecorr_apply
 #include <cuda_runtime.h>
 #include <float.h>
 
@@ -185,6 +187,76 @@ cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq
     else if (nc <= 32) k_prewhiten_apply<32><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns, status);
     else if (nc <= 64) k_prewhiten_apply<64><<<(unsigned)blocks, 128, 0, st>>>(data, W, nacq, nc, ns, status);
     else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------- navigator phase correction
+// One thread per (bin, sample k), in the reference's FP32 order: each
+// navigator's coil sum sum_c s_c(k) (channels in order), added to the bin in
+// scan order (phasecorr.rs:76-102); then avg = sum * (1 / count) and
+// c(k) = conj(avg) / |avg| with num_complex's division by (|avg|, 0), or 1
+// where |avg| < 1e-20 (phasecorr.rs:106-119).
+__global__ void k_phasecorr_fit(const float2* __restrict__ nav, const PcScan* __restrict__ scans,
+                                const PcBin* __restrict__ bins, float2* __restrict__ corr) {
+    const PcBin b = bins[blockIdx.y];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < b.ns; k += gridDim.x * blockDim.x) {
+        float sr = 0.f, si = 0.f;
+        for (int q = b.first; q < b.first + b.count; ++q) {
+            const PcScan sc = scans[q];
+            float cr = 0.f, ci = 0.f;
+            for (int c = 0; c < sc.nc; ++c) {
+                const float2 v = nav[sc.off + (long long)c * b.ns + k];
+                cr = __fadd_rn(cr, v.x);
+                ci = __fadd_rn(ci, v.y);
+            }
+            sr = __fadd_rn(sr, cr);
+            si = __fadd_rn(si, ci);
+        }
+        const float inv_n = __fdiv_rn(1.f, (float)b.count);
+        const float ar = __fmul_rn(sr, inv_n), ai = __fmul_rn(si, inv_n);
+        const float mag = hypotf(ar, ai);
+        float2 out = make_float2(1.f, 0.f);
+        if (!(mag < 1e-20f)) {
+            const float n2 = __fmul_rn(mag, mag);
+            out = make_float2(__fdiv_rn(__fmul_rn(ar, mag), n2), __fdiv_rn(__fmul_rn(-ai, mag), n2));
+        }
+        corr[b.corr + k] = out;
+    }
+}
+
+// row[k] *= c(k), k < min(ns, len(c)), every channel (phasecorr.rs:141-168)
+__global__ void k_phasecorr_apply(float2* __restrict__ data, long long nacq, int nc, int ns,
+                                  const int* __restrict__ scan_bin, const PcBin* __restrict__ bins,
+                                  const float2* __restrict__ corr) {
+    const long long per = (long long)nc * ns, total = nacq * per;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long a = t / per;
+        const int k = (int)((t - a * per) % ns);
+        const int b = scan_bin[a];
+        if (b < 0) continue;
+        const PcBin bb = bins[b];
+        if (k >= min(ns, bb.ns)) continue;
+        data[t] = cmul(data[t], corr[bb.corr + k]);
+    }
+}
+
+cudaError_t launch_phasecorr_fit(const float2* nav, const PcScan* scans, const PcBin* bins, int nbins, int max_ns,
+                                 float2* corr, cudaStream_t st) {
+    if (nbins <= 0 || max_ns <= 0) return cudaSuccess;
+    if (nbins > 65535) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)((max_ns + 127) / 128), (unsigned)nbins);
+    k_phasecorr_fit<<<grid, 128, 0, st>>>(nav, scans, bins, corr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_phasecorr_apply(float2* data, long long nacq, int nc, int ns, const int* scan_bin,
+                                   const PcBin* bins, const float2* corr, cudaStream_t st) {
+    const long long total = nacq * nc * (long long)ns;
+    if (total <= 0) return cudaSuccess;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_phasecorr_apply<<<(unsigned)blocks, 256, 0, st>>>(data, nacq, nc, ns, scan_bin, bins, corr);
     return cudaGetLastError();
 }
 

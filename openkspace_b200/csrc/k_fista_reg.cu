@@ -547,6 +547,13 @@ constexpr int occ_blocks() {
     constexpr int threads = P::T * (P::T == 32 ? 4 : 1);
     return (12 * 32 + threads - 1) / threads;
 }
+// The 18-warp form (a.occ = 2): a tighter register budget for more resident
+// warps (the 368 column pass compiles without spills at 6 CTAs per SM).
+template <class P>
+constexpr int occ_blocks_hi() {
+    constexpr int threads = P::T * (P::T == 32 ? 4 : 1);
+    return (18 * 32 + threads - 1) / threads;
+}
 
 template <class P, int MINB>
 static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream_t st, int mode, int it, bool row) {
@@ -593,6 +600,7 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
 
 template <class P>
 static cudaError_t launch_2d(const Fista2dArgs& a, long long units, cudaStream_t st, int mode, int it, bool row) {
+    if (a.occ == 2) return launch_2d_k<P, occ_blocks_hi<P>()>(a, units, st, mode, it, row);
     if (a.occ) return launch_2d_k<P, occ_blocks<P>()>(a, units, st, mode, it, row);
     return launch_2d_k<P, 1>(a, units, st, mode, it, row);
 }

@@ -173,7 +173,7 @@ struct Fista2dArgs {
     const float* alpha;
     long long nprob;
     int persist;              // register passes: grid of resident CTAs, units grid-strided
-    int occ;                  // register passes: 0 registers as needed, 1 at least 12 warps per SM
+    int occ;                  // register passes: 0 registers as needed, 1 at least 12 warps per SM, 2 at least 18
     int prefetch;             // register passes: next unit's loads in flight (cp.async); bit 0 column
                               // pass (separable masks), bit 1 row pass
 };

@@ -183,6 +183,8 @@ void okscuda_csrss_default(okscuda_csrss_cfg* cfg) {
 }
 
 const char* okscuda_csrss_name(void) { return "cs"; }
+size_t okscuda_acq_header_size(void) { return sizeof(okscuda_acq_header); }
+size_t okscuda_acq_set_size(void) { return sizeof(okscuda_acq_set); }
 
 int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, const okscuda_acq_set* A,
                               float* h_out, long long out_cap, int* out_dims) {
@@ -238,11 +240,81 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
             }
         }
     }
+    // --- 1b. calibration: navigator scans -> per-(slice, segment) phasors ----
+    // (phasecorr.rs:61-129): bins in order of first appearance; a scan whose
+    // sample count differs from its bin's first scan is dropped
+    std::map<std::pair<int, int>, int> pc_bin_of;
+    std::vector<oks::PcBin> pc_bins;
+    DevBuf dnav(ctx), dcorr(ctx), dpct(ctx);   // navigators, phasors, bin + scan tables
     if (cfg->phase_correct) {
-        for (long long a = 0; a < nacq; ++a)
-            if (H[a].flags & ACQ_IS_PHASECORR_DATA)
-                return set_err(ctx, OKS_ENOTSUP, "navigator phase correction is not part of this library");
+        std::vector<std::vector<long long>> members;
+        for (long long a = 0; a < nacq; ++a) {
+            if (!(H[a].flags & ACQ_IS_PHASECORR_DATA)) continue;
+            const int ns = H[a].number_of_samples, anc = H[a].active_channels;
+            if (ns == 0 || anc == 0) continue;
+            const auto key = std::make_pair((int)H[a].slice, (int)H[a].segment);
+            auto it = pc_bin_of.find(key);
+            if (it == pc_bin_of.end()) {
+                it = pc_bin_of.emplace(key, (int)pc_bins.size()).first;
+                oks::PcBin b{};
+                b.ns = ns;
+                pc_bins.push_back(b);
+                members.emplace_back();
+            }
+            if (pc_bins[it->second].ns != ns) continue;
+            members[it->second].push_back(a);
+        }
+        if (!pc_bins.empty()) {
+            std::vector<oks::PcScan> scans;
+            long long nav_len = 0, corr_len = 0;
+            int max_ns = 0;
+            for (size_t b = 0; b < pc_bins.size(); ++b) {
+                pc_bins[b].first = (int)scans.size();
+                pc_bins[b].count = (int)members[b].size();
+                pc_bins[b].corr = corr_len;
+                corr_len += pc_bins[b].ns;
+                max_ns = std::max(max_ns, pc_bins[b].ns);
+                for (long long a : members[b]) {
+                    oks::PcScan sc{};
+                    sc.off = nav_len;
+                    sc.nc = H[a].active_channels;
+                    scans.push_back(sc);
+                    nav_len += (long long)sc.nc * pc_bins[b].ns;
+                }
+            }
+            OKS_CUDA(dnav.alloc(sizeof(float2) * (size_t)nav_len));
+            OKS_CUDA(dcorr.alloc(sizeof(float2) * (size_t)corr_len));
+            for (size_t b = 0; b < pc_bins.size(); ++b)
+                for (size_t i = 0; i < members[b].size(); ++i) {
+                    const okscuda_acq_header& h = H[members[b][i]];
+                    OKS_CUDA(cudaMemcpyAsync(dnav.as<float2>() + scans[pc_bins[b].first + i].off, A->data + h.data_offset,
+                                             sizeof(float2) * (size_t)h.active_channels * h.number_of_samples, copy_kind,
+                                             ctx->stream));
+                }
+            // bins then scans, through a staging slot into memory this call owns
+            std::vector<unsigned char> tab(sizeof(oks::PcBin) * pc_bins.size() + sizeof(oks::PcScan) * scans.size());
+            std::memcpy(tab.data(), pc_bins.data(), sizeof(oks::PcBin) * pc_bins.size());
+            std::memcpy(tab.data() + sizeof(oks::PcBin) * pc_bins.size(), scans.data(), sizeof(oks::PcScan) * scans.size());
+            OKS_CUDA(dpct.alloc(tab.size()));
+            oks::Staging::Slot* slot = nullptr;
+            int rc = stage_upload(ctx, tab.data(), tab.size(), &slot);
+            if (rc) return rc;
+            OKS_CUDA(cudaMemcpyAsync(dpct.p, slot->dev, tab.size(), cudaMemcpyDeviceToDevice, ctx->stream));
+            stage_release(ctx, slot);
+            const auto* dbins = dpct.as<oks::PcBin>();
+            const auto* dscans = reinterpret_cast<const oks::PcScan*>(dbins + pc_bins.size());
+            ProfScope ps(ctx, "k_phasecorr_fit");
+            OKS_CUDA(oks::launch_phasecorr_fit(dnav.as<float2>(), dscans, dbins, (int)pc_bins.size(), max_ns,
+                                               dcorr.as<float2>(), ctx->stream));
+        }
     }
+    // bin of an image line: (slice, segment), else (u16::MAX, segment) (phasecorr.rs:145-153)
+    auto pc_bin = [&](const okscuda_acq_header& h) {
+        if (pc_bins.empty()) return -1;
+        auto it = pc_bin_of.find({(int)h.slice, (int)h.segment});
+        if (it == pc_bin_of.end()) it = pc_bin_of.find({65535, (int)h.segment});
+        return it == pc_bin_of.end() ? -1 : it->second;
+    };
     const bool os_on = cfg->remove_oversampling && os_ratio_ok(A->enc_x, A->rec_x);
 
     // --- 2. first pass over image scans: tensor shape (reader.rs:234-290) ----
@@ -312,6 +384,29 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
             ProfScope ps(ctx, "k_prewhiten_apply");
             OKS_CUDA(oks::launch_prewhiten_apply(raw.as<float2>(), dW.as<float2>(), ng, gnc, gns, ctx->stream,
                                                  dWstat.as<int>()));
+        }
+        // navigator phasors (phasecorr.rs:141-168), before oversampling removal
+        if (!pc_bins.empty()) {
+            std::vector<int> sb(ng);
+            bool any = false;
+            for (long long i = 0; i < ng; ++i) {
+                sb[i] = pc_bin(H[ids[i]]);
+                any = any || sb[i] >= 0;
+            }
+            if (any) {
+                oks::Staging::Slot* slot = nullptr;
+                int rc = stage_upload(ctx, sb.data(), sizeof(int) * sb.size(), &slot);
+                if (rc) return rc;
+                cudaError_t e;
+                {
+                    ProfScope ps(ctx, "k_phasecorr_apply");
+                    e = oks::launch_phasecorr_apply(raw.as<float2>(), ng, gnc, gns, static_cast<const int*>(slot->dev),
+                                                    dpct.as<oks::PcBin>(), dcorr.as<float2>(),
+                                                    ctx->stream);
+                }
+                stage_release(ctx, slot);
+                if (e != cudaSuccess) return cuda_err(ctx, e, "phase correction");
+            }
         }
         int pns = gns;
         DevBuf os(ctx);

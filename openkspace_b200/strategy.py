@@ -25,8 +25,8 @@ ACQ_IS_PHASECORR_DATA = 1 << 23
 HEADER_DTYPE = np.dtype([("flags", "<u8"), ("number_of_samples", "<u2"), ("active_channels", "<u2"),
                          ("discard_pre", "<u2"), ("discard_post", "<u2"), ("center_sample", "<u2"),
                          ("kspace_encode_step_1", "<u2"), ("kspace_encode_step_2", "<u2"), ("slice", "<u2"),
-                         ("data_offset", "<i8")])
-assert HEADER_DTYPE.itemsize == 32
+                         ("segment", "<u2"), ("data_offset", "<i8")], align=True)
+assert HEADER_DTYPE.itemsize == 40 and HEADER_DTYPE.fields["data_offset"][1] == 32
 
 
 class _AcqSet(ctypes.Structure):

@@ -293,6 +293,53 @@ def prewhiten_apply(w: np.ndarray, data: np.ndarray) -> np.ndarray:
 
 
 # --------------------------------------------------------------------------
+# phasecorr.rs
+# --------------------------------------------------------------------------
+def phase_corrector_from_acqs(scans):
+    """phasecorr.rs:61-129.  ``scans``: the phase-correction acquisitions in
+    file order as (slice, segment, [nc, ns] array).  Bins by (slice, segment):
+    the coil sum of each scan (channel order) is added to its bin in scan
+    order; a scan whose ns differs from the bin's first scan is dropped, scans
+    with no samples or channels are skipped.  Returns {(slice, segment):
+    c(k) = conj(avg) / |avg|, or 1 where |avg| < 1e-20}."""
+    bins = {}
+    for sl, seg, d in scans:
+        d = np.asarray(d, dtype=np.complex128)
+        nc, ns = d.shape
+        if ns == 0 or nc == 0:
+            continue
+        coil_sum = d.sum(axis=0)
+        key = (int(sl), int(seg))
+        if key not in bins:
+            bins[key] = [np.zeros(ns, np.complex128), 0]
+        if bins[key][0].shape[0] != ns:
+            continue
+        bins[key][0] = bins[key][0] + coil_sum
+        bins[key][1] += 1
+    out = {}
+    for key, (total, count) in bins.items():
+        avg = total * (1.0 / count)
+        mag = np.abs(avg)
+        out[key] = np.where(mag < 1e-20, 1.0 + 0j, np.conj(avg) / np.where(mag < 1e-20, 1.0, mag))
+    return out
+
+
+def phase_correct_apply(corr, data, slice_, segment):
+    """phasecorr.rs:141-168: multiply the first min(ns, len(c)) samples of
+    every channel by the phasor of (slice, segment), else of (65535, segment),
+    else leave the line untouched."""
+    c = corr.get((int(slice_), int(segment)))
+    if c is None:
+        c = corr.get((65535, int(segment)))
+    d = np.asarray(data, dtype=np.complex128).copy()
+    if c is None:
+        return d
+    n = min(d.shape[-1], c.shape[0])
+    d[..., :n] *= c[:n]
+    return d
+
+
+# --------------------------------------------------------------------------
 # oversampling.rs
 # --------------------------------------------------------------------------
 def oversampling_ratio(encoded_x: int, recon_x: int):

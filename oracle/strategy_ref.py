@@ -13,6 +13,7 @@ from oracle import cs_fp64 as o64
 
 NOISE = 1 << 18
 REVERSE = 1 << 21
+PHASECORR = 1 << 23
 NON_IMAGE = (1 << 18) | (1 << 23) | (1 << 22) | (1 << 27) | (1 << 25) | (1 << 26) | (1 << 28)
 
 
@@ -72,15 +73,23 @@ def read_kspace_with_mask(headers, data, encoded, ky_center, kz_center, preproce
 
 
 def csrss_reconstruct(headers, data, encoded, recon, ky_center, kz_center=0, iters=60, lam=0.01,
-                      remove_oversampling=True, prewhiten=True, fft_mode="auto", crop=True):
+                      remove_oversampling=True, prewhiten=True, fft_mode="auto", crop=True, phase_correct=True):
     noise = [_acq(headers, data, i) for i in range(len(headers)) if int(headers[i]["flags"]) & NOISE]
     w = o64.prewhitener_from_noise(noise) if prewhiten else None
+    pc = {}
+    if phase_correct:                                   # strategy.rs:790-794
+        pc = o64.phase_corrector_from_acqs(
+            [(int(headers[i]["slice"]), int(headers[i]["segment"]), _acq(headers, data, i))
+             for i in range(len(headers)) if (int(headers[i]["flags"]) & NOISE) == 0
+             and int(headers[i]["flags"]) & PHASECORR])
     enc_x, rec_x = encoded[0], recon[0]
     os_ok = remove_oversampling and o64.oversampling_ratio(enc_x, rec_x) is not None
 
     def preprocess(d, h):
         if w is not None and d.shape[0] == w.shape[0]:
             d = o64.prewhiten_apply(w, d)               # prewhiten.rs:118-142
+        if pc:
+            d = o64.phase_correct_apply(pc, d, h["slice"], h["segment"])   # phasecorr.rs:141-168
         if os_ok and d.shape[1] == enc_x:
             d = o64.oversampling_apply(d, enc_x, rec_x)  # oversampling.rs:103-155
             h["center_sample"] = rec_x // 2

@@ -38,3 +38,12 @@ def test_null_context_is_einval():
     L = _lib.load()
     assert L.okscuda_synchronize(None) == _lib.OKS_EINVAL
     assert L.okscuda_fista_cs(None, None, None, 1, 8, 8, 1, 0.01, None) == _lib.OKS_EINVAL
+
+
+def test_acquisition_structs_match_the_python_mirror():
+    """okscuda_acq_header / okscuda_acq_set as laid out by the compiler equal
+    the numpy dtype and ctypes struct the Python host side passes."""
+    from openkspace_b200.strategy import HEADER_DTYPE, _AcqSet
+    L = _lib.load()
+    assert L.okscuda_acq_header_size() == HEADER_DTYPE.itemsize == 40
+    assert L.okscuda_acq_set_size() == ctypes.sizeof(_AcqSet)

@@ -121,7 +121,9 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
              dict(mask_bits=1, occ2d=0, persist2d=0, fista2d_streams=1, fista2d_chunk=2),
              dict(mask_bits=1, occ2d=1, persist2d=0, fista2d_streams=3, fista2d_chunk=1),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=0),
-             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=3)]
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=3),
+             dict(mask_bits=1, occ2d=2, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=1),
+             dict(mask_bits=1, occ2d=2, persist2d=1, fista2d_streams=1, fista2d_chunk=2, prefetch2d=3)]
     default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0, prefetch2d=1)
     results = []
     try:

@@ -288,3 +288,48 @@ def test_csrss_threads_agree(rng):
     assert np.array_equal(r1, r4)
     r64 = o64.csrss_from_kspace(k, m, 20, 0.01)
     assert rel_l2(r1, r64) < 1e-5
+
+
+# ------------------------------------------------------------ phasecorr.rs
+def test_phasecorr_empty_corrector_is_noop():
+    """phasecorr.rs:189-196: no navigators, the line is unchanged."""
+    corr = o64.phase_corrector_from_acqs([])
+    assert corr == {}
+    d = np.array([[1.0 + 2.0j]])
+    assert np.array_equal(o64.phase_correct_apply(corr, d, 0, 0), d)
+
+
+def test_phasecorr_removes_constant_phase_offset():
+    """phasecorr.rs:198-228: a navigator at a constant phase pi/3 makes an
+    image line carrying the same phase on a real ramp real again."""
+    ns, phi = 8, np.pi / 3
+    nav = np.full((1, ns), np.exp(1j * phi))
+    corr = o64.phase_corrector_from_acqs([(0, 0, nav)])
+    assert set(corr) == {(0, 0)}
+    img = (np.exp(1j * phi) * np.arange(1, ns + 1))[None]
+    got = o64.phase_correct_apply(corr, img, 0, 0)
+    assert np.all(np.abs(got.real - np.arange(1, ns + 1)) < 1e-4) and np.all(np.abs(got.imag) < 1e-4)
+
+
+def test_phasecorr_binning_rules():
+    """phasecorr.rs:70-103, 141-168: coil sums averaged per (slice, segment);
+    a scan with another ns is dropped; empty scans are skipped; a line takes
+    its (slice, segment) bin, else (65535, segment), else stays as it is; only
+    the first min(ns, len(c)) samples are corrected; |avg| < 1e-20 gives 1."""
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal((2, 6)) + 1j * rng.standard_normal((2, 6))
+    b = rng.standard_normal((3, 6)) + 1j * rng.standard_normal((3, 6))
+    odd = rng.standard_normal((2, 5)) + 1j * rng.standard_normal((2, 5))
+    fall = rng.standard_normal((1, 4)) + 1j * rng.standard_normal((1, 4))
+    zero = np.zeros((1, 6), complex)
+    corr = o64.phase_corrector_from_acqs([(0, 1, a), (0, 1, odd), (0, 1, b), (0, 2, np.zeros((0, 6))),
+                                          (65535, 3, fall), (1, 1, zero)])
+    avg = (a.sum(0) + b.sum(0)) / 2
+    assert np.allclose(corr[(0, 1)], np.conj(avg) / np.abs(avg))
+    assert (0, 2) not in corr
+    assert np.array_equal(corr[(1, 1)], np.ones(6, complex))
+    line = rng.standard_normal((2, 6)) + 1j * rng.standard_normal((2, 6))
+    assert np.allclose(o64.phase_correct_apply(corr, line, 0, 1), line * corr[(0, 1)])
+    got = o64.phase_correct_apply(corr, line, 5, 3)          # slice 5 has no bin: the (65535, 3) one
+    assert np.allclose(got[:, :4], line[:, :4] * corr[(65535, 3)]) and np.array_equal(got[:, 4:], line[:, 4:])
+    assert np.array_equal(o64.phase_correct_apply(corr, line, 0, 7), line)
