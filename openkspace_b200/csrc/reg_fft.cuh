@@ -203,13 +203,16 @@ __device__ __forceinline__ void odd_pairs_for(int s, const float2* a, const floa
 
 // One stage over smem for intermediate stages: items f = t + TA*b, both
 // columns, any radix.  src/dst are padded exchange buffers.
-template <class P, int SIGN, int R, int p>
+// PRE: the inputs already carry this stage's twiddles (the previous stage
+// applied them as it stored, once per element; only for the split form).
+template <class P, int SIGN, int R, int p, bool PRE = false>
 __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float2* __restrict__ dst,
                                            const float2* __restrict__ tw, const float2* __restrict__ roots, int t) {
     constexpr int NB = P::N / R;
     constexpr int ITEMS = 2 * NB;
     constexpr bool BIG_ODD = (R % 2 == 1 && R > 5);
     constexpr int NS = BIG_ODD ? P::T / ITEMS : 1;   // threads sharing one butterfly
+    static_assert(!PRE || NS >= 2, "pre-twiddled inputs are for the split odd-radix form");
     if constexpr (NS >= 2) {
         // Fewer butterflies than threads: NS threads share each one.  All of
         // them fold the inputs (a_j, b_j); thread s of the group forms the
@@ -229,7 +232,7 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
         for (int j = 1; j <= H; ++j) {
             float2 u = src[padi(2 * (i + j * NB) + c)];
             float2 w = src[padi(2 * (i + (R - j) * NB) + c)];
-            if (p > 1) {
+            if (p > 1 && !PRE) {
                 u = twmul<SIGN>(u, tw[k * (R - 1) + j - 1]);
                 w = twmul<SIGN>(w, tw[k * (R - 1) + R - j - 1]);
             }
@@ -302,9 +305,15 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
 
 // A stage whose inputs are the thread's registers (w[b + j*E/R]); writes its
 // outputs to smem (exchange) or, when p*R == N, back into w in place.
-template <class P, int SIGN, int R, int p>
+// R2 > 0: the next stage (radix R2, P2 = p R) is the split odd-radix form;
+// each output o = i2 + j2 N/R2 is stored already multiplied by that stage's
+// twiddle w^(j2 k2), k2 = i2 mod P2 (tw2: its table), so the NS threads
+// sharing a butterfly there do not each repeat the 2 (R2 - 1) products.  The
+// products are the same, so the results are bit-identical.
+template <class P, int SIGN, int R, int p, int R2 = 0, int P2 = 0>
 __device__ __forceinline__ void stage_reg(float2* w, float2* __restrict__ dst, const float2* __restrict__ tw,
-                                          const float2* __restrict__ roots, int t) {
+                                          const float2* __restrict__ roots, int t,
+                                          const float2* __restrict__ tw2 = nullptr) {
     constexpr int BR = P::E / R;   // butterflies per thread
     constexpr bool LAST = (p * R == P::N);
     if (P::TA != P::T && t >= P::TA) return;
@@ -327,7 +336,16 @@ __device__ __forceinline__ void stage_reg(float2* w, float2* __restrict__ dst, c
         } else {
             const int ob = (i - k) * R + k;
 #pragma unroll
-            for (int j = 0; j < R; ++j) dst[padi(2 * (ob + j * p) + c)] = v[j];
+            for (int j = 0; j < R; ++j) {
+                float2 y = v[j];
+                if constexpr (R2 > 0) {
+                    constexpr int NB2 = P::N / R2;
+                    const int o = ob + j * p;
+                    const int j2 = o / NB2, k2 = (o - j2 * NB2) % P2;
+                    if (j2 > 0 && k2 > 0) y = twmul<SIGN>(y, tw2[k2 * (R2 - 1) + j2 - 1]);
+                }
+                dst[padi(2 * (ob + j * p) + c)] = y;
+            }
         }
     }
 }
@@ -355,6 +373,13 @@ __device__ __forceinline__ void stage_to_reg(const float2* __restrict__ src, flo
 #pragma unroll
         for (int j = 0; j < R; ++j) w[b + j * BR] = v[j];
     }
+}
+
+// True when a middle stage of radix R runs in the split odd-radix form (the
+// plan has fewer of its butterflies than threads).
+template <class P, int R>
+constexpr bool split_odd_stage() {
+    return R % 2 == 1 && R > 5 && P::T / (2 * (P::N / R)) >= 2;
 }
 
 // Barrier of one thread group.  NB (named barriers): groups of T >= 64
@@ -385,7 +410,8 @@ __device__ __forceinline__ void fwd_rest(float2* w, float2* A, float2* B, const 
         if constexpr (s == P::S - 1) {
             stage_to_reg<P, -1, R, p>(src, w, tw + off, roots, t);
         } else {
-            stage_smem<P, -1, R, p>(src, dst, tw + off, roots, t);
+            constexpr bool PRE = s == 1 && split_odd_stage<P, R>();   // twiddled by stage 0's stores
+            stage_smem<P, -1, R, p, PRE>(src, dst, tw + off, roots, t);
             group_sync<P, NB>();
             fwd_rest<P, s + 1, NB>(w, A, B, tw, roots, t);
         }
@@ -399,7 +425,10 @@ __device__ __forceinline__ void forward(float2* w, float2* A, float2* B, const f
     if constexpr (P::S == 1) {
         stage_reg<P, -1, R0, 1>(w, nullptr, tw, roots, t);
     } else {
-        stage_reg<P, -1, R0, 1>(w, A, tw, roots, t);   // outputs to A
+        if constexpr (P::S >= 3 && split_odd_stage<P, P::R[1]>())
+            stage_reg<P, -1, R0, 1, P::R[1], R0>(w, A, tw, roots, t, tw + Tw<P>::fwd(1));
+        else
+            stage_reg<P, -1, R0, 1>(w, A, tw, roots, t);   // outputs to A
         group_sync<P, NB>();
         fwd_rest<P, 1, NB>(w, A, B, tw, roots, t);
     }
@@ -418,7 +447,8 @@ __device__ __forceinline__ void inv_rest(float2* w, float2* A, float2* B, const 
         if constexpr (s == P::S - 1) {
             stage_to_reg<P, +1, R, p>(src, w, tw + off, roots, t);
         } else {
-            stage_smem<P, +1, R, p>(src, dst, tw + off, roots, t);
+            constexpr bool PRE = s == 1 && split_odd_stage<P, R>();   // twiddled by stage 0's stores
+            stage_smem<P, +1, R, p, PRE>(src, dst, tw + off, roots, t);
             group_sync<P, NB>();
             inv_rest<P, s + 1, NB>(w, A, B, tw, roots, t);
         }
@@ -432,7 +462,10 @@ __device__ __forceinline__ void inverse(float2* w, float2* A, float2* B, const f
     if constexpr (P::S == 1) {
         stage_reg<P, +1, R0, 1>(w, nullptr, tw + Tw<P>::inv(0), roots, t);
     } else {
-        stage_reg<P, +1, R0, 1>(w, A, tw + Tw<P>::inv(0), roots, t);
+        if constexpr (P::S >= 3 && split_odd_stage<P, P::R[P::S - 2]>())
+            stage_reg<P, +1, R0, 1, P::R[P::S - 2], R0>(w, A, tw + Tw<P>::inv(0), roots, t, tw + Tw<P>::inv(1));
+        else
+            stage_reg<P, +1, R0, 1>(w, A, tw + Tw<P>::inv(0), roots, t);
         group_sync<P, NB>();
         inv_rest<P, 1, NB>(w, A, B, tw, roots, t);
     }
