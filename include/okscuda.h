@@ -94,6 +94,12 @@ const char* okscuda_version(void);
  *                   shared-memory mixed-radix kernels for every length
  *   "xform_tile"    register column transform: column pairs per CTA, 0
  *                   (default: 8, or 4 where 8 do not fit), 2, 4 or 8
+ *   "xform_lanes"   register column transform with the lanes across the
+ *                   columns (whole row segments straight from and to global
+ *                   memory): 0 (default) for the lengths where it is faster
+ *                   (192, 256, 320, 512), 1-4 a (columns, threads per column)
+ *                   form (16,32) (16,64) (8,64) (8,32) for every length but 368,
+ *                   -1 never
  * Any other name returns OKS_EINVAL. */
 int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value);
 /* Autotuner (no reference counterpart): times the plan and launch-shape

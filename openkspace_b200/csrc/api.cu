@@ -103,6 +103,9 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value != 0 && value != 2 && value != 4 && value != 8)
             return set_err(ctx, OKS_EINVAL, "xform_tile: 0 (by length), 2, 4 or 8 column pairs");
         ctx->xform_tile = (int)value;
+    } else if (!std::strcmp(name, "xform_lanes")) {
+        if (value < -1 || value > 4) return set_err(ctx, OKS_EINVAL, "xform_lanes: -1 off, 0 by length, 1 to 4");
+        ctx->xform_lanes = (int)value;
     } else if (!std::strcmp(name, "fista2d_streams")) {
         if (value < 1 || value > 8) return set_err(ctx, OKS_EINVAL, "fista2d_streams: 1 to 8");
         ctx->fista2d_streams = (int)value;
@@ -203,7 +206,7 @@ int okscuda_centred_fft2(okscuda_ctx* ctx, okscuda_c64* d_data, int batch, int n
         OKS_CUDA(oks::launch_row_xform(ra, *px, ctx->stream));
     }
     oks::ColXformArgs ca{};
-    ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile;
+    ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile; ca.lanes = ctx->xform_lanes;
     ca.data = d; ca.nprob = batch; ca.ny = ny; ca.nx = nx; ca.prob_stride = (long long)ny * nx;
     ca.sign = inverse ? +1 : -1; ca.centred = 1;
     ca.scale = 1.0f / std::sqrt((float)ny * (float)nx);

@@ -79,6 +79,7 @@ struct okscuda_ctx {
     int row_engine = 0;                   // 2-D engine row pass: 0 SIMT FFT, 1 tensor-core DFT
     int xform_reg = 1;                    // row/column transforms: 1 register kernels where a plan exists
     int xform_tile = 0;                   // column pairs per CTA of the register column transform (0: by length)
+    int xform_lanes = 0;                  // lanes-across-columns form of it: 0 by length, 1..4, -1 off
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)
     cudaEvent_t fork_ev = nullptr;

@@ -232,6 +232,106 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
     cp_async_wait_all();
 }
 
+// ------------------------------------------------ columns across the lanes
+// Column transform with the lanes running across CW adjacent columns: thread
+// (c, tc) = (tid % CW, tid / CW) owns column x0 + c and the butterflies
+// b = tc, tc + TPC, ... of every stage.  A half-warp (CW = 16) touches one
+// row of 16 columns at a time, so stage 0 reads and the last stage writes
+// whole 128-byte row segments straight from and to global memory, and the
+// middle stages work in place on one [N][CW] shared-memory tile (each thread
+// reads all its butterflies' inputs before the barrier that precedes the
+// writes).  Twiddles depend on the row only: one broadcast per half-warp.
+template <class P, int SIGN, int CW, int TPC, int s>
+__device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2* __restrict__ TW,
+                                            const float2* __restrict__ RT, float2* __restrict__ col, int nx,
+                                            bool on, bool centred, float sc, int c, int tc) {
+    constexpr int S = P::S, N = P::N;
+    constexpr int R = SIGN < 0 ? P::R[s] : P::R[S - 1 - s];
+    constexpr int p = SIGN < 0 ? P::prod(s) : P::rprod(s);
+    constexpr int off = SIGN < 0 ? Tw<P>::fwd(s) : Tw<P>::inv(s);
+    constexpr int NB = N / R;
+    constexpr int BPT = (NB + TPC - 1) / TPC;   // butterflies per thread
+    float2 v[BPT][R];
+#pragma unroll
+    for (int bb = 0; bb < BPT; ++bb) {
+        const int b = tc + TPC * bb;
+        if (NB % TPC != 0 && b >= NB) break;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const int r = b + j * NB;
+            if constexpr (s == 0) {
+                float2 x = on ? col[r * nx] : make_float2(0.f, 0.f);   // N nx < 2^31 (launcher)
+                if (centred && (r & 1)) x = make_float2(-x.x, -x.y);
+                v[bb][j] = x;
+            } else {
+                v[bb][j] = D[r * CW + c];
+            }
+        }
+    }
+    if constexpr (s > 0 && s < S - 1) __syncthreads();   // in place: all inputs read before any output lands
+#pragma unroll
+    for (int bb = 0; bb < BPT; ++bb) {
+        const int b = tc + TPC * bb;
+        if (NB % TPC != 0 && b >= NB) break;
+        const int k = b % p;
+        if (p > 1) {
+#pragma unroll
+            for (int j = 1; j < R; ++j) v[bb][j] = twmul<SIGN>(v[bb][j], TW[off + k * (R - 1) + j - 1]);
+        }
+        bfly<SIGN, R>(v[bb], RT);
+        const int ob = (b - k) * R + k;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const int o = ob + j * p;
+            if constexpr (s == S - 1) {
+                if (on) col[o * nx] = v[bb][j] * ((centred && (o & 1)) ? -sc : sc);
+            } else {
+                D[o * CW + c] = v[bb][j];
+            }
+        }
+    }
+    if constexpr (s < S - 1) {
+        __syncthreads();
+        lanes_stage<P, SIGN, CW, TPC, s + 1>(D, TW, RT, col, nx, on, centred, sc, c, tc);
+    }
+}
+
+// Register budget of the lanes form: 64, or 96 where a stage keeps more than
+// 8 values per thread (radix 16, or two radix-8 butterflies).
+template <class P, int TPC>
+constexpr int lanes_regs() {
+    int most = 0;
+    for (int s = 0; s < P::S; ++s) {
+        const int v = (P::N / P::R[s] + TPC - 1) / TPC * P::R[s];
+        most = v > most ? v : most;
+    }
+    return most > 8 ? 96 : 64;
+}
+
+template <class P, int SIGN, int CW, int TPC>
+__global__ void __launch_bounds__(CW * TPC, xform_min_blocks<CW * TPC, lanes_regs<P, TPC>()>())
+k_col_lanes(ColXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
+    constexpr int N = P::N;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* D = sm;                                  // [N][CW]
+    float2* TWs = sm + N * CW;
+    float2* RT = TWs + tw_half<P>();
+    const float2* TW = load_twiddles<P, SIGN>(TWs, gtw);
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    const int c = threadIdx.x % CW, tc = threadIdx.x / CW;
+    const int ntx = (a.nx + CW - 1) / CW;
+    const long long total = a.nprob * ntx;
+    const float sc_n2 = (a.centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    for (long long u = blockIdx.x; u < total; u += gridDim.x) {
+        const long long pr = u / ntx;
+        const int x = (int)(u - pr * ntx) * CW + c;
+        const bool on = x < a.nx;
+        float2* col = a.data + pr * a.prob_stride + (on ? x : 0);
+        __syncthreads();                             // tables loaded; the last tile's final stage has read D
+        lanes_stage<P, SIGN, CW, TPC, 0>(D, TW, RT, col, (int)a.nx, on, a.centred != 0, sc_n2, c, tc);
+    }
+}
+
 // Resident CTAs per SM of a kernel at a dynamic shared-memory size, queried
 // once per (kernel, size) and device.
 static int ctas_per_sm(const void* fn, int threads, size_t smem) {
@@ -300,10 +400,56 @@ static cudaError_t col_pg(const ColXformArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <class P, int CW, int TPC>
+static cudaError_t col_lanes_k(const ColXformArgs& a, cudaStream_t st) {
+    const float2 *tw, *rt;
+    int nrt;
+    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)P::N * CW + tw_half<P>() + nrt);
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_col_lanes<P, -1, CW, TPC>)
+                                : reinterpret_cast<const void*>(k_col_lanes<P, +1, CW, TPC>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = a.nprob * ((a.nx + CW - 1) / CW);
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, CW * TPC, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    if (a.sign < 0) k_col_lanes<P, -1, CW, TPC><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw, rt, nrt);
+    else k_col_lanes<P, +1, CW, TPC><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw, rt, nrt);
+    return cudaGetLastError();
+}
+
+// Lanes form per column length, from B200 measurements of both column
+// kernels on 1 GiB of planes (GB/s, lanes form / tiles): 192 4361 / 3404,
+// 256 4863 / 4587, 320 3526 / 3224, 512 4206 / 4177; the tiles stay ahead at
+// 128 (5043 / 3907), 384 (4108 / 3788) and 640 (3706 / 2819).
+template <class P>
+constexpr int lanes_default() {
+    return P::N == 256 ? 1 : (P::N == 192 || P::N == 320 || P::N == 512) ? 4 : 0;
+}
+
+// Columns across the lanes: tile width CW and threads per column TPC
+// (lanes 1..4: (16, 32), (16, 64), (8, 64), (8, 32)).
+template <class P>
+static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) {
+    switch (lanes) {
+        case 2: return col_lanes_k<P, 16, 64>(a, st);
+        case 3: return col_lanes_k<P, 8, 64>(a, st);
+        case 4: return col_lanes_k<P, 8, 32>(a, st);
+        default: return col_lanes_k<P, 16, 32>(a, st);
+    }
+}
+
 // Column pairs per tile: 8 (128-byte row segments) where 8 groups fit one
 // CTA (1024 threads, 64 registers each) and one SM's shared memory, else 4.
 template <class P>
 static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
+    if constexpr (!big_odd_plan<P>()) {
+        // columns across the lanes (in-problem offsets in 32 bits) where that
+        // form measured faster than the tiles: 192, 256, 320, 512
+        const int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
+        if (a.tile == 0 && lanes > 0 && (long long)P::N * a.nx < (1ll << 31)) return col_lanes<P>(a, lanes, st);
+    }
     constexpr bool g8 = P::N <= 512 && P::T * 8 <= 1024 && !big_odd_plan<P>();
     int g = a.tile > 0 ? a.tile : (g8 ? 8 : 4);
     if (g >= 8 && P::N > 512) g = 4;

@@ -78,6 +78,7 @@ struct ColXformArgs {
     float scale;
     int reg = 1;         // register-resident kernel where a plan of length ny exists
     int tile = 0;        // column pairs per CTA of that kernel (0: by length; 2, 4, 8)
+    int lanes = 0;       // lanes-across-columns form: 0 by length, 1..4 a (width, threads) choice, -1 off
 };
 cudaError_t launch_col_xform(const ColXformArgs& a, const DevPlan& pl, cudaStream_t st);
 

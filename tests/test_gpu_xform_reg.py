@@ -76,6 +76,21 @@ def test_column_tile_widths(ctx, rng, tile, ny):
     assert rel_l2(got, want) < TOL
 
 
+@pytest.mark.parametrize("lanes", [-1, 1, 2, 3, 4])
+@pytest.mark.parametrize("n", LENGTHS)
+def test_column_lanes_forms(ctx, rng, n, lanes):
+    """Every (tile width, threads per column) form of the lanes-across-columns
+    kernel, and the tiles (lanes -1), on ragged column counts."""
+    x = crandn(rng, (2, n, 38 if n != 368 else 20))
+    want = o64.centred_ifft2(x)
+    ctx.set_option("xform_lanes", lanes)
+    try:
+        got = ctx.centred_fft2(x, True)
+    finally:
+        ctx.set_option("xform_lanes", 0)
+    assert rel_l2(got, want) < TOL
+
+
 @pytest.mark.parametrize("rows,n", [(1, 640), (301, 368), (7, 128), (1001, 320), (64, 512)])
 @pytest.mark.parametrize("inverse,centred", [(0, 1), (1, 1), (0, 0), (1, 0)])
 def test_rows_odd_counts_and_uncentred(ctx, rng, rows, n, inverse, centred):
