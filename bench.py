@@ -17,7 +17,8 @@ A step is one pass of the hot path over one batch of synthetic input:
              CsRss 3-D path (kz IFFT, 192 x 32 slice solves, RSS)
   served     Poisson arrivals through the request server beside the plain drop-in
   fft        the centred 2-D FFT alone: 1024 coil planes of 368 x 640 in place
-             (the row and column transform kernels; metric planes/s)
+             (the row and column transform kernels; metric planes/s);
+             --fft-shape NYxNX another plane shape at the same bytes per step
 value = slices/s with inputs resident in HBM; e2e = the same through the
 public API with pinned host buffers copied in and the result copied out inside
 the timed region.  Multi-GPU: one process per GPU, every rank solves its own
@@ -634,6 +635,8 @@ def main():
     ap.add_argument("--row-engine", default="simt", choices=["simt", "tc"],
                     help="2-D-mask engine readout transforms: FP32 SIMT FFT or tcgen05 3xBF16 DFT")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fft-shape", default="368x640",
+                    help="fft workloads: plane shape NYxNX (the column pass runs length NY, the row pass NX)")
     ap.add_argument("--no-extras", action="store_true",
                     help="precision: skip the short tensor-core and serving side measurements")
     ap.add_argument("--rates", default="50,200,800", help="served: Poisson arrival rates (req/s)")
@@ -650,6 +653,9 @@ def main():
             run_serving(args)
         return
     wl = WORKLOADS[args.workload]()
+    if wl.name == "fft":
+        ny, nx = (int(v) for v in args.fft_shape.lower().split("x"))
+        wl = FftWorkload(max(1, wl.nplanes * 368 * 640 // (ny * nx)), ny, nx)   # same bytes per step
 
     if args.impl == "reference":
         run_reference(args, wl, rank)
