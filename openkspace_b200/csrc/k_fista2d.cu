@@ -20,12 +20,6 @@
 
 namespace oks {
 
-__device__ __forceinline__ float2 shrink2d(float2 c, float lam) {
-    const float m = sqrtf(c.x * c.x + c.y * c.y);   // wavelet.rs:90 |z| (norm)
-    if (m <= lam) return make_float2(0.f, 0.f);
-    return c * ((m - lam) / m);
-}
-
 __device__ __forceinline__ float ysign(int r, int x) { return ((r + x) & 1) ? -1.f : 1.f; }
 
 // ------------------------------------------------------------ column pass
@@ -147,9 +141,9 @@ __global__ void k2d_row(Fista2dArgs a, FftPlan pl, const float2* __restrict__ gt
             float2 pll = (s0 + s1) * 0.5f, phl = (d0 + d1) * 0.5f;
             float2 plh = (s0 - s1) * 0.5f, phh = (d0 - d1) * 0.5f;
             // phh is the LL band of the demodulated image: left untouched
-            pll = shrink2d(pll, lam);
-            phl = shrink2d(phl, lam);
-            plh = shrink2d(plh, lam);
+            pll = shrink_c(pll, lam);
+            phl = shrink_c(phl, lam);
+            plh = shrink_c(plh, lam);
             const float2 t0 = pll + plh, t1 = phl + phh, t2 = pll - plh, t3 = phl - phh;
             const float2 xa = (t0 + t1) * 0.5f, xb = (t0 - t1) * 0.5f;
             const float2 xd = (t2 + t3) * 0.5f, xe = (t2 - t3) * 0.5f;
@@ -208,9 +202,9 @@ __global__ void k2d_prox(Fista2dArgs a, const float2* __restrict__ W, int mode, 
         float2 pll = (s0 + s1) * 0.5f, phl = (d0 + d1) * 0.5f;
         float2 plh = (s0 - s1) * 0.5f, phh = (d0 - d1) * 0.5f;
         // phh is the LL band of the demodulated image: left untouched
-        pll = shrink2d(pll, lam);
-        phl = shrink2d(phl, lam);
-        plh = shrink2d(plh, lam);
+        pll = shrink_c(pll, lam);
+        phl = shrink_c(phl, lam);
+        plh = shrink_c(plh, lam);
         const float2 t0 = pll + plh, t1 = phl + phh, t2 = pll - plh, t3 = phl - phh;
         const float2 xa = (t0 + t1) * 0.5f, xb = (t0 - t1) * 0.5f;
         const float2 xd = (t2 + t3) * 0.5f, xe = (t2 - t3) * 0.5f;

@@ -475,11 +475,6 @@ __device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
     return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
 }
 
-__device__ __forceinline__ float2 shrink_c(float2 c, float lam) {
-    const float m = sqrtf(c.x * c.x + c.y * c.y);   // wavelet.rs:90 |z|
-    if (m <= lam) return make_float2(0.f, 0.f);
-    return c * ((m - lam) / m);
-}
 
 // Register plans: N, active threads, radices.
 using P256 = Plan<256, 32, 16, 16>;

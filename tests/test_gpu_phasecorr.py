@@ -98,3 +98,14 @@ def test_phase_correct_off_ignores_navigators(ctx, vol):
     a = tse_acquisitions(vol)
     got = CsRss(iters=ITERS, lambda_=LAM, phase_correct=False).reconstruct(ctx, a).data
     assert o64.nrmse(got, oracle(a, phase_correct=False)) <= TOL
+
+
+def test_phase_correction_with_device_resident_samples(ctx, vol):
+    """data_on_device: the navigators are gathered device to device; same
+    volume as the host-sample call."""
+    a = tse_acquisitions(vol)
+    s = CsRss(iters=ITERS, lambda_=LAM)
+    host = s.reconstruct(ctx, a).data
+    d = ctx.to_device(a.data)
+    dev = s.reconstruct(ctx, a, device_data=d).data.to_host()
+    assert np.array_equal(dev, host)
