@@ -193,9 +193,9 @@ __global__ void k_fista_col(FistaColArgs a, FftPlan pl, const float2* __restrict
             float2 pll = (s0 + s1) * 0.5f, phl = (d0 + d1) * 0.5f;
             float2 plh = (s0 - s1) * 0.5f, phh = (d0 - d1) * 0.5f;
             // plh is the LL band of the demodulated image: left untouched
-            pll = shrink_c(pll, lam);
-            phl = shrink_c(phl, lam);
-            phh = shrink_c(phh, lam);
+            pll = shrink_exact(pll, lam);
+            phl = shrink_exact(phl, lam);
+            phh = shrink_exact(phh, lam);
             const float2 t0 = pll + plh, t1 = phl + phh, t2 = pll - plh, t3 = phl - phh;
             const float2 xa = (t0 + t1) * 0.5f, xb = (t0 - t1) * 0.5f;
             const float2 xd = (t2 + t3) * 0.5f, xe = (t2 - t3) * 0.5f;
@@ -309,7 +309,7 @@ __global__ void k_soft_threshold(float2* d, long long nprob, int ny, int nx, flo
         const long long rem = q % ((long long)ny * nx);
         const int i = (int)(rem / nx), j = (int)(rem - (long long)i * nx);
         if (i < hy && j < hx) continue;   // keep LL (wavelet.rs:86-88)
-        d[q] = shrink_c(d[q], lam);
+        d[q] = shrink_exact(d[q], lam);
     }
 }
 

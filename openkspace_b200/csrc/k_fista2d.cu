@@ -141,9 +141,9 @@ __global__ void k2d_row(Fista2dArgs a, FftPlan pl, const float2* __restrict__ gt
             float2 pll = (s0 + s1) * 0.5f, phl = (d0 + d1) * 0.5f;
             float2 plh = (s0 - s1) * 0.5f, phh = (d0 - d1) * 0.5f;
             // phh is the LL band of the demodulated image: left untouched
-            pll = shrink_c(pll, lam);
-            phl = shrink_c(phl, lam);
-            plh = shrink_c(plh, lam);
+            pll = shrink_exact(pll, lam);
+            phl = shrink_exact(phl, lam);
+            plh = shrink_exact(plh, lam);
             const float2 t0 = pll + plh, t1 = phl + phh, t2 = pll - plh, t3 = phl - phh;
             const float2 xa = (t0 + t1) * 0.5f, xb = (t0 - t1) * 0.5f;
             const float2 xd = (t2 + t3) * 0.5f, xe = (t2 - t3) * 0.5f;
@@ -202,9 +202,9 @@ __global__ void k2d_prox(Fista2dArgs a, const float2* __restrict__ W, int mode, 
         float2 pll = (s0 + s1) * 0.5f, phl = (d0 + d1) * 0.5f;
         float2 plh = (s0 - s1) * 0.5f, phh = (d0 - d1) * 0.5f;
         // phh is the LL band of the demodulated image: left untouched
-        pll = shrink_c(pll, lam);
-        phl = shrink_c(phl, lam);
-        plh = shrink_c(plh, lam);
+        pll = shrink_exact(pll, lam);
+        phl = shrink_exact(phl, lam);
+        plh = shrink_exact(plh, lam);
         const float2 t0 = pll + plh, t1 = phl + phh, t2 = pll - plh, t3 = phl - phh;
         const float2 xa = (t0 + t1) * 0.5f, xb = (t0 - t1) * 0.5f;
         const float2 xd = (t2 + t3) * 0.5f, xe = (t2 - t3) * 0.5f;
