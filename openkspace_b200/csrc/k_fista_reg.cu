@@ -315,18 +315,17 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
     const float lam = a.lambda;
     const bool b0 = (t & 1) != 0, b1 = (t & 2) != 0;
     const long long total = a.nprob * nrp, stride = (long long)gridDim.x * G;
-    // pipelined form (a.prefetch bit 1): the next unit's S, Z~, X~ are copied
+    // pipelined form (a.prefetch bit 1): the next unit's S is copied
     // (cp.async) into this thread's own shared-memory slots while the current
-    // unit's transforms run
-    float2* PF = RT + roots_total + G * 2 * P::SMEM_X + g * 3 * E * T;   // [E][T] S, Z~, X~
+    // unit's transforms run; Z~ and X~, needed only after the inverse
+    // transform, are loaded directly
+    float2* PF = RT + roots_total + G * 2 * P::SMEM_X + g * E * T;   // [E][T] S
     auto issue = [&](long long u) {
         const long long p = u / nrp;
         const int r0 = 2 * (int)(u - p * nrp);
         const uint32_t* cb = a.colbits + ((p + a.mask_offset) % a.mask_mod) * a.col_wstride;
         const long long base = p * a.st_stride + (long long)r0 * N;
         const float2* S = a.S + base;
-        const float2* X = a.X + base;
-        const float2* Z = a.Z + base;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int q = t + TA * e;
@@ -334,10 +333,6 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
             const long long off = (long long)(q & 1) * N + x;
             const bool on = live && ((__ldg(cb + (x >> 5)) >> (x & 31)) & 1u);
             cp_async8(PF + e * T + t, on ? S + off : S, on ? 8u : 0u);
-            if (mode) {
-                cp_async8(PF + (E + e) * T + t, live ? Z + off : Z, live ? 8u : 0u);
-                cp_async8(PF + (2 * E + e) * T + t, live ? X + off : X, live ? 8u : 0u);
-            }
         }
         cp_async_commit();
     };
@@ -359,11 +354,13 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
             cp_async_wait_all();
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                const int x = (t + TA * e) >> 1;
+                const int q = t + TA * e;
+                const int x = q >> 1;
+                const long long off = (long long)(q & 1) * N + x;
                 if (live && ((__ldg(cb + (x >> 5)) >> (x & 31)) & 1u)) cm |= 1u << e;
                 w[e] = PF[e * T + t];
-                zo[e] = mode ? PF[(E + e) * T + t] : make_float2(0.f, 0.f);
-                xo[e] = mode ? PF[(2 * E + e) * T + t] : make_float2(0.f, 0.f);
+                zo[e] = (mode && live) ? Z[off] : make_float2(0.f, 0.f);
+                xo[e] = (mode && live) ? X[off] : make_float2(0.f, 0.f);
             }
             if (unit + stride < total) issue(unit + stride);   // in flight during the transforms below
         } else {
@@ -563,15 +560,15 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    // the pipelined column pass (separable masks) adds each group's prefetch slots
-    // and the pipelined row pass its three
+    // the pipelined column pass (separable masks) adds each group's prefetch
+    // slots for S and y, the pipelined row pass its slots for S
     // (left out where they would cost resident CTAs below MINB per SM)
     Fista2dArgs b = a;
     const size_t base_smem = sizeof(float2) * (NTW + nrt + (size_t)G * 2 * P::SMEM_X);
-    const size_t pf_smem = sizeof(float2) * (size_t)G * (row ? 3 : 2) * P::E * P::T;
+    const size_t pf_smem = sizeof(float2) * (size_t)G * (row ? 1 : 2) * P::E * P::T;
     int pf = row ? ((a.prefetch & 2) ? 1 : 0) : ((a.separable && (a.prefetch & 1)) ? 1 : 0);
     if (pf && MINB > 1 && (base_smem + pf_smem + 1024) * MINB > 220u * 1024u) pf = 0;
-    b.prefetch = pf;
+    b.prefetch = pf ? (row ? 2 : 1) : 0;   // the kernels test their own bit
     const size_t smem = base_smem + (pf ? pf_smem : 0);
     if (row) e = set_smem_attr(reinterpret_cast<const void*>(k2d_row_reg<P, MINB>), smem);
     else e = set_smem_attr(reinterpret_cast<const void*>(k2d_col_reg<P, MINB>), smem);
