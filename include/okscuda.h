@@ -61,8 +61,9 @@ const char* okscuda_version(void);
  *                   compile-time plan exists for ny), 1 generic shared-memory
  *                   kernel, 2 register kernel (falls back to 1 for other ny)
  *   "col_variant"   register column engine: -1 (default) per column length
- *                   (the E = 8 alternative for 256, 384, 512), 0 primary plan,
- *                   1 the E = 8 alternative where one exists (192, 256, 384, 512)
+ *                   (the E = 8 alternative for 256, 320, 384, 512), 0 primary
+ *                   plan, 1 the E = 8 alternative where one exists (192, 256,
+ *                   320, 384, 512)
  *   "fista2d_chunk" problems per chunk of the 2-D-mask engine (0 = auto,
  *                   sized for L2 residency)
  *   "row_engine"    2-D-mask engine, readout-direction transforms: 0 (default)

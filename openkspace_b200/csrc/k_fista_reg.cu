@@ -739,6 +739,7 @@ cudaError_t launch_fista_col_reg(const FistaColArgs& a, RegTables& tabs, cudaStr
     if (a.variant == 1) {
         switch (a.ny) {
             case 192: return reg::launch_p<reg::S192>(a, st);
+            case 320: return reg::launch_p<reg::V320>(a, st);
             case 256: return reg::launch_p<reg::S256>(a, st);
             case 384: return reg::launch_p<reg::S384>(a, st);
             case 512: return reg::launch_p<reg::S512>(a, st);
@@ -757,7 +758,9 @@ cudaError_t launch_fista_col_reg(const FistaColArgs& a, RegTables& tabs, cudaStr
     }
 }
 
-int fista_col_reg_variants(int ny) { return (ny == 192 || ny == 256 || ny == 384 || ny == 512) ? 2 : 1; }
+int fista_col_reg_variants(int ny) {
+    return (ny == 192 || ny == 256 || ny == 320 || ny == 384 || ny == 512) ? 2 : 1;
+}
 
 cudaError_t launch_fista2d_col_reg(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st) {
     if (a.nprob <= 0) return cudaSuccess;

@@ -494,6 +494,8 @@ using S320 = Plan<320, 64, 10, 16, 2>;
 using S368 = Plan<368, 92, 4, 23, 4>;
 using S384 = Plan<384, 96, 8, 6, 8>;
 using S512 = Plan<512, 128, 8, 8, 8>;
+// E = 8 alternative for 320 (80 active threads of 96)
+using V320 = Plan<320, 80, 8, 5, 8>;
 
 template <class P>
 static void host_tables(float2* tw, int* ntw) {

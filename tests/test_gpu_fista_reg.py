@@ -33,12 +33,18 @@ def run(ctx, engine, k, m, iters, lam):
         ctx.check(ctx.lib.okscuda_set_option(ctx.handle, b"col_engine", 0))
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("ny", [128, 192, 256, 320, 368, 384, 512])
-def test_register_engine_matches(ctx2, rng, ny):
+def test_register_engine_matches(ctx2, rng, ny, variant):
+    """Both plans where a length has two (col_variant 1: the E = 8 one)."""
     nx, nc, iters = 12, 3, 12
     m = row_mask(rng, ny, nx)
     k = np.where(m[None], crandn(rng, (nc, ny, nx)), 0).astype(np.complex64)
-    reg = run(ctx2, 2, k, m, iters, 0.05)
+    ctx2.set_option("col_variant", variant)
+    try:
+        reg = run(ctx2, 2, k, m, iters, 0.05)
+    finally:
+        ctx2.set_option("col_variant", -1)
     gen = run(ctx2, 1, k, m, iters, 0.05)
     assert rel_l2(reg, gen) < 1e-5
     assert rel_l2(reg, o64.fista_cs_single_coil(k, m, iters, 0.05)) < TOL_CS
