@@ -140,8 +140,9 @@ inline TuneParams tune_params(const okscuda_ctx* ctx, int kind, int ny, int nx) 
         auto it = ctx->tuned.find(std::make_tuple(kind, ny, kind == 0 ? 0 : nx));
         if (it != ctx->tuned.end()) return it->second;
     }
-    // built-in plan variants, from okscuda_autotune runs on B200: the E = 8
-    // alternative plan is faster for column lengths 256, 384 and 512
+    // built-in plan variants, from okscuda_autotune runs and batched timings on
+    // B200: the E = 8 alternative plan is faster for column lengths 256, 320,
+    // 384 and 512
     const int variant =
         ctx->col_variant >= 0 ? ctx->col_variant : (ny == 256 || ny == 320 || ny == 384 || ny == 512) ? 1 : 0;
     return TuneParams{ctx->col_engine, variant, ctx->persist2d, ctx->occ2d,
