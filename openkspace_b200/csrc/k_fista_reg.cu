@@ -9,8 +9,9 @@
 //     up to whole warps);
 //   * every Stockham stage reads its inputs at rows i + j N/R, which for the
 //     first forward stage and the fused middle are exactly the thread's own
-//     registers (R | E); intermediate stages exchange through padded shared
-//     memory (index + index/32 keeps the strided writes conflict-free);
+//     registers (R | E); intermediate stages exchange through shared memory
+//     with an XOR-swizzled index (padi in reg_fft.cuh) that keeps the
+//     strided writes nearly conflict-free;
 //   * the last forward stage, the data residual and the first inverse stage
 //     (same radix) run back to back in registers;
 //   * the 2x2 Haar blocks pair q^1 (column) and q^2 (row): two xor-shuffle

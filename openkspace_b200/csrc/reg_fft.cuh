@@ -117,7 +117,9 @@ struct Plan {
     }
     static_assert(prod(S) == N_, "radices must multiply to N");
     static_assert(E % R[0] == 0 && E % R[S - 1] == 0, "first and last radix must divide E");
-    static constexpr int SMEM_X = 2 * N_ + (2 * N_) / 32 + 1;   // padded exchange buffer (float2)
+    // exchange buffer (float2); padi keeps indices below 2N rounded up to 16,
+    // so the last 2N/32 + 1 entries are slack kept from an earlier padding
+    static constexpr int SMEM_X = 2 * N_ + (2 * N_) / 32 + 1;
 };
 
 // Twiddle table offsets: forward stage s at tw_f(s), inverse stage s at
