@@ -117,8 +117,8 @@ struct Plan {
     }
     static_assert(prod(S) == N_, "radices must multiply to N");
     static_assert(E % R[0] == 0 && E % R[S - 1] == 0, "first and last radix must divide E");
-    // exchange buffer (float2); padi keeps indices below 2N rounded up to 16,
-    // so the last 2N/32 + 1 entries are slack kept from an earlier padding
+    // exchange buffer (float2): padi keeps every index below 2N rounded up
+    // to 16, so this size leaves 2N/32 + 1 entries unused
     static constexpr int SMEM_X = 2 * N_ + (2 * N_) / 32 + 1;
 };
 
