@@ -109,3 +109,18 @@ def test_phase_correction_with_device_resident_samples(ctx, vol):
     d = ctx.to_device(a.data)
     dev = s.reconstruct(ctx, a, device_data=d).data.to_host()
     assert np.array_equal(dev, host)
+
+
+def test_navigators_with_fewer_channels_than_the_lines(ctx, vol):
+    """The coil sum runs over the navigator's own channels (phasecorr.rs:79-86);
+    the phasor multiplies every channel of the image line (:161-168)."""
+    a = tse_acquisitions(vol)
+    h = a.headers.copy()
+    data = a.data.copy()
+    nav = np.flatnonzero(h["flags"] & ACQ_IS_PHASECORR_DATA)
+    # keep the first two channels of every navigator in place (same offsets)
+    for i in nav:
+        h[i]["active_channels"] = 2
+    b = AcquisitionSet(h, data, a.encoded, a.recon, a.ky_center, a.kz_center)
+    got = CsRss(iters=ITERS, lambda_=LAM).reconstruct(ctx, b).data
+    assert o64.nrmse(got, oracle(b)) <= TOL
