@@ -579,6 +579,8 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
     // (the kernels accept any grid)
     if (a.persist) {
         static int per_sm[2][2] = {{0, 0}, {0, 0}}, nsm = 0;
+        static std::mutex mu;
+        std::lock_guard<std::mutex> lk(mu);
         if (!per_sm[row][pf]) {
             int dev = 0;
             cudaGetDevice(&dev);

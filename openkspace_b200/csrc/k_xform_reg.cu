@@ -351,9 +351,11 @@ static int ctas_per_sm(const void* fn, int threads, size_t smem) {
 
 static int sm_count() {
     static int n[64] = {};
+    static std::mutex mu;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return 148;
+    std::lock_guard<std::mutex> lk(mu);
     if (!n[dev]) cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev);
     return n[dev] > 0 ? n[dev] : 148;
 }

@@ -528,9 +528,11 @@ template <class P>
 static cudaError_t plan_tables(const float2** tw, const float2** roots, int* nroots) {
     static float2* d_tab[64] = {};
     static int d_nrt[64] = {};
+    static std::mutex mu;   // contexts on different host threads may build a plan's tables at once
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
     if (!d_tab[dev]) {
         static float2 h[4096 + 64];
         int ntw = 0;
