@@ -73,10 +73,10 @@ __device__ __forceinline__ const float2* load_twiddles(float2* TWs, const float2
 }
 
 // The transform of direction SIGN (-1 forward, +1 unnormalised inverse).
-template <class P, int SIGN, bool NB = false>
+template <class P, int SIGN, bool NB = false, bool L = true>
 __device__ __forceinline__ void transform(float2* w, float2* A, float2* B, const float2* TW, const float2* RT, int t) {
-    if constexpr (SIGN < 0) forward<P, NB>(w, A, B, TW, RT, t);
-    else inverse<P, NB>(w, A, B, TW, RT, t);
+    if constexpr (SIGN < 0) forward<P, NB, L>(w, A, B, TW, RT, t);
+    else inverse<P, NB, L>(w, A, B, TW, RT, t);
 }
 
 template <class P, int SIGN>
@@ -208,7 +208,7 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
         }
         __syncthreads();                             // every group has read ST: refill it
         if (u + gridDim.x < total) issue(u + gridDim.x);
-        transform<P, SIGN, true>(w, A, B, TW, RT, t);
+        transform<P, SIGN, true, false>(w, A, B, TW, RT, t);   // padi layout throughout
         group_sync<P, true>();                       // the last stage has read A and B
         if (live) {
 #pragma unroll

@@ -26,6 +26,25 @@ namespace reg {
 // count (the former "+1 float2 per 32" padding: 1.25-1.75x).
 __device__ __forceinline__ int padi(int i) { return i ^ (((i >> 3) ^ (i >> 6)) & 15); }
 
+// Second exchange layout, one pad per 16 entries: lin16(v) = v + v / 16.  It
+// is linear in steps of 16, so a stage reading x[i + j N/R] with 2 N/R a
+// multiple of 16 addresses every j as one base plus a compile-time offset
+// (padi costs about five integer operations per access).  Stores of a first
+// stage of radix 4, 8 or 16 (lanes 2R apart) fall on distinct bank pairs in
+// it, so the buffer between the first and the second stage uses it.
+__device__ __forceinline__ int lin16(int v) { return v + (v >> 4); }
+
+// Source index of element (i + j NB, c) in the padi or the lin16 layout.
+template <bool LIN, int NB>
+struct SrcIdx {
+    int base;
+    __device__ __forceinline__ SrcIdx(int i, int c) : base(LIN ? lin16(2 * i + c) : 2 * i + c) {}
+    __device__ __forceinline__ int operator()(int j) const {
+        if constexpr (LIN) return base + j * (2 * NB + (2 * NB) / 16);
+        else return padi(base + 2 * j * NB);
+    }
+};
+
 // 8-byte asynchronous global -> shared copy; src_bytes 0 writes zeros (the
 // source address is then not read but must still be a valid pointer).
 __device__ __forceinline__ void cp_async8(float2* dst, const float2* src, uint32_t src_bytes) {
@@ -118,8 +137,8 @@ struct Plan {
     static_assert(prod(S) == N_, "radices must multiply to N");
     static_assert(E % R[0] == 0 && E % R[S - 1] == 0, "first and last radix must divide E");
     // exchange buffer (float2): padi keeps every index below 2N rounded up
-    // to 16, so this size leaves 2N/32 + 1 entries unused
-    static constexpr int SMEM_X = 2 * N_ + (2 * N_) / 32 + 1;
+    // to 16, lin16 below 2N + 2N/16
+    static constexpr int SMEM_X = 2 * N_ + (2 * N_) / 16 + 1;
 };
 
 // Twiddle table offsets: forward stage s at tw_f(s), inverse stage s at
@@ -207,10 +226,12 @@ __device__ __forceinline__ void odd_pairs_for(int s, const float2* a, const floa
 // columns, any radix.  src/dst are padded exchange buffers.
 // PRE: the inputs already carry this stage's twiddles (the previous stage
 // applied them as it stored, once per element; only for the split form).
-template <class P, int SIGN, int R, int p, bool PRE = false>
+// LIN: src is in the lin16 layout (written by a first stage with LINW).
+template <class P, int SIGN, int R, int p, bool PRE = false, bool LIN = false>
 __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float2* __restrict__ dst,
                                            const float2* __restrict__ tw, const float2* __restrict__ roots, int t) {
     constexpr int NB = P::N / R;
+    static_assert(!LIN || (2 * NB) % 16 == 0, "lin16 reads need 2 N/R to be a multiple of 16");
     constexpr int ITEMS = 2 * NB;
     constexpr bool BIG_ODD = (R % 2 == 1 && R > 5);
     constexpr int NS = BIG_ODD ? P::T / ITEMS : 1;   // threads sharing one butterfly
@@ -228,12 +249,13 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
         const int k = i % p;
         const int ob = (i - k) * R + k;
         float2 a[H], b[H];
-        const float2 x0 = src[padi(2 * i + c)];
+        const SrcIdx<LIN, NB> ix(i, c);
+        const float2 x0 = src[ix(0)];
         float2 y0 = x0;
 #pragma unroll
         for (int j = 1; j <= H; ++j) {
-            float2 u = src[padi(2 * (i + j * NB) + c)];
-            float2 w = src[padi(2 * (i + (R - j) * NB) + c)];
+            float2 u = src[ix(j)];
+            float2 w = src[ix(R - j)];
             if (p > 1 && !PRE) {
                 u = twmul<SIGN>(u, tw[k * (R - 1) + j - 1]);
                 w = twmul<SIGN>(w, tw[k * (R - 1) + R - j - 1]);
@@ -262,12 +284,13 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
             // R - 1 complex values stay live (bfly_odd keeps 3R)
             constexpr int H = (R - 1) / 2;
             float2 a[H], b[H];
-            const float2 x0 = src[padi(2 * i + c)];
+            const SrcIdx<LIN, NB> ix(i, c);
+            const float2 x0 = src[ix(0)];
             float2 y0 = x0;
 #pragma unroll
             for (int j = 1; j <= H; ++j) {
-                float2 u = src[padi(2 * (i + j * NB) + c)];
-                float2 w = src[padi(2 * (i + (R - j) * NB) + c)];
+                float2 u = src[ix(j)];
+                float2 w = src[ix(R - j)];
                 if (p > 1) {
                     u = twmul<SIGN>(u, tw[k * (R - 1) + j - 1]);
                     w = twmul<SIGN>(w, tw[k * (R - 1) + R - j - 1]);
@@ -292,9 +315,10 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
             }
         } else {
             float2 v[R];
+            const SrcIdx<LIN, NB> ix(i, c);
 #pragma unroll
             for (int j = 0; j < R; ++j) {
-                float2 x = src[padi(2 * (i + j * NB) + c)];
+                float2 x = src[ix(j)];
                 if (j > 0 && p > 1) x = twmul<SIGN>(x, tw[k * (R - 1) + j - 1]);
                 v[j] = x;
             }
@@ -312,7 +336,8 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
 // twiddle w^(j2 k2), k2 = i2 mod P2 (tw2: its table), so the NS threads
 // sharing a butterfly there do not each repeat the 2 (R2 - 1) products.  The
 // products are the same, so the results are bit-identical.
-template <class P, int SIGN, int R, int p, int R2 = 0, int P2 = 0>
+// LINW: store in the lin16 layout (the next stage reads with LIN).
+template <class P, int SIGN, int R, int p, int R2 = 0, int P2 = 0, bool LINW = false>
 __device__ __forceinline__ void stage_reg(float2* w, float2* __restrict__ dst, const float2* __restrict__ tw,
                                           const float2* __restrict__ roots, int t,
                                           const float2* __restrict__ tw2 = nullptr) {
@@ -346,7 +371,8 @@ __device__ __forceinline__ void stage_reg(float2* w, float2* __restrict__ dst, c
                     const int j2 = o / NB2, k2 = (o - j2 * NB2) % P2;
                     if (j2 > 0 && k2 > 0) y = twmul<SIGN>(y, tw2[k2 * (R2 - 1) + j2 - 1]);
                 }
-                dst[padi(2 * (ob + j * p) + c)] = y;
+                const int v = 2 * (ob + j * p) + c;
+                dst[LINW ? lin16(v) : padi(v)] = y;
             }
         }
     }
@@ -377,6 +403,20 @@ __device__ __forceinline__ void stage_to_reg(const float2* __restrict__ src, flo
     }
 }
 
+// True when the buffer between the first and the second stage of a direction
+// (first radix R0, second R1) takes the lin16 layout: a plan of 3 or more
+// stages, R0 in {4, 8, 16}, 2 N/R1 a multiple of 16.  The drivers' L = false
+// keeps padi throughout (the tiled column transform ran 5-7 % slower at 384
+// and 640 with lin16, while the row transforms ran 8-16 % faster).
+template <class P, int R0, int R1>
+constexpr bool lin_first() {
+    return P::S >= 3 && (R0 == 4 || R0 == 8 || R0 == 16) && R1 > 0 && (2 * (P::N / R1)) % 16 == 0;
+}
+template <class P>
+constexpr bool lin_fwd() { return lin_first<P, P::R[0], (P::S >= 2 ? P::R[P::S >= 2 ? 1 : 0] : 0)>(); }
+template <class P>
+constexpr bool lin_inv() { return lin_first<P, P::R[P::S - 1], (P::S >= 2 ? P::R[P::S >= 2 ? P::S - 2 : 0] : 0)>(); }
+
 // True when a middle stage of radix R runs in the split odd-radix form (the
 // plan has fewer of its butterflies than threads).
 template <class P, int R>
@@ -400,7 +440,7 @@ __device__ __forceinline__ void group_sync() {
 
 // Forward transform: registers (state layout) -> registers (mid layout of
 // the last radix).  Stages 0..S-2 go through smem buffers A/B.
-template <class P, int s, bool NB = false>
+template <class P, int s, bool NB = false, bool L = true>
 __device__ __forceinline__ void fwd_rest(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
                                          int t) {
     if constexpr (s < P::S) {
@@ -413,14 +453,14 @@ __device__ __forceinline__ void fwd_rest(float2* w, float2* A, float2* B, const 
             stage_to_reg<P, -1, R, p>(src, w, tw + off, roots, t);
         } else {
             constexpr bool PRE = s == 1 && split_odd_stage<P, R>();   // twiddled by stage 0's stores
-            stage_smem<P, -1, R, p, PRE>(src, dst, tw + off, roots, t);
+            stage_smem<P, -1, R, p, PRE, L && s == 1 && lin_fwd<P>()>(src, dst, tw + off, roots, t);
             group_sync<P, NB>();
-            fwd_rest<P, s + 1, NB>(w, A, B, tw, roots, t);
+            fwd_rest<P, s + 1, NB, L>(w, A, B, tw, roots, t);
         }
     }
 }
 
-template <class P, bool NB = false>
+template <class P, bool NB = false, bool L = true>
 __device__ __forceinline__ void forward(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
                                         int t) {
     constexpr int R0 = P::R[0];
@@ -428,16 +468,16 @@ __device__ __forceinline__ void forward(float2* w, float2* A, float2* B, const f
         stage_reg<P, -1, R0, 1>(w, nullptr, tw, roots, t);
     } else {
         if constexpr (P::S >= 3 && split_odd_stage<P, P::R[1]>())
-            stage_reg<P, -1, R0, 1, P::R[1], R0>(w, A, tw, roots, t, tw + Tw<P>::fwd(1));
+            stage_reg<P, -1, R0, 1, P::R[1], R0, L && lin_fwd<P>()>(w, A, tw, roots, t, tw + Tw<P>::fwd(1));
         else
-            stage_reg<P, -1, R0, 1>(w, A, tw, roots, t);   // outputs to A
+            stage_reg<P, -1, R0, 1, 0, 0, L && lin_fwd<P>()>(w, A, tw, roots, t);   // outputs to A
         group_sync<P, NB>();
-        fwd_rest<P, 1, NB>(w, A, B, tw, roots, t);
+        fwd_rest<P, 1, NB, L>(w, A, B, tw, roots, t);
     }
 }
 
 // Inverse transform: registers (mid layout of R[S-1]) -> registers (state).
-template <class P, int s, bool NB = false>
+template <class P, int s, bool NB = false, bool L = true>
 __device__ __forceinline__ void inv_rest(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
                                          int t) {
     if constexpr (s < P::S) {
@@ -450,14 +490,14 @@ __device__ __forceinline__ void inv_rest(float2* w, float2* A, float2* B, const 
             stage_to_reg<P, +1, R, p>(src, w, tw + off, roots, t);
         } else {
             constexpr bool PRE = s == 1 && split_odd_stage<P, R>();   // twiddled by stage 0's stores
-            stage_smem<P, +1, R, p, PRE>(src, dst, tw + off, roots, t);
+            stage_smem<P, +1, R, p, PRE, L && s == 1 && lin_inv<P>()>(src, dst, tw + off, roots, t);
             group_sync<P, NB>();
-            inv_rest<P, s + 1, NB>(w, A, B, tw, roots, t);
+            inv_rest<P, s + 1, NB, L>(w, A, B, tw, roots, t);
         }
     }
 }
 
-template <class P, bool NB = false>
+template <class P, bool NB = false, bool L = true>
 __device__ __forceinline__ void inverse(float2* w, float2* A, float2* B, const float2* tw, const float2* roots,
                                         int t) {
     constexpr int R0 = P::R[P::S - 1];
@@ -465,11 +505,12 @@ __device__ __forceinline__ void inverse(float2* w, float2* A, float2* B, const f
         stage_reg<P, +1, R0, 1>(w, nullptr, tw + Tw<P>::inv(0), roots, t);
     } else {
         if constexpr (P::S >= 3 && split_odd_stage<P, P::R[P::S - 2]>())
-            stage_reg<P, +1, R0, 1, P::R[P::S - 2], R0>(w, A, tw + Tw<P>::inv(0), roots, t, tw + Tw<P>::inv(1));
+            stage_reg<P, +1, R0, 1, P::R[P::S - 2], R0, L && lin_inv<P>()>(w, A, tw + Tw<P>::inv(0), roots, t,
+                                                                  tw + Tw<P>::inv(1));
         else
-            stage_reg<P, +1, R0, 1>(w, A, tw + Tw<P>::inv(0), roots, t);
+            stage_reg<P, +1, R0, 1, 0, 0, L && lin_inv<P>()>(w, A, tw + Tw<P>::inv(0), roots, t);
         group_sync<P, NB>();
-        inv_rest<P, 1, NB>(w, A, B, tw, roots, t);
+        inv_rest<P, 1, NB, L>(w, A, B, tw, roots, t);
     }
 }
 
