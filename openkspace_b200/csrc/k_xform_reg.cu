@@ -30,10 +30,11 @@ __device__ __forceinline__ void cp_async16(float2* dst, const float2* src, uint3
                  : "memory");
 }
 
-// Exchange buffer of one group: the XOR swizzle of padi stays inside aligned
-// blocks of 16, so 2N rounded up to 16 entries suffice.
+// Exchange buffer of one group, rounded up to 16 entries: padi keeps every
+// index below 2N rounded up to 16, lin16 (the first stage's output) below
+// 2N + 2N/16.
 template <class P>
-constexpr int xbuf() { return (2 * P::N + 15) / 16 * 16; }
+constexpr int xbuf() { return (P::SMEM_X + 15) / 16 * 16; }
 
 // Groups per CTA of the row kernel (warp-sized groups share a CTA).
 template <class P>
