@@ -234,10 +234,30 @@ class BatchedWorkload:
     dominant = ("k_fista_col_reg",)
     bytes_model = "state model: 40 B per pixel per coil per iteration (read z, x, y; write x', z')"
 
-    def __init__(self, n: int = 64):
+    def __init__(self, n: int = 64, reqs=None):
         from openkspace_b200 import synth
-        self.reqs = synth.uneven_requests(n=n)
-        self.units = n
+        self.reqs = reqs if reqs is not None else synth.uneven_requests(n=n)
+        self.units = len(self.reqs)
+
+    @classmethod
+    def from_files(cls, d):
+        """The 64 slices written by _side_inputs."""
+        from openkspace_b200 import synth
+        meta = json.load(open(os.path.join(d, "reqs.json")))
+        reqs = [synth.SliceRequest(np.load(os.path.join(d, f"req{i}_k.npy")),
+                                   np.load(os.path.join(d, f"req{i}_m.npy")), int(it), float(lam))
+                for i, (it, lam) in enumerate(meta)]
+        return cls(reqs=reqs)
+
+    def check_indices(self):
+        """One slice per matrix size, the lightest of each (coils x iterations)."""
+        best = {}
+        for i, r in enumerate(self.reqs):
+            key = r.kspace.shape[1:]
+            w = r.kspace.shape[0] * r.iters
+            if key not in best or w < best[key][0]:
+                best[key] = (w, i)
+        return sorted(i for _, i in best.values())
 
     def config(self):
         return {"workload": f"batched_uneven_{self.units}slices", "sizes": "256^2,320^2,384^2,368x640",
@@ -298,15 +318,23 @@ class Volume3dWorkload:
     dominant = ("k_fista_col_reg", "k_fista_col")
     bytes_model = "state model: 40 B per pixel per coil per iteration (read z, x, y; write x', z')"
 
-    def __init__(self, nz: int = 192, nc: int = 32, iters: int = 80):
+    def __init__(self, nz: int = 192, nc: int = 32, iters: int = 80, data=None):
         from openkspace_b200 import synth
         from openkspace_b200.strategy import CsRss, cartesian3d_acquisitions
-        self.k, self.mask_rows = synth.volume_3d(nc=nc, nz=nz)
+        self.k, self.mask_rows = data if data is not None else synth.volume_3d(nc=nc, nz=nz)
         self.acqs = cartesian3d_acquisitions(self.k, self.mask_rows)
         self.strategy = CsRss(iters=iters, lambda_=0.01)
         self.nc, self.nz, self.ny, self.nx = self.k.shape
         self.iters = iters
         self.units = nz
+
+    @classmethod
+    def from_files(cls, d):
+        """The volume written by _side_inputs."""
+        k = np.load(os.path.join(d, "vol_k.npy"))
+        m = np.load(os.path.join(d, "vol_m.npy"))
+        os.unlink(os.path.join(d, "vol_k.npy"))
+        return cls(nz=k.shape[1], nc=k.shape[0], data=(k, m))
 
     def config(self):
         return {"workload": f"cartesian3d_{self.nc}c_{self.ny}x{self.nx}x{self.nz}_R6_I{self.iters}",
@@ -625,6 +653,150 @@ def run_reference(args, wl, rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------ kernel roofline records
+def precision_kernel_roofline(ctx, wl, hbm, peak_kind):
+    """Per-kernel roofline of the 2-D engine's two passes, from one profiled
+    step with the CUDA graph off and one stream (every launch timed alone
+    with CUDA events on its own stream).  Algorithmic bytes are what each
+    pass must move per problem (f_c sampled kx columns, f_r sampled ky rows):
+      k2d_row_reg: iteration launches read S (8 f_c), Z~, X~ (16) and write
+                   X~, Z~ (16), S (8 f_c): 32 + 16 f_c B per pixel; the
+                   initial launch reads S, writes X~, Z~, S: 16 + 16 f_c
+      k2d_col_reg: iteration launches read and write S (16 f_c) and read y'
+                   on the sampled points (8 f_c f_r); the initial launch
+                   reads y' and writes S: 8 f_c + 8 f_c f_r."""
+    f_c = wl.vol.rec_x / wl.nx
+    f_r = len(wl.vol.ky_index[0]) / wl.ny
+    npx = float(wl.ny * wl.nx * wl.nc * wl.nz)
+    I = wl.iters
+    model = {"k2d_row_reg": ((32 + 16 * f_c) * I + (16 + 16 * f_c)) * npx,
+             "k2d_col_reg": ((16 * f_c + 8 * f_c * f_r) * I + (8 * f_c + 8 * f_c * f_r)) * npx}
+    ctx.set_option("graph2d", 0)
+    ctx.set_option("fista2d_streams", 1)
+    try:
+        wl.step_device()
+        ctx.synchronize()
+        ctx.profile(True)
+        wl.step_device()
+        ctx.synchronize()
+        prof = ctx.profile_read()
+        ctx.profile(False)
+    finally:
+        ctx.set_option("graph2d", 1)
+        ctx.set_option("fista2d_streams", 2)
+    kernels = {}
+    step_ms = sum(v[0] for v in prof.values())
+    for k, b in model.items():
+        ms, n = prof.get(k, (0.0, 0))
+        if n == 0 or ms <= 0:
+            continue
+        gbs = b / (ms / 1e3) / 1e9
+        kernels[k] = {"launches": int(n), "us_per_launch": 1e3 * ms / n, "ms_per_step": ms,
+                      "share_of_step": ms / step_ms if step_ms > 0 else None,
+                      "algorithmic_bytes_per_launch": b / n, "achieved": gbs, "frac": gbs / hbm}
+    return kernels, prof
+
+
+def measure(ctx, wl, stream, steps, warmup, flush_bytes=None):
+    """Device and end-to-end rate of one workload (no profiling): a short
+    side measurement of the default line."""
+    import torch
+    flush = None
+    if wl.input_bytes() < L2_BYTES:
+        flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        wl.step_device()
+    wl.step_e2e()
+    torch.cuda.synchronize()
+
+    def run(fn, profile=False):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if profile:
+            ctx.profile(True)
+        torch.cuda.synchronize()
+        for a, b in evs:
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        prof = ctx.profile_read() if profile else {}
+        if profile:
+            ctx.profile(False)
+        return sum(a.elapsed_time(b) for a, b in evs), prof
+
+    ms, prof = run(wl.step_device, profile=True)
+    ms_e2e, _ = run(wl.step_e2e)
+    hbm, kind = peaks()
+    dom = next((k for k in wl.dominant if k in prof), wl.dominant[0])
+    dms, dn = prof.get(dom, (0.0, 0))
+    ach = wl.dominant_bytes_per_step() * steps / (dms / 1e3) / 1e9 if dms > 0 else 0.0
+    h2d, d2h = wl.e2e_bytes()
+    return {"config": wl.config(), "steps": steps, "ms_per_step": ms / steps,
+            "value": wl.units * steps / (ms / 1e3), "unit": "slices/s",
+            "e2e": {"value": wl.units * steps / (ms_e2e / 1e3), "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "l2": "flushed between steps" if flush is not None else "inputs larger than L2",
+            "gpu_launches": int(sum(n for _, n in prof.values())),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "peak_kind": kind,
+                         "unit": "GB/s", "frac": ach / hbm, "model": wl.bytes_model,
+                         "note": "register/L2-resident state: the state model can exceed HBM"}}
+
+
+# ------------------------------------------------------- the CPU baseline leg
+def cpu_baseline_leg(wl, gpu_slice0, nthreads, extras):
+    """The CPU baseline of the default line and the parity of the timed
+    output, both through the oracle (the checker):
+      * the FP32 C restatement of the reference (oracle/cs_ref.c) runs slice 0
+        of the precision workload -- noise fit, prewhitening, oversampling
+        removal, placement, FISTA on all coils, RSS -- on `nthreads` host
+        threads: the timed CPU baseline;
+      * the GPU's timed output for slice 0 is compared with that output
+        (relative L2, the stand-in for the reference `cs` output) and with
+        the FP64 oracle of the same pipeline (NRMSE);
+      * `extras`: (name, gpu_rss, kspace, mask, iters, lambda) slices of the
+        side workloads, checked against the FP64 oracle."""
+    from oracle import csref
+    from oracle import cs_fp64 as o64
+    from oracle import strategy_ref
+    from openkspace_b200 import synth
+    from openkspace_b200.strategy import oversampled_acquisitions
+    vol = wl.vol
+    t = time.perf_counter()
+    w = csref.prewhiten_fit(vol.noise)
+    lines = csref.prewhiten_apply(w, vol.lines[0])
+    os_ = csref.oversampling_apply(lines, vol.enc_x, vol.rec_x)
+    k = np.zeros((wl.nc, 1, wl.ny, wl.nx), np.complex64)
+    m = np.zeros((1, wl.ny, wl.nx), bool)
+    x0 = wl.nx // 2 - vol.rec_x // 2
+    k[:, 0, vol.ky_index[0], x0:x0 + vol.rec_x] = np.transpose(os_, (1, 0, 2))
+    m[0, vol.ky_index[0], x0:x0 + vol.rec_x] = True
+    port = csref.csrss(k, m, wl.iters, 0.005, nthreads=nthreads)
+    dt = time.perf_counter() - t
+    port = o64.maybe_crop(port, (vol.rec_x, wl.ny, 1))
+    base = {"value": 1.0 / dt, "unit": "slices/s", "cores": nthreads, "kind": "port",
+            "sample": f"slice 0 of the workload: noise fit, prewhitening, oversampling removal and placement of "
+                      f"its {vol.lines.shape[1]} lines, FISTA on all {wl.nc} coils ({wl.iters} iterations), RSS, "
+                      f"crop; oracle/cs_ref.c on {nthreads} host threads"}
+    a1 = oversampled_acquisitions(synth.oversampled_volume(nz=1))    # slice 0: same seeds
+    t = time.perf_counter()
+    want = strategy_ref.csrss_reconstruct(a1.headers, a1.data, a1.encoded, a1.recon, a1.ky_center, a1.kz_center,
+                                          iters=wl.iters, lam=0.005, workers=nthreads)
+    t64 = time.perf_counter() - t
+    parity = {"slice": 0, "nrmse_vs_fp64": o64.nrmse(gpu_slice0, want[0]),
+              "rel_l2_vs_port": o64.nrmse(gpu_slice0, port[0]),
+              "port_nrmse_vs_fp64": o64.nrmse(port[0], want[0]), "fp64_oracle_s": t64,
+              "tolerance": 1e-4, "image": "RSS magnitude after crop (368 x 320)"}
+    checks = {}
+    for name, rss, ks, mask, iters, lam in extras:
+        x = o64.csrss_from_kspace(ks[:, None], mask[None], iters, lam, workers=nthreads)
+        checks[name] = o64.nrmse(rss, x[0])
+    parity["side_workloads_nrmse_vs_fp64"] = checks
+    return base, parity
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -638,9 +810,10 @@ def main():
     ap.add_argument("--fft-shape", default="368x640",
                     help="fft workloads: plane shape NYxNX (the column pass runs length NY, the row pass NX)")
     ap.add_argument("--no-extras", action="store_true",
-                    help="precision: skip the short tensor-core and serving side measurements")
+                    help="precision: skip the side measurements (other readout engine, FFT stages, serving, "
+                         "configurations 0, 2 and 4)")
     ap.add_argument("--rates", default="50,200,800", help="served: Poisson arrival rates (req/s)")
-    ap.add_argument("--seconds", type=float, default=4.0, help="served: arrivals per rate x this many seconds")
+    ap.add_argument("--seconds", type=float, default=60.0, help="served: arrivals per rate x this many seconds")
     ap.add_argument("--requests", type=int, default=2000, help="served: at most this many requests per rate")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -660,6 +833,16 @@ def main():
     if args.impl == "reference":
         run_reference(args, wl, rank)
         return
+
+    extras = wl.name == "precision" and not args.no_extras and world == 1 and rank == 0
+    side_inputs = None
+    if extras:
+        # the side workloads' synthetic inputs are generated in a separate
+        # process (spawned before the first GPU call) while this one measures
+        import multiprocessing as mp
+        side_pool = mp.get_context("spawn").Pool(1)
+        side_dir = tempfile.mkdtemp()
+        side_inputs = side_pool.apply_async(_side_inputs, (side_dir,))
 
     import torch
     torch.cuda.set_device(local)
@@ -720,6 +903,62 @@ def main():
     ms, prof = timed(wl.step_device, args.steps, profile=True)
     ms_e2e, _ = timed(wl.step_e2e, args.steps)
     clk = clocks.stop()
+    gpu_slice0 = None
+    if wl.name == "precision":
+        gpu_slice0 = wl.d_out.to_host()[0]       # slice 0 of the last timed step's output
+
+    units = wl.units * args.steps * world
+    value = units / (ms / 1e3)
+    e2e_value = units / (ms_e2e / 1e3)
+    hbm, peak_kind = peaks()
+    launches = int(sum(n for _, n in prof.values()))
+    h2d, d2h = wl.e2e_bytes()
+    metric = getattr(wl, "metric", "FISTA-CS slices/s at NRMSE<=1e-4 vs FP64")
+    vunit = getattr(wl, "unit", "slices/s")
+    tfile = os.path.join(ROOT, "profiles", "dram_traffic.json")   # per-launch ncu DRAM bytes, by workload
+    traffic_tab = json.load(open(tfile)) if os.path.exists(tfile) else {}
+
+    if wl.name == "precision" and args.row_engine == "simt":
+        # the dominant kernel's own roofline (non-graph profiled step); the
+        # whole engine against the state model beside it
+        kernels, prof_ng = precision_kernel_roofline(ctx, wl, hbm, peak_kind)
+        dom_name = max(kernels, key=lambda k: kernels[k]["ms_per_step"]) if kernels else "k2d_row_reg"
+        kd = kernels.get(dom_name, {"achieved": 0.0, "frac": 0.0})
+        t = traffic_tab.get("precision_chunk_12x368x640", {}).get(dom_name)
+        graph_ms = prof.get("k2d_graph", (ms, 1))[0]
+        state_b = 40.0 * wl.ny * wl.nx * wl.nc * wl.nz * wl.iters * args.steps
+        roofline = {"bound": "hbm", "kernel": dom_name, "achieved": kd["achieved"], "peak": hbm,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": kd["frac"],
+                    "traffic": float(t["dram_bytes_per_launch"]) if t else None,
+                    "traffic_note": (t or {}).get("note"),
+                    "model": precision_kernel_roofline.__doc__.split("Algorithmic bytes", 1)[1].strip(),
+                    "timing": "one profiled step with the CUDA graph off and one stream: each launch timed alone",
+                    "kernels": kernels,
+                    "engine_state_model": {
+                        "model": "40 B per pixel per coil per iteration (read z, x, y; write x', z') over the "
+                                 "2-D engine's graph time in the timed steps",
+                        "achieved": state_b / (graph_ms / 1e3) / 1e9,
+                        "frac": state_b / (graph_ms / 1e3) / 1e9 / hbm}}
+    else:
+        bound, unit, peak, model = "hbm", "GB/s", hbm, wl.bytes_model
+        dom_name = next((k for k in wl.dominant if k in prof), wl.dominant[0])
+        dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
+        dbytes = (wl.dominant_bytes_per_step(dom_name) if wl.name in ("precision", "fft")
+                  else wl.dominant_bytes_per_step())
+        achieved = dbytes * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+        if wl.name == "precision" and args.row_engine == "tc":
+            # tensor-core row DFTs: the tcgen05 FLOPs they issue / their device time
+            dom_name = "k_dft_tc"
+            dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
+            bound, unit = "tensor", "TFLOP/s"
+            peak, peak_kind = tc_peak()
+            achieved = wl.tc_flops_per_step() * args.steps / (dom_ms / 1e3) / 1e12 if dom_ms > 0 else 0.0
+            model = wl.tc_flops_model
+        t = traffic_tab.get(wl.config()["workload"], {}).get(dom_name)
+        roofline = {"bound": bound, "kernel": dom_name, "achieved": achieved, "peak": peak,
+                    "peak_kind": peak_kind, "unit": unit, "frac": achieved / peak,
+                    "traffic": float(t) if isinstance(t, (int, float)) else None, "model": model}
+
     # precision workload: the other readout engine, a few steps, for the
     # SIMT FFT vs tensor-core DFT comparison on the same configuration
     other = None
@@ -734,37 +973,10 @@ def main():
                  "value": wl.units * k_other * world / (ms_o / 1e3), "unit": "slices/s",
                  "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof_o.items()}}
 
-    units = wl.units * args.steps * world
-    value = units / (ms / 1e3)
-    e2e_value = units / (ms_e2e / 1e3)
-    hbm, peak_kind = peaks()
-    bound, unit, peak, model = "hbm", "GB/s", hbm, wl.bytes_model
-    dom_name = next((k for k in wl.dominant if k in prof), wl.dominant[0])
-    dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
-    # algorithmic bytes of the dominant kernel over the timed steps / its device time
-    dbytes = (wl.dominant_bytes_per_step(dom_name) if wl.name in ("precision", "fft")
-              else wl.dominant_bytes_per_step())
-    achieved = dbytes * args.steps / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
-    if wl.name == "precision" and args.row_engine == "tc":
-        # tensor-core row DFTs: the tcgen05 FLOPs they issue / their device time
-        dom_name = "k_dft_tc"
-        dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
-        bound, unit = "tensor", "TFLOP/s"
-        peak, peak_kind = tc_peak()
-        achieved = wl.tc_flops_per_step() * args.steps / (dom_ms / 1e3) / 1e12 if dom_ms > 0 else 0.0
-        model = wl.tc_flops_model
-    launches = int(sum(n for _, n in prof.values()))
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "dram_traffic.json")   # per-launch ncu DRAM bytes, by workload
-    if os.path.exists(tfile):
-        t = json.load(open(tfile)).get(wl.config()["workload"], {}).get(dom_name)
-        traffic = float(t) if t is not None else None
-
     if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
         return
-    h2d, d2h = wl.e2e_bytes()
-    metric = getattr(wl, "metric", "FISTA-CS slices/s at NRMSE<=1e-4 vs FP64")
-    vunit = getattr(wl, "unit", "slices/s")
     line = {
         "metric": metric,
         "value": value, "unit": vunit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -775,9 +987,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": vunit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof.items()},
-        "roofline": {"bound": bound, "kernel": dom_name, "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": unit, "frac": achieved / peak, "traffic": traffic,
-                     "model": model},
+        "roofline": roofline,
         "clocks": clk,
     }
     if wl.name == "precision":
@@ -785,22 +995,52 @@ def main():
                                         else "tcgen05 split-3xBF16 DFT-as-GEMM, FP32 accumulation")
     if other is not None:
         line["other_row_engine"] = other
-    if wl.name == "precision" and not args.no_extras and world == 1:
-        # the metric's served-vs-plain half: Poisson arrivals at 800 req/s of
-        # the uneven request mix through the request server, beside the
-        # plain per-slice drop-in (host clock, submit -> result on the host)
-        sctx = Context(local)
-        served, plain = serving_measure(sctx, [800.0], 2.0, 400)
-        sctx.close()
-        line["serving"] = {"served": served, "plain": plain,
-                           "served_over_plain": served["800"]["slices_per_s"] / plain["slices_per_s"],
-                           "requests": "sizes {256^2,320^2,384^2,368x640}, coils U{8..32}, R {2,3,4,6}, "
-                                       "iters U{30..150}; --workload served for 50/200/800 req/s"}
-    if wl.name == "precision" and not args.no_extras:
+    side_checks = []
+    if extras:
         # the FFT stages on their own: row and column passes of the centred
         # 2-D FFT at the configuration's lengths, against the HBM roofline
         line["fft_stages"] = fft_stages(ctx)
-    if not args.no_cpu_baseline:
+        # the metric's served-vs-plain half: Poisson arrivals of the uneven
+        # request mix through the request server at three rates, beside the
+        # plain per-slice drop-in (host clock, submit -> result on the host)
+        sctx = Context(local)
+        served, plain = serving_measure(sctx, [50.0, 200.0, 800.0], 20.0, 2000)
+        sctx.close()
+        line["serving"] = {"served": served, "plain": plain,
+                           "served_over_plain": {r: v["slices_per_s"] / plain["slices_per_s"]
+                                                 for r, v in served.items()},
+                           "requests": "sizes {256^2,320^2,384^2,368x640}, coils U{8..32}, R {2,3,4,6}, "
+                                       "iters U{30..150}; up to 2000 requests or 20 s of arrivals per rate"}
+        # configurations 0, 2 and 4, each a short device + end-to-end measurement
+        configs = {}
+        pw = PlainWorkload(1)
+        pw.prepare(ctx)
+        configs["plain_8x256x256_I50"] = measure(ctx, pw, stream, 10, 3)
+        rss0 = pw.d_out.to_host()[0]
+        side_checks.append(("plain_8x256x256_I50", rss0, pw.k[:, 0], pw.mask[0].astype(bool), pw.iters, pw.lam))
+        del pw
+        d = side_inputs.get(timeout=1800)
+        bw = BatchedWorkload.from_files(d)
+        bw.prepare(ctx)
+        configs["batched_uneven_64"] = measure(ctx, bw, stream, 5, 3)
+        for i in bw.check_indices():
+            r = bw.reqs[i]
+            side_checks.append((f"batched_uneven_64[{i}] {r.kspace.shape[0]}x{r.kspace.shape[1]}x"
+                                f"{r.kspace.shape[2]} I{r.iters}", bw.d_out[i].to_host(), r.kspace,
+                                np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1), r.iters, r.lam))
+        del bw
+        vw = Volume3dWorkload.from_files(d)
+        vw.prepare(ctx)
+        configs["cartesian3d_32x256x256x192_I80"] = measure(ctx, vw, stream, 3, 3)
+        del vw
+        side_pool.close()
+        import shutil
+        shutil.rmtree(side_dir, ignore_errors=True)
+        line["configurations"] = configs
+    if not args.no_cpu_baseline and wl.name == "precision" and world == 1:
+        nthreads = os.cpu_count() or 1
+        line["cpu_baseline"], line["parity"] = cpu_baseline_leg(wl, gpu_slice0, nthreads, side_checks)
+    elif not args.no_cpu_baseline:
         nthreads = 1
         dt, u, sample = wl.cpu_sample(nthreads)
         line["cpu_baseline"] = {"value": u / dt, "unit": vunit, "cores": nthreads, "kind": "port",
@@ -808,6 +1048,22 @@ def main():
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def _side_inputs(tmpdir):
+    """Synthetic inputs of configurations 2 (64 uneven slices) and 4 (the
+    3-D Cartesian volume), saved as .npy files in tmpdir (run in a spawned
+    process while the main one measures)."""
+    from openkspace_b200 import synth
+    reqs = synth.uneven_requests(n=64)
+    for i, r in enumerate(reqs):
+        np.save(os.path.join(tmpdir, f"req{i}_k.npy"), r.kspace)
+        np.save(os.path.join(tmpdir, f"req{i}_m.npy"), r.mask_rows)
+    json.dump([[r.iters, r.lam] for r in reqs], open(os.path.join(tmpdir, "reqs.json"), "w"))
+    k, m = synth.volume_3d(nc=32, nz=192)
+    np.save(os.path.join(tmpdir, "vol_k.npy"), k)
+    np.save(os.path.join(tmpdir, "vol_m.npy"), m)
+    return tmpdir
 
 
 if __name__ == "__main__":

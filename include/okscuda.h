@@ -145,6 +145,12 @@ int okscuda_dft_rows(okscuda_ctx* ctx, const okscuda_c64* d_in, okscuda_c64* d_o
  * context stream): 0 = no bounded wait ran out since the last read.  No
  * reference counterpart. */
 int okscuda_tc_status(okscuda_ctx* ctx, int* status);
+/* Bounds-checked build only (libokscuda_bounds.so, compiled with
+ * -DOKS_BOUNDS_CHECK): ORs the error words of every kernel unit into *word
+ * after synchronising the device (bit 1 exchange buffer, 2 staging buffer,
+ * 4 column tile; 0 = no index ran out of range) and clears them when `clear`
+ * is set.  The normal build returns OKS_ENOTSUP.  No reference counterpart. */
+int okscuda_debug_bounds(okscuda_ctx* ctx, unsigned int* word, int clear);
 /* wavelet.rs:32-52 haar_forward / wavelet.rs:55-75 haar_inverse, batch x [ny, nx]. */
 int okscuda_haar_forward(okscuda_ctx* ctx, const okscuda_c64* d_in, okscuda_c64* d_out, int batch,
                          int ny, int nx);

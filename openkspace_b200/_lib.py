@@ -12,6 +12,9 @@ import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libokscuda.so")
+# the bounds-checked build of the same sources (tests select it through
+# OKSCUDA_LIB=bounds in a child process)
+BOUNDS_LIB_PATH = os.path.join(HERE, "libokscuda_bounds.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "okscuda.h")
 
 OKS_OK = 0
@@ -54,6 +57,7 @@ SIGNATURES = {
     "okscuda_centred_fft2": (_i, [_vp, _vp, _i, _i, _i, _i]),
     "okscuda_dft_rows": (_i, [_vp, _vp, _vp, _c.c_longlong, _i, _i, _i, _i]),
     "okscuda_tc_status": (_i, [_vp, _c.POINTER(_i)]),
+    "okscuda_debug_bounds": (_i, [_vp, _c.POINTER(_c.c_uint), _i]),
     "okscuda_haar_forward": (_i, [_vp, _vp, _vp, _i, _i, _i]),
     "okscuda_haar_inverse": (_i, [_vp, _vp, _vp, _i, _i, _i]),
     "okscuda_soft_threshold_details": (_i, [_vp, _vp, _i, _i, _i, _f]),
@@ -108,6 +112,16 @@ def load(build_if_missing: bool = True):
     global _lib
     if _lib is not None:
         return _lib
+    if os.environ.get("OKSCUDA_LIB") == "bounds":
+        if not os.path.exists(BOUNDS_LIB_PATH):
+            raise OSError(f"{BOUNDS_LIB_PATH} is missing: build it with `python -m openkspace_b200.build`")
+        L = ctypes.CDLL(BOUNDS_LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+        return L
     if build_if_missing:
         from . import build as _b
         if _b.needs_build():

@@ -3,9 +3,40 @@
 #include "ctx.h"
 
 // ====================================================================== C-ABI
+namespace oks {
+// Readers of the per-translation-unit error words of the bounds-checked
+// build (reg_fft.cuh registers one per unit at load; none in the normal build).
+static std::vector<unsigned (*)(int)>& bounds_readers() {
+    static std::vector<unsigned (*)(int)> v;
+    return v;
+}
+void bounds_register(unsigned (*reader)(int clear)) { bounds_readers().push_back(reader); }
+}  // namespace oks
+
 extern "C" {
 
-const char* okscuda_version(void) { return "okscuda 0.1 (sm_100a)"; }
+const char* okscuda_version(void) {
+#ifdef OKS_BOUNDS_CHECK
+    return "okscuda 0.1 (sm_100a, bounds-checked)";
+#else
+    return "okscuda 0.1 (sm_100a)";
+#endif
+}
+
+int okscuda_debug_bounds(okscuda_ctx* ctx, unsigned int* word, int clear) {
+    OKS_CHECK_CTX();
+    if (!word) return set_err(ctx, OKS_EINVAL, "debug_bounds: null word");
+    *word = 0;
+#ifndef OKS_BOUNDS_CHECK
+    (void)clear;
+    return set_err(ctx, OKS_ENOTSUP, "debug_bounds: not a bounds-checked build (libokscuda_bounds.so)");
+#else
+    OKS_CUDA(cudaStreamSynchronize(ctx->stream));
+    OKS_CUDA(cudaDeviceSynchronize());
+    for (auto r : oks::bounds_readers()) *word |= r(clear);
+    return OKS_OK;
+#endif
+}
 
 int okscuda_create(int device, okscuda_ctx** out) {
     if (!out) return OKS_EINVAL;

@@ -201,6 +201,7 @@ k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float
                 const long long off = (long long)r * nx + x0 + (q & 1);
                 const bool m = live && (((__ldg(rb + (r >> 5)) >> (r & 31)) & (cpair >> (q & 1)) & 1u) != 0);
                 if (m) mb |= 1u << e;
+                if (!OKS_IN(e * T + t, E * T, OKS_B_STAGE)) continue;
                 cp_async8(PY + e * T + t, m ? y + off : y, m ? 8u : 0u);
                 if (mode) cp_async8(PS + e * T + t, live ? S + off : S, live ? 8u : 0u);
             }
@@ -333,7 +334,7 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
             const int x = q >> 1;
             const long long off = (long long)(q & 1) * N + x;
             const bool on = live && ((__ldg(cb + (x >> 5)) >> (x & 31)) & 1u);
-            cp_async8(PF + e * T + t, on ? S + off : S, on ? 8u : 0u);
+            if (OKS_IN(e * T + t, E * T, OKS_B_STAGE)) cp_async8(PF + e * T + t, on ? S + off : S, on ? 8u : 0u);
         }
         cp_async_commit();
     };

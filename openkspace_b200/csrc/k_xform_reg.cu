@@ -32,9 +32,9 @@ __device__ __forceinline__ void cp_async16(float2* dst, const float2* src, uint3
 
 // Exchange buffer of one group, rounded up to 16 entries: padi keeps every
 // index below 2N rounded up to 16, lin16 (the first stage's output) below
-// 2N + 2N/16.
-template <class P>
-constexpr int xbuf() { return (P::SMEM_X + 15) / 16 * 16; }
+// 2N + 2N/16.  LIN = false: a kernel whose transforms use padi only.
+template <class P, bool LIN = true>
+constexpr int xbuf() { return ((LIN ? P::LIN16_END : P::PADI_END) + 15) / 16 * 16; }
 
 // Groups per CTA of the row kernel (warp-sized groups share a CTA).
 template <class P>
@@ -113,14 +113,16 @@ k_row_xform_reg(RowXformArgs a, const float2* __restrict__ gtw, const float2* __
             for (int k = t; k < N; k += T) {         // N chunks of two elements
                 const int c = k >= N / 2, x = 2 * (k - c * (N / 2));
                 const bool on = c ? k1 : k0;
-                cp_async16(ST + c * N + x, on ? (c ? r1 : r0) + x : a.in, on ? 16u : 0u);
+                if (OKS_IN(c * N + x + 1, 2 * N, OKS_B_STAGE))
+                    cp_async16(ST + c * N + x, on ? (c ? r1 : r0) + x : a.in, on ? 16u : 0u);
             }
         } else {
 #pragma unroll
             for (int k = t; k < 2 * N; k += T) {
                 const int c = k >= N, x = k - c * N;
                 const bool on = c ? k1 : k0;
-                cp_async8(ST + c * N + x, on ? (c ? r1 : r0) + x : a.in, on ? 8u : 0u);
+                if (OKS_IN(c * N + x, 2 * N, OKS_B_STAGE))
+                    cp_async8(ST + c * N + x, on ? (c ? r1 : r0) + x : a.in, on ? 8u : 0u);
             }
         }
         cp_async_commit();
@@ -135,7 +137,7 @@ k_row_xform_reg(RowXformArgs a, const float2* __restrict__ gtw, const float2* __
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int x = (t + TA * e) >> 1;
-            float2 v = live ? ST[cs * N + x] : make_float2(0.f, 0.f);
+            float2 v = (live && OKS_IN(cs * N + x, 2 * N, OKS_B_STAGE)) ? ST[cs * N + x] : make_float2(0.f, 0.f);
             if (a.centred && (x & 1)) v = make_float2(-v.x, -v.y);
             w[e] = v;
         }
@@ -163,7 +165,8 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
     constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
     constexpr int TC = 2 * G;                        // columns per tile
     constexpr int SS = TC + 2;                       // staging row stride (float2)
-    constexpr int GS = 2 * xbuf<P>() + 2;            // per-group stride of the A, B buffers
+    constexpr int XB = xbuf<P, false>();             // padi layout throughout (transform<..., L = false>)
+    constexpr int GS = 2 * XB + 2;                   // per-group stride of the A, B buffers
     static_assert(G == 2 || G == 4 || G == 8, "2, 4 or 8 column pairs per tile");
     extern __shared__ __align__(16) float2 sm[];
     const int g = threadIdx.x / T, t = threadIdx.x % T;
@@ -174,7 +177,7 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
     float2* ST = sm;                                 // [N][SS] staging of the next tile
     float2* AB = sm + N * SS;
     float2* A = AB + g * GS;
-    float2* B = A + xbuf<P>();
+    float2* B = A + XB;
     float2* TWs = AB + G * GS;
     float2* RT = TWs + tw_half<P>();
     const float2* TW = load_twiddles<P, SIGN>(TWs, gtw);
@@ -188,7 +191,8 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
         for (int k = threadIdx.x; k < N * G; k += T * G) {
             const int r = k / G, j = k % G;
             const bool on = x0 + 2 * j < a.nx;       // nx is even: chunks are whole
-            cp_async16(ST + r * SS + 2 * j, on ? base + (long long)r * a.nx + 2 * j : a.data, on ? 16u : 0u);
+            if (OKS_IN(r * SS + 2 * j + 1, N * SS, OKS_B_STAGE))
+                cp_async16(ST + r * SS + 2 * j, on ? base + (long long)r * a.nx + 2 * j : a.data, on ? 16u : 0u);
         }
         cp_async_commit();
     };
@@ -203,7 +207,8 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int q = t + TA * e, r = q >> 1;
-            float2 v = live ? ST[r * SS + 2 * g + (q & 1)] : make_float2(0.f, 0.f);
+            float2 v = (live && OKS_IN(r * SS + 2 * g + (q & 1), N * SS, OKS_B_STAGE)) ? ST[r * SS + 2 * g + (q & 1)]
+                                                                                      : make_float2(0.f, 0.f);
             if (a.centred && (r & 1)) v = make_float2(-v.x, -v.y);
             w[e] = v;
         }
@@ -215,7 +220,7 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int q = t + TA * e, k = q >> 1;
-                A[q] = w[e] * ((a.centred && (k & 1)) ? -sc_n2 : sc_n2);
+                if (OKS_IN(q, 2 * N, OKS_B_XCHG)) A[q] = w[e] * ((a.centred && (k & 1)) ? -sc_n2 : sc_n2);
             }
         }
         __syncthreads();
@@ -226,6 +231,7 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
         for (int k = threadIdx.x; k < N * G; k += T * G) {
             const int r = k / G, j = k % G;
             if (x0 + 2 * j >= a.nx) continue;
+            if (!OKS_IN(j * GS + 2 * r + 1, G * GS, OKS_B_STAGE)) continue;
             *reinterpret_cast<float4*>(base + (long long)r * a.nx + 2 * j) =
                 *reinterpret_cast<const float4*>(AB + j * GS + 2 * r);
         }
@@ -265,7 +271,7 @@ __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2
                 if (centred && (r & 1)) x = make_float2(-x.x, -x.y);
                 v[bb][j] = x;
             } else {
-                v[bb][j] = D[r * CW + c];
+                v[bb][j] = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? D[r * CW + c] : make_float2(0.f, 0.f);
             }
         }
     }
@@ -286,7 +292,7 @@ __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2
             const int o = ob + j * p;
             if constexpr (s == S - 1) {
                 if (on) col[o * nx] = v[bb][j] * ((centred && (o & 1)) ? -sc : sc);
-            } else {
+            } else if (OKS_IN(o * CW + c, N * CW, OKS_B_TILE)) {
                 D[o * CW + c] = v[bb][j];
             }
         }
@@ -366,8 +372,14 @@ static cudaError_t row_p(const RowXformArgs& a, cudaStream_t st) {
     constexpr int G = row_groups<P>();
     const float2 *tw, *rt;
     int nrt;
-    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
-    if (e != cudaSuccess) return e;
+    cudaError_t e = cudaSuccess;
+    if (a.tables) {   // caller-owned tables: nothing is allocated here
+        tw = a.tables;
+        rt = a.tables + Tw<P>::total();
+        nrt = a.tables_nroots;
+    } else if ((e = plan_tables<P>(&tw, &rt, &nrt)) != cudaSuccess) {
+        return e;
+    }
     const size_t smem = sizeof(float2) * ((size_t)G * 2 * (P::N + xbuf<P>()) + tw_half<P>() + nrt);
     const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_row_xform_reg<P, -1>)
                                 : reinterpret_cast<const void*>(k_row_xform_reg<P, +1>);
@@ -390,7 +402,7 @@ static cudaError_t col_pg(const ColXformArgs& a, cudaStream_t st) {
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
     const size_t smem =
-        sizeof(float2) * ((size_t)P::N * (2 * G + 2) + (size_t)G * (2 * xbuf<P>() + 2) + tw_half<P>() + nrt);
+        sizeof(float2) * ((size_t)P::N * (2 * G + 2) + (size_t)G * (2 * xbuf<P, false>() + 2) + tw_half<P>() + nrt);
     const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_col_xform_reg<P, G, -1>)
                                 : reinterpret_cast<const void*>(k_col_xform_reg<P, G, +1>);
     if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
@@ -490,6 +502,29 @@ cudaError_t launch_row_xform_reg(const RowXformArgs& a, int n, cudaStream_t st) 
         case 512: return reg::row_p<reg::S512>(a, st);
         case 640: return reg::row_p<reg::P640>(a, st);
         default: return cudaErrorInvalidValue;
+    }
+}
+
+namespace reg {
+template <class P>
+static int row_tables_p(float2* h, int cap, int* nroots) {
+    if (cap < Tw<P>::total() + P::N) return 0;   // roots: at most one per radix point
+    return host_plan_tables<P>(h, nroots);
+}
+}  // namespace reg
+
+// The plans here must be the ones launch_row_xform_reg picks per length.
+int row_xform_reg_tables(int n, float2* h, int cap, int* nroots) {
+    switch (n) {
+        case 128: return reg::row_tables_p<reg::S128>(h, cap, nroots);
+        case 192: return reg::row_tables_p<reg::R192>(h, cap, nroots);
+        case 256: return reg::row_tables_p<reg::S256>(h, cap, nroots);
+        case 320: return reg::row_tables_p<reg::S320>(h, cap, nroots);
+        case 368: return reg::row_tables_p<reg::S368>(h, cap, nroots);
+        case 384: return reg::row_tables_p<reg::S384>(h, cap, nroots);
+        case 512: return reg::row_tables_p<reg::S512>(h, cap, nroots);
+        case 640: return reg::row_tables_p<reg::P640>(h, cap, nroots);
+        default: return 0;
     }
 }
 

@@ -65,6 +65,10 @@ struct RowXformArgs {
     RowMasks keep;
     int reg = 1;         // register-resident kernel where a plan of length n exists
     int vec16 = 0;       // set by the launcher: rows start on 16-byte boundaries
+    // caller-owned device tables of the register plan (row_xform_reg_tables
+    // layout); null: the tables the library builds on first use
+    const float2* tables = nullptr;
+    int tables_nroots = 0;
 };
 cudaError_t launch_row_xform(const RowXformArgs& a, const DevPlan& pl, cudaStream_t st);
 
@@ -86,6 +90,10 @@ cudaError_t launch_col_xform(const ColXformArgs& a, const DevPlan& pl, cudaStrea
 // a register plan; even lengths only, the shifts folded into sign flips.
 bool xform_reg_supported(int n);
 cudaError_t launch_row_xform_reg(const RowXformArgs& a, int n, cudaStream_t st);
+// Host image of the tables the register row transform of length n uses
+// (RowXformArgs::tables): returns the number of float2 written to h (0 when
+// n has no register plan or cap is too small), the roots count in *nroots.
+int row_xform_reg_tables(int n, float2* h, int cap, int* nroots);
 cudaError_t launch_col_xform_reg(const ColXformArgs& a, cudaStream_t st);
 
 // One problem (one coil of one slice) of a batched launch with per-problem

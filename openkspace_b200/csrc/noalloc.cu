@@ -2,10 +2,11 @@
 // for callers that cannot allocate device memory -- applications that hand
 // all device memory to their own allocator (a framework memory pool, or a
 // scanner pipeline that reserves its budget at start-up and forbids device
-// allocation afterwards).  Nothing is allocated, on the device or the host:
-// the coil images, FFT tables, momentum weights and row mask live in one
-// file-scope device array, `g_noalloc_scratch`, which every GPU that loads
-// this library holds until the process exits.
+// allocation afterwards).  No device or pinned host memory is allocated: the
+// coil images, FFT tables (those of the register row transform included),
+// momentum weights and row mask live in one file-scope device array,
+// `g_noalloc_scratch`, which every GPU that loads this library holds until
+// the process exits.
 //
 // Host code never uses the array's name as an address: in host code it is a
 // host-side stand-in, and a kernel given it would fault (or, where the GPU
@@ -75,6 +76,8 @@ extern "C" int okscuda_cs_slice_noalloc(okscuda_ctx* ctx, const okscuda_c64* d_k
     const size_t o_rty = take(sizeof(float2) * (ny + 1));
     const size_t o_twx = take(sizeof(float2) * (2 * nx + 1));
     const size_t o_rtx = take(sizeof(float2) * (nx + 1));
+    constexpr int kRegTab = 4096 + 64;                // register row plan: twiddles + roots
+    const size_t o_reg = take(sizeof(float2) * kRegTab);
     if (off > kTableBytes) return set_err(ctx, OKS_ENOTSUP, "cs_slice_noalloc: tables exceed %zu bytes", kTableBytes);
 
     uint32_t* words = reinterpret_cast<uint32_t*>(g_host_tables + o_mask);
@@ -108,6 +111,13 @@ extern "C" int okscuda_cs_slice_noalloc(okscuda_ctx* ctx, const okscuda_c64* d_k
     py.roots = reinterpret_cast<float2*>(base + o_rty);
     px.tw = reinterpret_cast<float2*>(base + o_twx);
     px.roots = reinterpret_cast<float2*>(base + o_rtx);
+    // the register row transform's tables go into the array too (the
+    // library's own per-length tables would be allocated on first use)
+    int reg_nroots = 0;
+    const int reg_n = ctx->xform_reg && oks::xform_reg_supported(nx)
+                          ? oks::row_xform_reg_tables(nx, reinterpret_cast<float2*>(g_host_tables + o_reg), kRegTab,
+                                                      &reg_nroots)
+                          : 0;
     // pageable source: returns once the bytes are staged, so the host tables
     // may be rewritten by the next call
     OKS_CUDA(cudaMemcpyAsync(base, g_host_tables, off, cudaMemcpyHostToDevice, ctx->stream));
@@ -115,7 +125,9 @@ extern "C" int okscuda_cs_slice_noalloc(okscuda_ctx* ctx, const okscuda_c64* d_k
     float2* coils = reinterpret_cast<float2*>(base + kTableBytes);
     const oks::RowMasks rm{reinterpret_cast<const uint32_t*>(base + o_mask), wstride, 1};
     oks::RowXformArgs ra{};
-    ra.reg = ctx->xform_reg;
+    ra.reg = reg_n > 0 ? 1 : 0;
+    ra.tables = reg_n > 0 ? reinterpret_cast<const float2*>(base + o_reg) : nullptr;
+    ra.tables_nroots = reg_nroots;
     ra.in = reinterpret_cast<const float2*>(d_kspace);
     ra.out = coils;
     ra.nrows = (long long)nc * ny;

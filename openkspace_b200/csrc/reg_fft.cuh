@@ -14,6 +14,48 @@
 #include "fft_dev.cuh"
 #include "kernels.h"
 
+// Bounds-checked build (-DOKS_BOUNDS_CHECK, libokscuda_bounds.so): every
+// exchange-buffer and staging-buffer index is range-checked before use; an
+// index out of range sets a bit of a device error word (one per translation
+// unit, read through okscuda_debug_bounds) and the access is skipped.  No
+// assert and no trap: the kernel runs on and returns.  In the normal build
+// OKS_IN is the constant true and the checks compile away.
+#ifdef OKS_BOUNDS_CHECK
+namespace oks {
+static __device__ unsigned int g_bounds_word;
+__device__ __forceinline__ bool bounds_ok(long long i, long long n, unsigned code) {
+    if (i >= 0 && i < n) return true;
+    atomicOr(&g_bounds_word, code);
+    return false;
+}
+// Host side: this translation unit's word, read (and cleared) by
+// okscuda_debug_bounds through a registry defined in api.cu.
+void bounds_register(unsigned (*reader)(int clear));
+namespace {
+unsigned bounds_read_tu(int clear) {
+    unsigned v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_bounds_word, sizeof v) != cudaSuccess) return 0x80000000u;
+    if (clear) {
+        const unsigned z = 0;
+        cudaMemcpyToSymbol(g_bounds_word, &z, sizeof z);
+    }
+    return v;
+}
+struct BoundsRegistrar {
+    BoundsRegistrar() { bounds_register(&bounds_read_tu); }
+};
+static BoundsRegistrar g_bounds_registrar;
+}  // namespace
+}  // namespace oks
+#define OKS_IN(i, n, code) ::oks::bounds_ok((long long)(i), (long long)(n), (code))
+#else
+#define OKS_IN(i, n, code) true
+#endif
+// Error-word bits of the bounds-checked build.
+#define OKS_B_XCHG 1u      // exchange buffer (logical index outside [0, 2N))
+#define OKS_B_STAGE 2u     // staging / prefetch buffer
+#define OKS_B_TILE 4u      // column tile (lanes form)
+
 namespace oks {
 namespace reg {
 
@@ -139,6 +181,12 @@ struct Plan {
     // exchange buffer (float2): padi keeps every index below 2N rounded up
     // to 16, lin16 below 2N + 2N/16
     static constexpr int SMEM_X = 2 * N_ + (2 * N_) / 16 + 1;
+    // largest index each layout writes: padi stays inside the aligned block
+    // of 16 of its argument (< 2N rounded up to 16), lin16 reaches lin16(2N - 1)
+    static constexpr int PADI_END = (2 * N_ + 15) / 16 * 16;
+    static constexpr int LIN16_END = (2 * N_ - 1) + (2 * N_ - 1) / 16 + 1;
+    static_assert(PADI_END <= SMEM_X, "padi exchange indices overrun the buffer");
+    static_assert(LIN16_END <= SMEM_X, "lin16 exchange indices overrun the buffer");
 };
 
 // Twiddle table offsets: forward stage s at tw_f(s), inverse stage s at
@@ -250,6 +298,7 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
         const int ob = (i - k) * R + k;
         float2 a[H], b[H];
         const SrcIdx<LIN, NB> ix(i, c);
+        if (!OKS_IN(2 * (i + (R - 1) * NB) + c, 2 * P::N, OKS_B_XCHG)) return;
         const float2 x0 = src[ix(0)];
         float2 y0 = x0;
 #pragma unroll
@@ -264,6 +313,7 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
             b[j - 1] = u - w;
             y0 = y0 + a[j - 1];
         }
+        if (!OKS_IN(2 * (ob + (R - 1) * p) + c, 2 * P::N, OKS_B_XCHG)) return;
         if (s == 0) dst[padi(2 * ob + c)] = y0;
         // output pairs with compile-time q: the roots are immediates
         odd_pairs_for<SIGN, R, NS, 0>(s, a, b, x0, dst, ob, p, c);
@@ -285,6 +335,9 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
             constexpr int H = (R - 1) / 2;
             float2 a[H], b[H];
             const SrcIdx<LIN, NB> ix(i, c);
+            if (!OKS_IN(2 * (i + (R - 1) * NB) + c, 2 * P::N, OKS_B_XCHG) ||
+                !OKS_IN(2 * (ob + (R - 1) * p) + c, 2 * P::N, OKS_B_XCHG))
+                continue;
             const float2 x0 = src[ix(0)];
             float2 y0 = x0;
 #pragma unroll
@@ -316,6 +369,9 @@ __device__ __forceinline__ void stage_smem(const float2* __restrict__ src, float
         } else {
             float2 v[R];
             const SrcIdx<LIN, NB> ix(i, c);
+            if (!OKS_IN(2 * (i + (R - 1) * NB) + c, 2 * P::N, OKS_B_XCHG) ||
+                !OKS_IN(2 * (ob + (R - 1) * p) + c, 2 * P::N, OKS_B_XCHG))
+                continue;
 #pragma unroll
             for (int j = 0; j < R; ++j) {
                 float2 x = src[ix(j)];
@@ -372,7 +428,7 @@ __device__ __forceinline__ void stage_reg(float2* w, float2* __restrict__ dst, c
                     if (j2 > 0 && k2 > 0) y = twmul<SIGN>(y, tw2[k2 * (R2 - 1) + j2 - 1]);
                 }
                 const int v = 2 * (ob + j * p) + c;
-                dst[LINW ? lin16(v) : padi(v)] = y;
+                if (OKS_IN(v, 2 * P::N, OKS_B_XCHG)) dst[LINW ? lin16(v) : padi(v)] = y;
             }
         }
     }
@@ -393,7 +449,8 @@ __device__ __forceinline__ void stage_to_reg(const float2* __restrict__ src, flo
         float2 v[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            float2 x = src[padi(2 * (i + j * NB) + c)];
+            float2 x = OKS_IN(2 * (i + j * NB) + c, 2 * P::N, OKS_B_XCHG) ? src[padi(2 * (i + j * NB) + c)]
+                                                                           : make_float2(0.f, 0.f);
             if (j > 0) x = twmul<SIGN>(x, tw[i * (R - 1) + j - 1]);
             v[j] = x;
         }
@@ -563,6 +620,27 @@ static void host_tables(float2* tw, int* ntw) {
     *ntw = o;
 }
 
+// Host image of plan P's device tables: the twiddles (host_tables order)
+// followed by the roots of its generic odd radix (or one unit root).  Writes
+// Tw<P>::total() + *nroots entries to h (at most 4096 + 64).
+template <class P>
+static int host_plan_tables(float2* h, int* nroots) {
+    int ntw = 0;
+    host_tables<P>(h, &ntw);
+    int nrt = 1;
+    h[ntw] = make_float2(1.f, 0.f);
+    for (int s = 0; s < P::S; ++s)
+        if (P::R[s] % 2 == 1 && P::R[s] > 5) {   // generic odd radix: (cos, sin)(2 pi m / R)
+            nrt = P::R[s];
+            for (int m = 0; m < nrt; ++m) {
+                const double ang = 6.283185307179586476925286766559 * m / nrt;
+                h[ntw + m] = make_float2((float)cos(ang), (float)sin(ang));
+            }
+        }
+    *nroots = nrt;
+    return ntw + nrt;
+}
+
 // Twiddle / root tables of plan P on the current device, built on first use
 // and kept for the life of the process (a few KB per plan and device).
 template <class P>
@@ -576,22 +654,12 @@ static cudaError_t plan_tables(const float2** tw, const float2** roots, int* nro
     std::lock_guard<std::mutex> lk(mu);
     if (!d_tab[dev]) {
         static float2 h[4096 + 64];
-        int ntw = 0;
-        host_tables<P>(h, &ntw);
         int nrt = 1;
-        h[ntw] = make_float2(1.f, 0.f);
-        for (int s = 0; s < P::S; ++s)
-            if (P::R[s] % 2 == 1 && P::R[s] > 5) {   // generic odd radix: (cos, sin)(2 pi m / R)
-                nrt = P::R[s];
-                for (int m = 0; m < nrt; ++m) {
-                    const double ang = 6.283185307179586476925286766559 * m / nrt;
-                    h[ntw + m] = make_float2((float)cos(ang), (float)sin(ang));
-                }
-            }
+        const int total = host_plan_tables<P>(h, &nrt);
         float2* d = nullptr;
-        cudaError_t e = cudaMalloc(&d, sizeof(float2) * (ntw + nrt));
+        cudaError_t e = cudaMalloc(&d, sizeof(float2) * total);
         if (e != cudaSuccess) return e;
-        e = cudaMemcpy(d, h, sizeof(float2) * (ntw + nrt), cudaMemcpyHostToDevice);
+        e = cudaMemcpy(d, h, sizeof(float2) * total, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return e;
         d_tab[dev] = d;
         d_nrt[dev] = nrt;

@@ -372,10 +372,12 @@ def oversampling_apply(data: np.ndarray, encoded_x: int, recon_x: int) -> np.nda
 # --------------------------------------------------------------------------
 def csrss_from_kspace(kspace: np.ndarray, mask: np.ndarray, iters: int, lam: float,
                       three_d: bool = False, recon_matrix=None,
-                      return_coils: bool = False):
+                      return_coils: bool = False, workers: int = 1):
     """strategy.rs:817-891 on placed k-space ``[nc, nz, ny, nx]`` and
     ``mask [nz, ny, nx]``: optional kz decoupling, odd-dim fallback to
-    IFFT+RSS, per-slice per-coil FISTA, RSS, optional crop."""
+    IFFT+RSS, per-slice per-coil FISTA, RSS, optional crop.  ``workers`` > 1
+    solves the coils of a slice on that many threads (the coil solves are
+    independent, strategy.rs:850-869; the results are the same)."""
     k = np.asarray(kspace, dtype=np.complex128)
     if three_d:
         k = ifft1_inplace(k, 1)                          # strategy.rs:824-827
@@ -385,11 +387,20 @@ def csrss_from_kspace(kspace: np.ndarray, mask: np.ndarray, iters: int, lam: flo
         return maybe_crop(mag, recon_matrix) if recon_matrix is not None else mag
     out = np.zeros((nz, ny, nx), dtype=np.float64)
     coils = np.zeros_like(k) if return_coils else None
+    pool = None
+    if workers > 1 and nc > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        pool = ThreadPoolExecutor(min(workers, nc))
     for kz in range(nz):
-        x = fista_cs_single_coil(k[:, kz], mask[kz], iters, lam)
+        if pool is not None:
+            x = np.stack(list(pool.map(lambda c: fista_cs_single_coil(k[c, kz], mask[kz], iters, lam), range(nc))))
+        else:
+            x = fista_cs_single_coil(k[:, kz], mask[kz], iters, lam)
         out[kz] = rss_combine(x)
         if return_coils:
             coils[:, kz] = x
+    if pool is not None:
+        pool.shutdown()
     if recon_matrix is not None:
         out = maybe_crop(out, recon_matrix)
     return (out, coils) if return_coils else out

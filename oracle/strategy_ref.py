@@ -73,7 +73,8 @@ def read_kspace_with_mask(headers, data, encoded, ky_center, kz_center, preproce
 
 
 def csrss_reconstruct(headers, data, encoded, recon, ky_center, kz_center=0, iters=60, lam=0.01,
-                      remove_oversampling=True, prewhiten=True, fft_mode="auto", crop=True, phase_correct=True):
+                      remove_oversampling=True, prewhiten=True, fft_mode="auto", crop=True, phase_correct=True,
+                      workers=1):
     noise = [_acq(headers, data, i) for i in range(len(headers)) if int(headers[i]["flags"]) & NOISE]
     w = o64.prewhitener_from_noise(noise) if prewhiten else None
     pc = {}
@@ -102,4 +103,4 @@ def csrss_reconstruct(headers, data, encoded, recon, ky_center, kz_center=0, ite
     three_d = fft_mode == "3d" or (fft_mode == "auto" and any(int(headers[i]["kspace_encode_step_2"]) > 0
                                                               for i in img))
     return o64.csrss_from_kspace(k, filled, iters, lam, three_d=three_d,
-                                 recon_matrix=tuple(recon) if crop else None)
+                                 recon_matrix=tuple(recon) if crop else None, workers=workers)
