@@ -70,6 +70,11 @@ const char* okscuda_version(void);
  *                   SIMT FFT fused with the prox; 1 tensor-core DFT-as-GEMM
  *                   (split 3xBF16, okscuda_dft_rows engine 1) over the sampled
  *                   kx columns, with the prox in between (nx <= 2048)
+ *   "tc_gate_test"  tests of the bounded waits only: > 0 makes every
+ *                   tensor-core launch of okscuda_dft_rows first wait at most
+ *                   that many clock cycles on a device word nothing sets; it
+ *                   then records code 7 (okscuda_tc_status) and returns with
+ *                   no work issued.  0 (default) off
  *   "fista2d_streams" chunks of the 2-D-mask engine in flight at once, on
  *                   forked streams with separate state (1 to 8, default 2)
  *   "persist2d"     2-D register passes: 1 (default) = one CTA per resident
@@ -98,9 +103,13 @@ const char* okscuda_version(void);
  *   "xform_lanes"   register column transform with the lanes across the
  *                   columns (whole row segments straight from and to global
  *                   memory): 0 (default) for the lengths where it is faster
- *                   (192, 256, 320, 512), 1-4 a (columns, threads per column)
+ *                   (192, 256, 320, 384, 512, 640), 1-4 a (columns, threads per column)
  *                   form (16,32) (16,64) (8,64) (8,32) for every length but 368,
  *                   -1 never
+ *   "xform_lanes_pf" lanes form: 1 (default) = software-pipelined (the next
+ *                   tile is copied into shared memory with cp.async while the
+ *                   current one is transformed; even nx and 16-byte aligned
+ *                   data), 0 = stage 0 reads global memory directly
  * Any other name returns OKS_EINVAL. */
 int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value);
 /* Autotuner (no reference counterpart): times the plan and launch-shape
@@ -218,20 +227,49 @@ int okscuda_sense_cs(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_
                      int iters, float lambda, int walsh_window, int walsh_iters, int power_iters, float* d_mag,
                      okscuda_c64* d_maps, okscuda_c64* d_x, double* h_lipschitz);
 
+/* -------------------------------------------------------- output writers */
+/* openkspace-cli/src/main.rs:1147-1153 percentile(): the element at index
+ * round(pct / 100 * (n - 1)) (f32, half away from zero, clamped to n - 1) of
+ * d_vals[n] in ascending order, found on the device by radix select (exact,
+ * no sort); 0 for n = 0.  Synchronous: the value lands in *h_out. */
+int okscuda_percentile(okscuda_ctx* ctx, const float* d_vals, long long n, float pct, float* h_out);
+/* main.rs:1095-1110 write_png_linear (gamma = 0) and main.rs:1112-1140
+ * write_png_windowed (gamma = 1) pixel mapping on the device:
+ * d_out[i] = round(clamp((v - lo) / (hi - lo), 0, 1)^g * 255) with g = 1 or
+ * 0.9 and hi raised to at least lo + FLT_EPSILON. */
+int okscuda_window_u8(okscuda_ctx* ctx, const float* d_img, long long n, float lo, float hi, int gamma,
+                      uint8_t* d_out);
+/* main.rs:1033-1074 write_nifti_volume: NIfTI-1 single file (.nii) of the
+ * host volume h_vol[nz, ny, nx] (float32, x fastest): dim = [3, nx, ny, nz],
+ * 1 mm voxels, vox_offset 352, no extensions.  Host only (no context). */
+int okscuda_write_nifti(const float* h_vol, int nz, int ny, int nx, const char* path);
+/* The 8-bit grayscale PNG the reference writes with image::save_buffer
+ * (main.rs:1108, 1137): h_gray[height, width], zlib stream of stored deflate
+ * blocks.  Host only (no context). */
+int okscuda_write_png(const uint8_t* h_gray, int width, int height, const char* path);
+
 /* ------------------------------------------------------- request server */
 /* No counterpart in the reference (which reconstructs one file at a time).
- * A request is one slice (strategy.rs:850-880).  Each admitted request runs
- * upload -> FISTA -> RSS -> download on one stream of a pool, so requests
- * that arrive while others run overlap with them on the GPU.  Admission is
- * by an HBM budget and an in-flight limit: okscuda_server_submit returns
- * OKS_EAGAIN when the request does not fit now.  Host buffers of a request
- * must stay valid until it completes (pinned memory keeps the copies
+ * A request is one slice (strategy.rs:850-880).  Admission is by an HBM
+ * budget and an in-flight limit: okscuda_server_submit returns OKS_EAGAIN
+ * when the request does not fit now, and an admitted request is queued.
+ * Mode 0 (default, continuous batching): a dispatcher thread takes every
+ * queued request whenever one of the server's batch slots is free and runs
+ * them as one batched pass (okscuda_cs_batch: uploads, readout transforms,
+ * one column-engine launch per column length over the (coil, column pair)
+ * units of all of them, RSS, downloads) on that slot's streams; requests that
+ * arrive while batches run join the next one, and the slots' batches overlap
+ * on the GPU.  Mode 1: each request runs its own upload -> FISTA -> RSS ->
+ * download chain on one stream of a pool.  Results are the same in both modes
+ * and the same as the request solved alone.  Host buffers of a request must
+ * stay valid until it completes (pinned memory keeps the copies
  * asynchronous).  submit / poll / wait / stats are thread-safe. */
 typedef struct okscuda_server okscuda_server;
 typedef struct {
-    int max_inflight;              /* 0: 32                                    */
+    int max_inflight;              /* 0: 32 (queued + running)                 */
     size_t hbm_budget_bytes;       /* 0: half the free device memory           */
-    int n_streams;                 /* 0: 8                                     */
+    int n_streams;                 /* 0: 8 (mode 1), 2 batch slots (mode 0)    */
+    int mode;                      /* 0: continuous batching, 1: stream per request */
 } okscuda_server_cfg;
 typedef struct {
     const okscuda_c64* h_kspace;   /* [nc, ny, nx] host k-space, or NULL ...   */
@@ -240,6 +278,9 @@ typedef struct {
     int nc, ny, nx, iters;
     float lambda;
     float* h_rss;                  /* [ny, nx] host output                     */
+    long long coil_stride;         /* elements from one coil plane of the input to
+                                      the next (0: ny * nx); e.g. nz * ny * nx for
+                                      slice z of a [nc, nz, ny, nx] volume     */
 } okscuda_request;
 int okscuda_server_create(okscuda_ctx* ctx, const okscuda_server_cfg* cfg, okscuda_server** out);
 void okscuda_server_destroy(okscuda_server* srv);

@@ -69,6 +69,10 @@ SIGNATURES = {
     "okscuda_cs_batch": (_i, [_vp, _vp, _i]),
     "okscuda_sense_cs": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _i, _i, _i, _vp, _vp, _vp,
                               _c.POINTER(_c.c_double)]),
+    "okscuda_percentile": (_i, [_vp, _vp, _c.c_longlong, _f, _c.POINTER(_f)]),
+    "okscuda_window_u8": (_i, [_vp, _vp, _c.c_longlong, _f, _f, _i, _vp]),
+    "okscuda_write_nifti": (_i, [_vp, _i, _i, _i, _c.c_char_p]),
+    "okscuda_write_png": (_i, [_vp, _i, _i, _c.c_char_p]),
     "okscuda_server_create": (_i, [_vp, _vp, _c.POINTER(_vp)]),
     "okscuda_server_destroy": (None, [_vp]),
     "okscuda_server_submit": (_i, [_vp, _vp, _c.POINTER(_c.c_uint64)]),

@@ -134,12 +134,21 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value != 0 && value != 2 && value != 4 && value != 8)
             return set_err(ctx, OKS_EINVAL, "xform_tile: 0 (by length), 2, 4 or 8 column pairs");
         ctx->xform_tile = (int)value;
+    } else if (!std::strcmp(name, "xform_lanes_pf")) {
+        if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "xform_lanes_pf: 0 or 1");
+        ctx->xform_lanes_pf = (int)value;
     } else if (!std::strcmp(name, "xform_lanes")) {
         if (value < -1 || value > 4) return set_err(ctx, OKS_EINVAL, "xform_lanes: -1 off, 0 by length, 1 to 4");
         ctx->xform_lanes = (int)value;
     } else if (!std::strcmp(name, "fista2d_streams")) {
         if (value < 1 || value > 8) return set_err(ctx, OKS_EINVAL, "fista2d_streams: 1 to 8");
         ctx->fista2d_streams = (int)value;
+    } else if (!std::strcmp(name, "tc_gate_test")) {
+        // tests of the bounded waits: the next tensor-core launches wait at
+        // most `value` clock cycles on a device word nothing sets, then record
+        // the time-out (code 7) and return without work; 0 turns it off
+        if (value < 0) return set_err(ctx, OKS_EINVAL, "tc_gate_test must be >= 0");
+        ctx->tc_gate_cycles = value;
     } else if (!std::strcmp(name, "fista2d_chunk")) {
         if (value < 0) return set_err(ctx, OKS_EINVAL, "fista2d_chunk must be >= 0");
         ctx->fista2d_chunk = value;
@@ -237,7 +246,7 @@ int okscuda_centred_fft2(okscuda_ctx* ctx, okscuda_c64* d_data, int batch, int n
         OKS_CUDA(oks::launch_row_xform(ra, *px, ctx->stream));
     }
     oks::ColXformArgs ca{};
-    ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile; ca.lanes = ctx->xform_lanes;
+    ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile; ca.lanes = ctx->xform_lanes; ca.lanes_pf = ctx->xform_lanes_pf;
     ca.data = d; ca.nprob = batch; ca.ny = ny; ca.nx = nx; ca.prob_stride = (long long)ny * nx;
     ca.sign = inverse ? +1 : -1; ca.centred = 1;
     ca.scale = 1.0f / std::sqrt((float)ny * (float)nx);

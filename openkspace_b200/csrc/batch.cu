@@ -17,8 +17,12 @@ struct Item {
 
 }  // namespace
 
-extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs, int n) {
-    OKS_CHECK_CTX();
+// The batched pass on the context stream.  The column-length groups run on
+// forked streams: aux[k % naux] (joined back before the RSS), the context's
+// own auxiliary streams when aux is null.  The request server gives each of
+// its batch slots separate fork streams, so that batches overlap.
+int oks_cs_batch_core(okscuda_ctx* ctx, const okscuda_slice_req* reqs, int n, okscuda_ctx::Aux* aux, int naux,
+                      cudaEvent_t fork_ev) {
     if (n < 0 || (n > 0 && !reqs)) return set_err(ctx, OKS_EINVAL, "cs_batch: bad arguments");
     if (n == 0) return OKS_OK;
     int max_iters = 0, wstride = 1;
@@ -125,13 +129,19 @@ extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs,
     if (!rc && !table.empty()) {
         // fork: group k on aux stream k (ordered after everything so far)
         const int ng = (int)spans.size();
-        rc = ensure_aux_streams(ctx, ng);
-        if (!rc) OKS_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
+        if (!aux) {
+            rc = ensure_aux_streams(ctx, ng);
+            aux = ctx->aux.data();
+            naux = ng;
+            fork_ev = ctx->fork_ev;
+        }
+        if (!rc) OKS_CUDA(cudaEventRecord(fork_ev, ctx->stream));
         int k = 0;
         for (auto& g : groups) {
             if (rc) break;
-            cudaStream_t s = ctx->aux[k].stream;
-            OKS_CUDA(cudaStreamWaitEvent(s, ctx->fork_ev, 0));
+            okscuda_ctx::Aux& ax = aux[k % naux];
+            cudaStream_t s = ax.stream;
+            OKS_CUDA(cudaStreamWaitEvent(s, fork_ev, 0));
             oks::FistaColArgs fa{};
             fa.ny = g.first;
             fa.minv = 1.0f / (float)g.first;
@@ -147,8 +157,8 @@ extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs,
                 e = oks::launch_fista_col_reg(fa, ctx->reg_tables, s);
             }
             if (e != cudaSuccess) rc = cuda_err(ctx, e, "batched column engine");
-            OKS_CUDA(cudaEventRecord(ctx->aux[k].done, s));
-            OKS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->aux[k].done, 0));
+            OKS_CUDA(cudaEventRecord(ax.done, s));
+            OKS_CUDA(cudaStreamWaitEvent(ctx->stream, ax.done, 0));
             ++k;
         }
     }
@@ -176,4 +186,9 @@ extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs,
     if (mslot) stage_release(ctx, mslot);
     if (scratch) cudaFreeAsync(scratch, ctx->stream);
     return rc;
+}
+
+extern "C" int okscuda_cs_batch(okscuda_ctx* ctx, const okscuda_slice_req* reqs, int n) {
+    OKS_CHECK_CTX();
+    return oks_cs_batch_core(ctx, reqs, n, nullptr, 0, nullptr);
 }

@@ -75,11 +75,13 @@ struct okscuda_ctx {
     // sets), device column lists, error flag
     struct TcMat { void* hi = nullptr; void* lo = nullptr; int* in_cols = nullptr; int* out_cols = nullptr; };
     std::map<std::string, TcMat> tc_mats;
-    int* tc_err = nullptr;
+    int* tc_err = nullptr;                // [0] bounded-wait error word, [1] a word nothing sets (gate test)
+    long long tc_gate_cycles = 0;         // > 0: tensor-core launches first wait on tc_err[1] (tests only)
     int row_engine = 0;                   // 2-D engine row pass: 0 SIMT FFT, 1 tensor-core DFT
     int xform_reg = 1;                    // row/column transforms: 1 register kernels where a plan exists
     int xform_tile = 0;                   // column pairs per CTA of the register column transform (0: by length)
     int xform_lanes = 0;                  // lanes-across-columns form of it: 0 by length, 1..4, -1 off
+    int xform_lanes_pf = 1;               // lanes form: 1 = next tile staged in shared memory while transforming
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)
     cudaEvent_t fork_ev = nullptr;
@@ -310,8 +312,8 @@ inline int tc_matrix(okscuda_ctx* ctx, int n, int sign, int centred, const std::
 
 inline int tc_err_flag(okscuda_ctx* ctx) {
     if (!ctx->tc_err) {
-        OKS_CUDA(cudaMalloc(&ctx->tc_err, sizeof(int)));
-        OKS_CUDA(cudaMemset(ctx->tc_err, 0, sizeof(int)));
+        OKS_CUDA(cudaMalloc(&ctx->tc_err, 2 * sizeof(int)));
+        OKS_CUDA(cudaMemset(ctx->tc_err, 0, 2 * sizeof(int)));
     }
     return OKS_OK;
 }
@@ -322,5 +324,9 @@ using namespace oks_internal;
 
 // FISTA on nprob problems [nprob][ny][nx] (problem b uses host mask b % nmask),
 // dispatching to the fused column engine (ky-only masks) or the 2-D engine.
+// okscuda_cs_batch on the context stream with the column-length groups on
+// the fork streams aux[0..naux) (the context's own when aux is null).
+int oks_cs_batch_core(okscuda_ctx* ctx, const okscuda_slice_req* reqs, int n, okscuda_ctx::Aux* aux, int naux,
+                      cudaEvent_t fork_ev);
 extern "C" int oks_fista_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uint8_t* h_mask, int nmask,
                               long long nprob, int ny, int nx, int iters, float lambda, okscuda_c64* d_out);

@@ -50,6 +50,10 @@ extern "C" int okscuda_dft_rows(okscuda_ctx* ctx, const okscuda_c64* d_in, okscu
     a.b_hi = mat->hi; a.b_lo = mat->lo;
     a.scratch = scratch;
     a.err = ctx->tc_err;
+    if (ctx->tc_gate_cycles > 0) {   // bounded-wait test: a gate that never opens
+        a.gate = ctx->tc_err + 1;
+        a.gate_cycles = ctx->tc_gate_cycles;
+    }
     cudaError_t e;
     {
         ProfScope ps(ctx, "k_dft_tc");

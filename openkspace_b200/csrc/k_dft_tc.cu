@@ -150,6 +150,11 @@ struct Epilogue {
     int rows_per_prob;
     long long mask_offset;
     int mask_mod;
+    // start gate (tests of the bounded waits only): when non-null, the CTA
+    // waits at most gate_cycles for *gate != 0 before any copy or MMA is
+    // issued; on time-out it records code 7 and returns without work
+    const int* gate;
+    long long gate_cycles;
 };
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
@@ -175,6 +180,18 @@ k_dft_tc(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CU
     const uint32_t done = smem_u32(bars + 2 * NST + 4);
     const int ntiles = m_tiles * n_tiles;
 
+    if (ep.gate) {
+        __shared__ int s_abort;
+        if (threadIdx.x == 0) {
+            const long long t0 = clock64();
+            int open = *(volatile const int*)ep.gate;
+            while (!open && clock64() - t0 <= ep.gate_cycles) open = *(volatile const int*)ep.gate;
+            s_abort = open ? 0 : 1;
+            if (!open) atomicExch(err, 7);
+        }
+        __syncthreads();
+        if (s_abort) return;   // nothing issued, no tensor memory held
+    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < NST; ++s) {
             mbar_init(full0 + 8 * s, 1);
@@ -445,6 +462,8 @@ cudaError_t launch_dft_tc(const DftTcArgs& a, cudaStream_t st) {
     ep.rows_per_prob = a.rows_per_prob > 0 ? a.rows_per_prob : 1;
     ep.mask_offset = a.mask_offset;
     ep.mask_mod = a.mask_mod > 0 ? a.mask_mod : 1;
+    ep.gate = a.gate;
+    ep.gate_cycles = a.gate_cycles;
     const int n_tiles = np / BN, m_tiles = (int)((a.M + BM - 1) / BM);
     static int nsm = 0;
     if (!nsm) {

@@ -248,10 +248,17 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
 // middle stages work in place on one [N][CW] shared-memory tile (each thread
 // reads all its butterflies' inputs before the barrier that precedes the
 // writes).  Twiddles depend on the row only: one broadcast per half-warp.
-template <class P, int SIGN, int CW, int TPC, int s>
+// PF: stage 0 reads its inputs from the staging tile ST ([N][CW], filled by
+// cp.async while the previous tile was transformed) instead of global memory.
+// After every thread has read ST, refill() issues the next tile's copies.
+struct NoRefill {
+    __device__ void operator()() const {}
+};
+template <class P, int SIGN, int CW, int TPC, int s, bool PF = false, class F = NoRefill>
 __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2* __restrict__ TW,
                                             const float2* __restrict__ RT, float2* __restrict__ col, int nx,
-                                            bool on, bool centred, float sc, int c, int tc) {
+                                            bool on, bool centred, float sc, int c, int tc,
+                                            const float2* __restrict__ ST = nullptr, const F& refill = F()) {
     constexpr int S = P::S, N = P::N;
     constexpr int R = SIGN < 0 ? P::R[s] : P::R[S - 1 - s];
     constexpr int p = SIGN < 0 ? P::prod(s) : P::rprod(s);
@@ -267,7 +274,9 @@ __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2
         for (int j = 0; j < R; ++j) {
             const int r = b + j * NB;
             if constexpr (s == 0) {
-                float2 x = on ? col[r * nx] : make_float2(0.f, 0.f);   // N nx < 2^31 (launcher)
+                float2 x;
+                if constexpr (PF) x = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? ST[r * CW + c] : make_float2(0.f, 0.f);
+                else x = on ? col[r * nx] : make_float2(0.f, 0.f);   // N nx < 2^31 (launcher)
                 if (centred && (r & 1)) x = make_float2(-x.x, -x.y);
                 v[bb][j] = x;
             } else {
@@ -276,6 +285,10 @@ __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2
         }
     }
     if constexpr (s > 0 && s < S - 1) __syncthreads();   // in place: all inputs read before any output lands
+    if constexpr (PF && s == 0) {
+        __syncthreads();                                  // ST read by every thread: refill it
+        refill();
+    }
 #pragma unroll
     for (int bb = 0; bb < BPT; ++bb) {
         const int b = tc + TPC * bb;
@@ -315,7 +328,7 @@ constexpr int lanes_regs() {
     return most > 8 ? 96 : 64;
 }
 
-template <class P, int SIGN, int CW, int TPC>
+template <class P, int SIGN, int CW, int TPC, bool PF = false>
 __global__ void __launch_bounds__(CW * TPC, xform_min_blocks<CW * TPC, lanes_regs<P, TPC>()>())
 k_col_lanes(ColXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
     constexpr int N = P::N;
@@ -323,12 +336,50 @@ k_col_lanes(ColXformArgs a, const float2* __restrict__ gtw, const float2* __rest
     float2* D = sm;                                  // [N][CW]
     float2* TWs = sm + N * CW;
     float2* RT = TWs + tw_half<P>();
+    // PF: [N][CW] staging after the tables, on a 16-byte boundary
+    float2* ST = sm + (((size_t)N * CW + tw_half<P>() + roots_total + 1) & ~size_t(1));
     const float2* TW = load_twiddles<P, SIGN>(TWs, gtw);
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
     const int c = threadIdx.x % CW, tc = threadIdx.x / CW;
     const int ntx = (a.nx + CW - 1) / CW;
     const long long total = a.nprob * ntx;
     const float sc_n2 = (a.centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    if constexpr (PF) {
+        // software-pipelined form: tile u + gridDim.x is copied into ST
+        // (16-byte cp.async, whole row segments, L2 only) while tile u is
+        // transformed; stage 0 reads ST.  nx is even and the rows start on
+        // 16-byte boundaries (launcher), so chunks are whole.
+        auto issue = [&](long long u) {
+            const long long pr = u / ntx;
+            const int x0 = (int)(u - pr * ntx) * CW;
+            const float2* base = a.data + pr * a.prob_stride + x0;
+            for (int k = threadIdx.x; k < N * (CW / 2); k += CW * TPC) {
+                const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+                const bool on = x0 + j < a.nx;
+                if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                    cp_async16(ST + r * CW + j, on ? base + (long long)r * a.nx + j : a.data, on ? 16u : 0u);
+            }
+            cp_async_commit();
+        };
+        long long u = blockIdx.x;
+        if (u < total) issue(u);
+        for (; u < total; u += gridDim.x) {
+            const long long pr = u / ntx;
+            const int x = (int)(u - pr * ntx) * CW + c;
+            const bool on = x < a.nx;
+            float2* col = a.data + pr * a.prob_stride + (on ? x : 0);
+            cp_async_wait_all();
+            __syncthreads();                         // ST holds tile u; the last tile's final stage has read D
+            const long long un = u + gridDim.x;
+            auto refill = [&]() {
+                if (un < total) issue(un);
+            };
+            lanes_stage<P, SIGN, CW, TPC, 0, true>(D, TW, RT, col, (int)a.nx, on, a.centred != 0, sc_n2, c, tc, ST,
+                                                   refill);
+        }
+        cp_async_wait_all();
+        return;
+    }
     for (long long u = blockIdx.x; u < total; u += gridDim.x) {
         const long long pr = u / ntx;
         const int x = (int)(u - pr * ntx) * CW + c;
@@ -415,32 +466,45 @@ static cudaError_t col_pg(const ColXformArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <class P, int CW, int TPC>
-static cudaError_t col_lanes_k(const ColXformArgs& a, cudaStream_t st) {
+template <class P, int CW, int TPC, bool PF>
+static cudaError_t col_lanes_kp(const ColXformArgs& a, cudaStream_t st) {
     const float2 *tw, *rt;
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(float2) * ((size_t)P::N * CW + tw_half<P>() + nrt);
-    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_col_lanes<P, -1, CW, TPC>)
-                                : reinterpret_cast<const void*>(k_col_lanes<P, +1, CW, TPC>);
+    size_t elems = (size_t)P::N * CW + tw_half<P>() + nrt;
+    if (PF) elems = ((elems + 1) & ~size_t(1)) + (size_t)P::N * CW;
+    const size_t smem = sizeof(float2) * elems;
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_col_lanes<P, -1, CW, TPC, PF>)
+                                : reinterpret_cast<const void*>(k_col_lanes<P, +1, CW, TPC, PF>);
     if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
     const long long tiles = a.nprob * ((a.nx + CW - 1) / CW);
     long long grid = tiles;
     const long long cap = (long long)ctas_per_sm(fn, CW * TPC, smem) * sm_count();
     if (grid > cap) grid = cap;
-    if (a.sign < 0) k_col_lanes<P, -1, CW, TPC><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw, rt, nrt);
-    else k_col_lanes<P, +1, CW, TPC><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw, rt, nrt);
+    if (a.sign < 0) k_col_lanes<P, -1, CW, TPC, PF><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw, rt, nrt);
+    else k_col_lanes<P, +1, CW, TPC, PF><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw, rt, nrt);
     return cudaGetLastError();
 }
 
-// Lanes form per column length, from B200 measurements of both column
-// kernels on 1 GiB of planes (GB/s, lanes form / tiles): 192 4361 / 3404,
-// 256 4863 / 4587, 320 3526 / 3224, 512 4206 / 4177; the tiles stay ahead at
-// 128 (5043 / 3907), 384 (4108 / 3788) and 640 (3706 / 2819).
+// The pipelined form needs whole 16-byte chunks: even nx, 16-byte aligned data.
+template <class P, int CW, int TPC>
+static cudaError_t col_lanes_k(const ColXformArgs& a, cudaStream_t st) {
+    const bool pf_ok = (a.nx % 2) == 0 && (reinterpret_cast<uintptr_t>(a.data) & 15) == 0;
+    if (a.lanes_pf > 0 && pf_ok) return col_lanes_kp<P, CW, TPC, true>(a, st);
+    return col_lanes_kp<P, CW, TPC, false>(a, st);
+}
+
+// Lanes form per column length, from B200 measurements on 1 GiB of planes
+// (GB/s of the column pass; pipelined lanes form at its best (width,
+// threads) choice / direct lanes form / tiles): 192 5074 / 4346 / 3368 (form
+// 4), 256 5065 / 4807 / 4535 (form 4), 320 4528 / 3514 / 3177 (form 1), 384
+// 4581 / 3782 / 4063 (form 3), 512 4805 / 4154 / 4144 (form 1), 640 4078 /
+// 2784 / 3689 (form 2).  The tiles stay at 128 (5043 / 3907 against the direct
+// lanes form) and at 368, whose radix-23 plan has no lanes form.
 template <class P>
 constexpr int lanes_default() {
-    return P::N == 256 ? 1 : (P::N == 192 || P::N == 320 || P::N == 512) ? 4 : 0;
+    return (P::N == 192 || P::N == 256) ? 4 : (P::N == 320 || P::N == 512) ? 1 : P::N == 384 ? 3 : P::N == 640 ? 2 : 0;
 }
 
 // Columns across the lanes: tile width CW and threads per column TPC
@@ -461,7 +525,7 @@ template <class P>
 static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
     if constexpr (!big_odd_plan<P>()) {
         // columns across the lanes (in-problem offsets in 32 bits) where that
-        // form measured faster than the tiles: 192, 256, 320, 512
+        // form measured faster than the tiles: 192, 256, 320, 384, 512, 640
         const int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
         if (a.tile == 0 && lanes > 0 && (long long)P::N * a.nx < (1ll << 31)) return col_lanes<P>(a, lanes, st);
     }

@@ -83,6 +83,7 @@ struct ColXformArgs {
     int reg = 1;         // register-resident kernel where a plan of length ny exists
     int tile = 0;        // column pairs per CTA of that kernel (0: by length; 2, 4, 8)
     int lanes = 0;       // lanes-across-columns form: 0 by length, 1..4 a (width, threads) choice, -1 off
+    int lanes_pf = 1;    // lanes form: 1 = next tile staged in shared memory (cp.async) during the current one
 };
 cudaError_t launch_col_xform(const ColXformArgs& a, const DevPlan& pl, cudaStream_t st);
 
@@ -290,6 +291,10 @@ struct DftTcArgs {
     const void* b_lo;
     void* scratch;            // dft_tc_scratch_bytes(M, nin)
     int* err;                 // bounded-wait error flag
+    // bounded-wait test: a device word the kernel waits on (at most
+    // gate_cycles) before any work; null in every production launch
+    const int* gate = nullptr;
+    long long gate_cycles = 0;
 };
 cudaError_t launch_dft_tc(const DftTcArgs& a, cudaStream_t st);
 // Haar prox + momentum between the two tensor-core transforms of the 2-D

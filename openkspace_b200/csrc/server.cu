@@ -1,15 +1,33 @@
-// Request server for FISTA-CS slices (continuous batching on one device).
+// Request server for FISTA-CS slices on one device.
 //
-// Each admitted request runs its own chain -- upload, row IDFT, fused column
-// FISTA (or the 2-D engine), RSS, download -- on one stream of a pool, so
-// requests that arrive while others are running overlap with them on the
-// GPU.  Admission is by an HBM budget and an in-flight limit: a request that
-// does not fit is refused with OKS_EAGAIN and may be resubmitted once others
+// Admission is by an HBM budget and an in-flight limit: a request that does
+// not fit is refused with OKS_EAGAIN and may be resubmitted once others
 // complete.  Device memory per request comes from the stream-ordered pool
-// (cudaMallocAsync) and is returned stream-ordered when the chain ends.
-// All entry points are serialised by one mutex, so any host thread may call
-// them; waits are bounded by the caller's timeout.
+// (cudaMallocAsync) and is returned stream-ordered when its work ends.
+//
+// Mode 0, continuous batching (default): submit only queues the request.  A
+// dispatcher thread takes every queued request whenever one of the batch
+// slots is free and runs them together as one batched pass on that slot's
+// stream -- uploads, readout transforms, one register column-engine launch
+// per column length over the (coil, column pair) units of every request of
+// the batch (longest first, the lengths on the slot's own fork streams), RSS,
+// downloads.  Requests that arrive while batches run join the next batch;
+// the slots' batches overlap on the GPU, so one batch's launch tails and
+// copies overlap another's kernels.  A batch ends with a host callback that
+// wakes the dispatcher.
+//
+// Mode 1: each admitted request runs its own upload -> FISTA -> RSS ->
+// download chain on one stream of a pool, as soon as it is submitted.
+//
+// Both modes compute every (coil, column pair) unit with the same kernels and
+// plans as the per-slice drop-in, so a result does not depend on what else is
+// in flight.  All entry points are serialised by one mutex, so any host
+// thread may call them; waits are bounded by the caller's timeout.  In mode 0
+// the dispatcher uses the server's context: other work belongs on another
+// context while the server exists.
 #include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -19,43 +37,60 @@
 struct okscuda_server {
     okscuda_ctx* ctx = nullptr;
     std::mutex mu;
-    std::vector<cudaStream_t> streams;
+    int mode = 0;
+    std::vector<cudaStream_t> streams;     // mode 1: the request streams
     int next_stream = 0;
     int max_inflight = 32;
     size_t budget = 0;
     size_t reserved = 0;
     uint64_t next_id = 1;
     struct Req {
+        okscuda_request q{};
+        int state = 0;                     // 0 queued, 1 launched, 2 finished
         cudaEvent_t done = nullptr;
         size_t bytes = 0;
         int status = OKS_OK;
-        bool finished = false;
         // pageable output: the device result goes to a pinned bounce buffer
         // and is copied to the caller's buffer when completion is observed
         void* bounce = nullptr;
-        size_t bounce_bytes = 0;
-        void* user_out = nullptr;
+        size_t bounce_cap = 0;
     };
     std::unordered_map<uint64_t, Req> reqs;
+    std::deque<uint64_t> pending;          // mode 0: admitted, not yet launched
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<void*, size_t>> pinned_pool;   // free pinned bounce buffers
     long long completed = 0;
+    // mode 0: batch slots and the dispatcher
+    struct Slot {
+        cudaStream_t st = nullptr;
+        okscuda_ctx::Aux aux[4];           // fork streams of the column-length groups
+        cudaEvent_t fork = nullptr;
+        cudaEvent_t done = nullptr;
+        bool busy = false;
+    };
+    std::vector<Slot> slots;
+    std::condition_variable cv;
+    std::thread dispatcher;
+    bool stop = false;
+    long long batches = 0;
 };
 
 namespace {
+
+constexpr int kMaxBatchRequests = 64;
 
 // Marks finished requests and returns their reservations (mutex held).
 void reap(okscuda_server* s) {
     for (auto& kv : s->reqs) {
         auto& r = kv.second;
-        if (r.finished) continue;
+        if (r.state != 1) continue;
         const cudaError_t q = cudaEventQuery(r.done);
         if (q == cudaErrorNotReady) continue;
-        r.finished = true;
-        if (q != cudaSuccess) r.status = OKS_ECUDA;
+        r.state = 2;
+        if (q != cudaSuccess && r.status == OKS_OK) r.status = OKS_ECUDA;
         if (r.bounce) {
-            if (r.status == OKS_OK) std::memcpy(r.user_out, r.bounce, r.bounce_bytes);
-            s->pinned_pool.push_back({r.bounce, r.bounce_bytes});
+            if (r.status == OKS_OK) std::memcpy(r.q.h_rss, r.bounce, sizeof(float) * (size_t)r.q.ny * r.q.nx);
+            s->pinned_pool.push_back({r.bounce, r.bounce_cap});
             r.bounce = nullptr;
         }
         s->reserved -= r.bytes;
@@ -98,6 +133,177 @@ cudaEvent_t take_event(okscuda_server* s) {
     return e;
 }
 
+size_t request_bytes(const okscuda_request* q) {
+    const size_t N = (size_t)q->ny * q->nx;
+    const size_t kbytes = sizeof(float2) * (size_t)q->nc * N;
+    // work copy of the k-space (solved in place) + RSS + the 2-D engine's
+    // worst-case scratch
+    return kbytes + sizeof(float) * N + 3 * kbytes;
+}
+
+// The request's k-space on stream st: *work (allocated here) receives the
+// coil images, *src is what the FISTA pass reads -- the caller's contiguous
+// device k-space (left unmodified), else *work after the upload or the
+// gather of coil planes `coil_stride` apart.  Mutex held.
+int stage_input(okscuda_server* s, const okscuda_request* q, cudaStream_t st, const okscuda_c64** src,
+                okscuda_c64** work) {
+    okscuda_ctx* ctx = s->ctx;
+    const size_t N = (size_t)q->ny * q->nx;
+    const size_t plane = sizeof(float2) * N, kbytes = plane * (size_t)q->nc;
+    const long long cs = q->coil_stride > 0 ? q->coil_stride : (long long)N;
+    void* w = nullptr;
+    cudaError_t e = cudaMallocAsync(&w, kbytes, st);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "server: coil buffer");
+    *work = static_cast<okscuda_c64*>(w);
+    *src = *work;
+    if (q->h_kspace) {
+        if (cs == (long long)N) e = cudaMemcpyAsync(w, q->h_kspace, kbytes, cudaMemcpyHostToDevice, st);
+        else e = cudaMemcpy2DAsync(w, plane, q->h_kspace, sizeof(float2) * (size_t)cs, plane, q->nc,
+                                   cudaMemcpyHostToDevice, st);
+    } else if (cs == (long long)N) {
+        *src = q->d_kspace;
+    } else {
+        e = cudaMemcpy2DAsync(w, plane, q->d_kspace, sizeof(float2) * (size_t)cs, plane, q->nc,
+                              cudaMemcpyDeviceToDevice, st);
+    }
+    if (e != cudaSuccess) {
+        cudaFreeAsync(w, st);
+        return cuda_err(ctx, e, "server: k-space upload");
+    }
+    return OKS_OK;
+}
+
+// RSS [ny, nx] on the device -> the caller's buffer (directly when pinned,
+// else through a pinned bounce buffer copied out when completion is seen).
+int stage_output(okscuda_server* s, okscuda_server::Req& r, const float* drss, cudaStream_t st) {
+    const size_t bytes = sizeof(float) * (size_t)r.q.ny * r.q.nx;
+    void* dst = r.q.h_rss;
+    if (!is_pinned(r.q.h_rss)) {
+        r.bounce = take_pinned(s, bytes, &r.bounce_cap);
+        if (!r.bounce) return set_err(s->ctx, OKS_ENOMEM, "server: pinned bounce buffer");
+        dst = r.bounce;
+    }
+    const cudaError_t e = cudaMemcpyAsync(dst, drss, bytes, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_err(s->ctx, e, "server: download");
+    return OKS_OK;
+}
+
+// Mode 1: the request's own chain on the next stream of the pool.  Mutex held.
+int run_chain(okscuda_server* s, okscuda_server::Req& r) {
+    okscuda_ctx* ctx = s->ctx;
+    const okscuda_request* q = &r.q;
+    cudaStream_t st = s->streams[s->next_stream];
+    s->next_stream = (s->next_stream + 1) % (int)s->streams.size();
+    cudaStream_t saved = ctx->stream;
+    ctx->stream = st;
+    const okscuda_c64* src = nullptr;
+    okscuda_c64* work = nullptr;
+    void* drss = nullptr;
+    int rc = stage_input(s, q, st, &src, &work);
+    if (!rc) {
+        const cudaError_t e = cudaMallocAsync(&drss, sizeof(float) * (size_t)q->ny * q->nx, st);
+        if (e != cudaSuccess) rc = cuda_err(ctx, e, "server: RSS buffer");
+    }
+    if (!rc) rc = oks_fista_core(ctx, src, q->h_mask, 1, q->nc, q->ny, q->nx, q->iters, q->lambda, work);
+    if (!rc) rc = okscuda_rss_crop(ctx, work, q->nc, q->ny, q->nx, q->ny, q->nx, static_cast<float*>(drss));
+    if (!rc) rc = stage_output(s, r, static_cast<const float*>(drss), st);
+    if (work) cudaFreeAsync(work, st);
+    if (drss) cudaFreeAsync(drss, st);
+    r.done = take_event(s);
+    cudaEventRecord(r.done, st);
+    ctx->stream = saved;
+    r.state = 1;
+    r.status = rc;
+    return rc;
+}
+
+void CUDART_CB wake_dispatcher(void* p) { static_cast<okscuda_server*>(p)->cv.notify_all(); }
+
+// Mode 0: the first free batch slot (-1 when every slot is busy).  Mutex held.
+int free_slot(okscuda_server* s) {
+    for (size_t k = 0; k < s->slots.size(); ++k) {
+        auto& sl = s->slots[k];
+        if (sl.busy && cudaEventQuery(sl.done) != cudaErrorNotReady) sl.busy = false;
+        if (!sl.busy) return (int)k;
+    }
+    return -1;
+}
+
+// Mode 0: every queued request (up to kMaxBatchRequests) as one batched pass
+// on slot k.  Mutex held.
+void launch_batch(okscuda_server* s, int k) {
+    okscuda_ctx* ctx = s->ctx;
+    auto& sl = s->slots[k];
+    cudaStream_t saved = ctx->stream;
+    ctx->stream = sl.st;
+    std::vector<uint64_t> ids;
+    std::vector<okscuda_slice_req> br;
+    std::vector<void*> bufs;
+    while (!s->pending.empty() && (int)ids.size() < kMaxBatchRequests) {
+        const uint64_t id = s->pending.front();
+        s->pending.pop_front();
+        auto& r = s->reqs[id];
+        const okscuda_request* q = &r.q;
+        const okscuda_c64* src = nullptr;
+        okscuda_c64* work = nullptr;
+        void* drss = nullptr;
+        int rc = stage_input(s, q, sl.st, &src, &work);
+        if (!rc) {
+            const cudaError_t e = cudaMallocAsync(&drss, sizeof(float) * (size_t)q->ny * q->nx, sl.st);
+            if (e != cudaSuccess) {
+                rc = cuda_err(ctx, e, "server: RSS buffer");
+                cudaFreeAsync(work, sl.st);
+            }
+        }
+        if (rc) {   // this request fails alone; the rest of the batch goes on
+            r.status = rc;
+            r.done = take_event(s);
+            cudaEventRecord(r.done, sl.st);
+            r.state = 1;
+            continue;
+        }
+        okscuda_slice_req b{};
+        b.d_kspace = src;
+        b.h_mask = q->h_mask;
+        b.nc = q->nc; b.ny = q->ny; b.nx = q->nx; b.iters = q->iters; b.lambda = q->lambda;
+        b.d_rss = static_cast<float*>(drss);
+        b.d_coils = work;
+        br.push_back(b);
+        ids.push_back(id);
+        bufs.push_back(work);
+        bufs.push_back(drss);
+    }
+    const int rc = br.empty() ? OKS_OK : oks_cs_batch_core(ctx, br.data(), (int)br.size(), sl.aux, 4, sl.fork);
+    for (size_t i = 0; i < ids.size(); ++i) {
+        auto& r = s->reqs[ids[i]];
+        r.status = rc;
+        if (!rc) r.status = stage_output(s, r, br[i].d_rss, sl.st);
+        r.done = take_event(s);
+        cudaEventRecord(r.done, sl.st);
+        r.state = 1;
+    }
+    for (void* p : bufs) cudaFreeAsync(p, sl.st);
+    cudaEventRecord(sl.done, sl.st);
+    cudaLaunchHostFunc(sl.st, wake_dispatcher, s);
+    sl.busy = true;
+    s->batches += 1;
+    ctx->stream = saved;
+}
+
+void dispatch_loop(okscuda_server* s) {
+    cudaSetDevice(s->ctx->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        // woken by submit and by the end of a batch; the time-out only
+        // guards against a missed wake-up
+        s->cv.wait_for(lk, std::chrono::milliseconds(5),
+                       [&] { return s->stop || (!s->pending.empty() && free_slot(s) >= 0); });
+        if (s->stop) break;
+        const int k = s->pending.empty() ? -1 : free_slot(s);
+        if (k >= 0) launch_batch(s, k);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -106,22 +312,50 @@ int okscuda_server_create(okscuda_ctx* ctx, const okscuda_server_cfg* cfg, okscu
     OKS_CHECK_CTX();
     if (!out) return set_err(ctx, OKS_EINVAL, "server_create: null out");
     *out = nullptr;
+    const int mode = cfg ? cfg->mode : 0;
+    if (mode != 0 && mode != 1) return set_err(ctx, OKS_EINVAL, "server_create: mode %d (0 or 1)", mode);
     auto* s = new okscuda_server();
     s->ctx = ctx;
-    const int ns = (cfg && cfg->n_streams > 0) ? cfg->n_streams : 8;
+    s->mode = mode;
     s->max_inflight = (cfg && cfg->max_inflight > 0) ? cfg->max_inflight : 32;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     s->budget = (cfg && cfg->hbm_budget_bytes > 0) ? cfg->hbm_budget_bytes : free_b / 2;
-    for (int i = 0; i < ns; ++i) {
-        cudaStream_t st;
-        cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-        if (e != cudaSuccess) {
-            for (auto x : s->streams) cudaStreamDestroy(x);
-            delete s;
-            return cuda_err(ctx, e, "server streams");
+    auto fail = [&](cudaError_t e, const char* what) {
+        for (auto x : s->streams) cudaStreamDestroy(x);
+        for (auto& sl : s->slots) {
+            if (sl.st) cudaStreamDestroy(sl.st);
+            for (auto& a : sl.aux) {
+                if (a.stream) cudaStreamDestroy(a.stream);
+                if (a.done) cudaEventDestroy(a.done);
+            }
+            if (sl.fork) cudaEventDestroy(sl.fork);
+            if (sl.done) cudaEventDestroy(sl.done);
         }
-        s->streams.push_back(st);
+        delete s;
+        return cuda_err(ctx, e, what);
+    };
+    if (mode == 1) {
+        const int ns = (cfg && cfg->n_streams > 0) ? cfg->n_streams : 8;
+        for (int i = 0; i < ns; ++i) {
+            cudaStream_t st;
+            cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+            if (e != cudaSuccess) return fail(e, "server streams");
+            s->streams.push_back(st);
+        }
+    } else {
+        const int nslots = (cfg && cfg->n_streams > 0) ? std::min(cfg->n_streams, 8) : 2;
+        s->slots.resize(nslots);
+        for (auto& sl : s->slots) {
+            cudaError_t e = cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.fork, cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+            for (auto& a : sl.aux) {
+                if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&a.stream, cudaStreamNonBlocking);
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a.done, cudaEventDisableTiming);
+            }
+            if (e != cudaSuccess) return fail(e, "server batch slots");
+        }
     }
     // keep freed pool memory for reuse between requests
     cudaMemPool_t pool;
@@ -129,21 +363,38 @@ int okscuda_server_create(okscuda_ctx* ctx, const okscuda_server_cfg* cfg, okscu
         uint64_t thr = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
+    if (mode == 0) s->dispatcher = std::thread(dispatch_loop, s);
     *out = s;
     return OKS_OK;
 }
 
 void okscuda_server_destroy(okscuda_server* s) {
     if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->dispatcher.joinable()) s->dispatcher.join();
     cudaSetDevice(s->ctx->device);
     for (auto st : s->streams) cudaStreamSynchronize(st);
+    for (auto& sl : s->slots) cudaStreamSynchronize(sl.st);
     for (auto& kv : s->reqs) {
-        cudaEventDestroy(kv.second.done);
+        if (kv.second.done) cudaEventDestroy(kv.second.done);
         if (kv.second.bounce) cudaFreeHost(kv.second.bounce);
     }
     for (auto& b : s->pinned_pool) cudaFreeHost(b.first);
     for (auto e : s->ev_pool) cudaEventDestroy(e);
     for (auto st : s->streams) cudaStreamDestroy(st);
+    for (auto& sl : s->slots) {
+        for (auto& a : sl.aux) {
+            cudaStreamDestroy(a.stream);
+            cudaEventDestroy(a.done);
+        }
+        cudaEventDestroy(sl.fork);
+        cudaEventDestroy(sl.done);
+        cudaStreamDestroy(sl.st);
+    }
     delete s;
 }
 
@@ -153,80 +404,38 @@ int okscuda_server_submit(okscuda_server* s, const okscuda_request* q, uint64_t*
     okscuda_ctx* ctx = s->ctx;
     OKS_CHECK_CTX();
     if ((!q->h_kspace && !q->d_kspace) || !q->h_mask || !q->h_rss || q->nc <= 0 || q->ny <= 0 || q->nx <= 0 ||
-        q->iters < 0)
+        q->iters < 0 || (q->coil_stride != 0 && q->coil_stride < (long long)q->ny * q->nx))
         return set_err(ctx, OKS_EINVAL, "server_submit: bad request");
     if (q->ny % 2 || q->nx % 2)
         return set_err(ctx, OKS_EODD, "CS: Ny (%d) and Nx (%d) must both be even for Haar wavelet", q->ny, q->nx);
     reap(s);
-    const size_t N = (size_t)q->ny * q->nx;
-    const size_t kbytes = sizeof(float2) * (size_t)q->nc * N;
-    // k-space (solved in place) + RSS + the 2-D engine's worst-case scratch
-    const size_t need = kbytes + sizeof(float) * N + 3 * kbytes;
+    const size_t need = request_bytes(q);
     int inflight = 0;
-    for (auto& kv : s->reqs) inflight += kv.second.finished ? 0 : 1;
+    for (auto& kv : s->reqs) inflight += kv.second.state != 2 ? 1 : 0;
     if (inflight >= s->max_inflight || s->reserved + need > s->budget)
         return set_err(ctx, OKS_EAGAIN, "admission refused: %d in flight, %zu of %zu bytes reserved", inflight,
                        s->reserved, s->budget);
-    cudaStream_t st = s->streams[s->next_stream];
-    s->next_stream = (s->next_stream + 1) % (int)s->streams.size();
-    cudaStream_t saved = ctx->stream;
-    ctx->stream = st;   // the request's chain runs on its own stream
-    int rc = OKS_OK;
-    void* dk = nullptr;
-    void* drss = nullptr;
-    cudaError_t e = cudaSuccess;
-    if (q->h_kspace) {
-        e = cudaMallocAsync(&dk, kbytes, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(dk, q->h_kspace, kbytes, cudaMemcpyHostToDevice, st);
-    } else {
-        dk = const_cast<okscuda_c64*>(q->d_kspace);
-    }
-    if (e == cudaSuccess) e = cudaMallocAsync(&drss, sizeof(float) * N, st);
-    if (e != cudaSuccess) rc = cuda_err(ctx, e, "server_submit: device memory");
-    void* coils = nullptr;
-    if (!rc && !q->h_kspace) {
-        // device-resident input is left untouched: solve into a copy
-        e = cudaMallocAsync(&coils, kbytes, st);
-        if (e != cudaSuccess) rc = cuda_err(ctx, e, "server_submit: coil buffer");
-    }
-    okscuda_c64* work = static_cast<okscuda_c64*>(coils ? coils : dk);
-    if (!rc) rc = oks_fista_core(ctx, static_cast<const okscuda_c64*>(dk), q->h_mask, 1, q->nc, q->ny, q->nx,
-                                 q->iters, q->lambda, work);
-    if (!rc) rc = okscuda_rss_crop(ctx, work, q->nc, q->ny, q->nx, q->ny, q->nx, static_cast<float*>(drss));
-    void* bounce = nullptr;
-    size_t bounce_cap = 0;
-    if (!rc) {
-        // a copy into pageable memory would block this call until the chain
-        // ends; bounce through pinned memory instead
-        void* dst = q->h_rss;
-        if (!is_pinned(q->h_rss)) {
-            bounce = take_pinned(s, sizeof(float) * N, &bounce_cap);
-            if (!bounce) rc = set_err(ctx, OKS_ENOMEM, "server_submit: pinned bounce buffer");
-            dst = bounce;
-        }
-        if (!rc) e = cudaMemcpyAsync(dst, drss, sizeof(float) * N, cudaMemcpyDeviceToHost, st);
-        if (!rc && e != cudaSuccess) rc = cuda_err(ctx, e, "server_submit: download");
-    }
-    if (q->h_kspace && dk) cudaFreeAsync(dk, st);
-    if (coils) cudaFreeAsync(coils, st);
-    if (drss) cudaFreeAsync(drss, st);
     okscuda_server::Req r;
-    r.done = take_event(s);
-    cudaEventRecord(r.done, st);
-    ctx->stream = saved;
-    if (rc) {
-        cudaEventSynchronize(r.done);
-        if (bounce) s->pinned_pool.push_back({bounce, bounce_cap});
-        s->ev_pool.push_back(r.done);
-        return rc;
-    }
-    r.bounce = bounce;
-    r.bounce_bytes = sizeof(float) * N;
-    r.user_out = q->h_rss;
+    r.q = *q;
     r.bytes = need;
+    const uint64_t rid = s->next_id++;
+    auto& rr = s->reqs.emplace(rid, r).first->second;
     s->reserved += need;
-    *id = s->next_id++;
-    s->reqs[*id] = r;
+    if (s->mode == 1) {
+        const int rc = run_chain(s, rr);
+        if (rc) {   // nothing of it stays in flight: report the error now
+            cudaEventSynchronize(rr.done);
+            if (rr.bounce) s->pinned_pool.push_back({rr.bounce, rr.bounce_cap});
+            s->ev_pool.push_back(rr.done);
+            s->reserved -= need;
+            s->reqs.erase(rid);
+            return rc;
+        }
+    } else {
+        s->pending.push_back(rid);
+        s->cv.notify_all();
+    }
+    *id = rid;
     return OKS_OK;
 }
 
@@ -237,8 +446,8 @@ int okscuda_server_poll(okscuda_server* s, uint64_t id, int* done) {
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return set_err(s->ctx, OKS_EINVAL, "unknown request %llu", (unsigned long long)id);
     reap(s);
-    *done = it->second.finished ? 1 : 0;
-    if (it->second.finished) {
+    *done = it->second.state == 2 ? 1 : 0;
+    if (*done) {
         const int st = it->second.status;
         s->ev_pool.push_back(it->second.done);
         s->reqs.erase(it);
@@ -255,9 +464,11 @@ int okscuda_server_wait(okscuda_server* s, uint64_t id, int timeout_ms) {
         const int rc = okscuda_server_poll(s, id, &done);
         if (rc != OKS_OK || done) return rc;
         const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0);
-        if (timeout_ms >= 0 && ms.count() >= timeout_ms)
+        if (timeout_ms >= 0 && ms.count() >= timeout_ms) {
+            std::lock_guard<std::mutex> lock(s->mu);
             return set_err(s->ctx, OKS_ETIMEDOUT, "request %llu not done after %d ms", (unsigned long long)id,
                            timeout_ms);
+        }
         std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
 }
@@ -268,7 +479,7 @@ int okscuda_server_stats(okscuda_server* s, long long* inflight, long long* comp
     cudaSetDevice(s->ctx->device);
     reap(s);
     long long n = 0;
-    for (auto& kv : s->reqs) n += kv.second.finished ? 0 : 1;
+    for (auto& kv : s->reqs) n += kv.second.state != 2 ? 1 : 0;
     if (inflight) *inflight = n;
     if (completed) *completed = s->completed;
     if (reserved_bytes) *reserved_bytes = s->reserved;

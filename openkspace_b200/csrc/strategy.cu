@@ -125,7 +125,7 @@ int okscuda_ifft1_kz(okscuda_ctx* ctx, okscuda_c64* d_data, int nc, int nz, int 
     int rc = get_plan(ctx, nz, &pz);
     if (rc) return rc;
     oks::ColXformArgs ca{};
-    ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile; ca.lanes = ctx->xform_lanes;
+    ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile; ca.lanes = ctx->xform_lanes; ca.lanes_pf = ctx->xform_lanes_pf;
     ca.data = reinterpret_cast<float2*>(d_data);
     ca.nprob = nc;
     ca.ny = nz;
@@ -150,7 +150,7 @@ int okscuda_ifft2(okscuda_ctx* ctx, okscuda_c64* d_data, long long batch, int ny
         int rc = get_plan(ctx, ny, &py);
         if (rc) return rc;
         oks::ColXformArgs ca{};
-        ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile; ca.lanes = ctx->xform_lanes;
+        ca.reg = ctx->xform_reg; ca.tile = ctx->xform_tile; ca.lanes = ctx->xform_lanes; ca.lanes_pf = ctx->xform_lanes_pf;
         ca.data = d; ca.nprob = batch; ca.ny = ny; ca.nx = nx; ca.prob_stride = (long long)ny * nx;
         ca.sign = +1; ca.centred = 1; ca.scale = 1.0f / (float)ny;
         ProfScope ps(ctx, "k_col_xform");

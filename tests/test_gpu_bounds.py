@@ -43,11 +43,14 @@ with Context(0) as ctx:
                 out["errors"].append(f"fft2 {n} inv={inv}")
         for opt, vals in (("xform_tile", (2, 4, 8)), ("xform_lanes", (1, 2, 3, 4))):
             for v in vals:
-                ctx.set_option(opt, v)
-                got = ctx.centred_fft2(x, True)
-                ctx.set_option(opt, 0)
-                if rel(got, o64.centred_ifft2(x)) > 1e-5:
-                    out["errors"].append(f"fft2 {n} {opt}={v}")
+                for pf in ((0, 1) if opt == "xform_lanes" else (0,)):
+                    ctx.set_option(opt, v)
+                    ctx.set_option("xform_lanes_pf", pf)
+                    got = ctx.centred_fft2(x, True)
+                    ctx.set_option(opt, 0)
+                    ctx.set_option("xform_lanes_pf", 1)
+                    if rel(got, o64.centred_ifft2(x)) > 1e-5:
+                        out["errors"].append(f"fft2 {n} {opt}={v} pf={pf}")
     for n in (128, 192, 256, 320, 368, 384, 512):       # column engine, both plans
         rows = rng.random(n) < 0.35
         rows[n // 2 - 2:n // 2 + 2] = True

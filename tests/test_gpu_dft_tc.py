@@ -108,3 +108,23 @@ def test_fista_row_engine_tc_ragged_and_per_slice_masks(ctx, rng):
     assert ctx.tc_status() == 0
     want = o64.csrss_from_kspace(k, m, 15, 0.02)
     assert o64.nrmse(rss, want) < 1e-4
+
+
+def test_bounded_wait_times_out_and_returns(ctx, rng):
+    """The tensor-core kernel's bounded waits: with the gate test on, every
+    CTA first waits on a device word that nothing sets, for at most ~1 ms of
+    clock cycles; the call returns, okscuda_tc_status reports the time-out
+    (code 7) and clears it, and the next launch (gate off) is correct -- the
+    context stays usable."""
+    x = crandn(rng, (256, 128))
+    ctx.set_option("tc_gate_test", 2_000_000)
+    try:
+        ctx.dft_rows(x, inverse=False, centred=True, engine=1)
+        ctx.synchronize()
+        assert ctx.tc_status() == 7
+        assert ctx.tc_status() == 0          # read and cleared
+    finally:
+        ctx.set_option("tc_gate_test", 0)
+    got = ctx.dft_rows(x, inverse=False, centred=True, engine=1)
+    assert ctx.tc_status() == 0
+    assert rel_l2(got, ref_rows(x, False, True)) < TOL_TC

@@ -81,3 +81,46 @@ def test_cartesian3d_subvolume_32_coils(ctx):
                                           iters=80, lam=0.01, workers=WORKERS)
     assert got.shape == want.shape == (8, 256, 256)
     assert o64.nrmse(got, want) < TOL_CS
+
+
+def test_cartesian3d_slices_through_the_server(ctx):
+    """Configuration 4's path through the request server: the kz-decoupled
+    32-coil 256 x 256 x 8 volume's slices submitted in place beside serving
+    requests, under an HBM budget that refuses some submissions; each slice
+    equals the CsRss 3-D path's slice, and each serving request its result
+    alone."""
+    from openkspace_b200 import Context
+    k, m = synth.volume_3d(nc=32, nz=8, ny=256, nx=256)
+    want = CsRss(iters=80, lambda_=0.01).reconstruct(ctx, cartesian3d_acquisitions(k, m)).data
+    reqs = synth.uneven_requests(n=4, workload=3, iter_range=(15, 25))
+    masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in reqs]
+    alone = [ctx.cs_slice(r.kspace, mk, r.iters, r.lam) for r, mk in zip(reqs, masks)]
+    with Context(0) as sctx:
+        d = sctx.to_device(k)
+        nc, nz, ny, nx = k.shape
+        sctx.check(sctx.lib.okscuda_ifft1_kz(sctx.handle, d.ptr, nc, nz, ny, nx))
+        m2 = np.repeat(m[:, None], nx, 1)
+        refused = 0
+        with Server(sctx, max_inflight=6, hbm_budget_bytes=400 << 20) as srv:
+            ids, sids = [], []
+            todo = [("v", z) for z in range(nz)] + [("r", i) for i in range(len(reqs))]
+            todo = [todo[i] for i in (0, 8, 1, 9, 2, 10, 3, 11, 4, 5, 6, 7)]
+            for kind, i in todo:
+                while True:
+                    try:
+                        if kind == "v":
+                            ids.append((i, srv.submit(None, m2, 80, 0.01, device_slice=(d, i))))
+                        else:
+                            sids.append((i, srv.submit(reqs[i].kspace, masks[i], reqs[i].iters, reqs[i].lam)))
+                        break
+                    except OksError as e:
+                        assert e.code == _lib.OKS_EAGAIN
+                        refused += 1
+                        time.sleep(0.001)
+            for _, (rid, _) in ids + sids:
+                srv.wait(rid, 120000)
+    assert refused > 0                                   # the budget did push back
+    for z, (_, out) in ids:
+        assert o64.nrmse(out, want[z]) < 1e-6, z
+    for i, (_, out) in sids:
+        assert o64.nrmse(out, alone[i]) < 1e-6, i

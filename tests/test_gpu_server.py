@@ -15,12 +15,15 @@ pytestmark = pytest.mark.gpu
 TOL_CS = 1e-4
 
 
-def test_mix_equals_alone(ctx):
+@pytest.mark.parametrize("mode", [0, 1])
+def test_mix_equals_alone(ctx, mode):
+    """Mode 0 merges the queued requests into batched passes, mode 1 runs one
+    chain per request: every result equals the request solved alone."""
     reqs = synth.uneven_requests(n=12, sizes=((256, 256), (320, 320), (368, 64), (64, 48)), coil_range=(2, 6),
                                  iter_range=(5, 25))
     masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in reqs]
     alone = [ctx.cs_slice(r.kspace, m, r.iters, r.lam) for r, m in zip(reqs, masks)]
-    with Server(ctx, max_inflight=8, n_streams=4) as srv:
+    with Server(ctx, max_inflight=8, n_streams=4 if mode else 2, mode=mode) as srv:
         pending = list(range(len(reqs)))
         ids = {}
         while pending:                       # submit everything, resubmitting refused requests
@@ -71,3 +74,29 @@ def test_device_resident_request(ctx, rng):
         srv.wait(rid, 60000)
     assert o64.nrmse(out, ctx.cs_slice(s.kspace, s.mask2d, 20, 0.01)) < 1e-6
     assert np.array_equal(d.to_host(), s.kspace)   # input left untouched
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_volume_slices_in_place_and_2d_masks(ctx, mode):
+    """Slices of a device-resident [nc, nz, ny, nx] volume submitted in place
+    (coil planes nz * ny * nx apart), a 2-D (partial-row) mask request in the
+    same batch, and a pageable output: each equals the slice solved alone."""
+    rng = np.random.default_rng(3)
+    nc, nz, ny, nx = 3, 4, 64, 48
+    rows = rng.random(ny) < 0.4
+    rows[ny // 2 - 3:ny // 2 + 3] = True
+    m = np.repeat(rows[:, None], nx, 1)
+    vol = np.where(m[None, None], crandn(rng, (nc, nz, ny, nx)), 0).astype(np.complex64)
+    d = ctx.to_device(vol)
+    m2 = m.copy()
+    m2[:, :8] = False                                   # rows partial in kx: the 2-D engine
+    k2 = np.where(m2[None], crandn(rng, (2, ny, nx)), 0).astype(np.complex64)
+    with Server(ctx, mode=mode) as srv:
+        ids = [srv.submit(None, m, 12, 0.01, device_slice=(d, z)) for z in range(nz)]
+        i2 = srv.submit(k2, m2, 9, 0.02)
+        for rid, _ in ids + [i2]:
+            srv.wait(rid, 60000)
+    for z, (_, out) in enumerate(ids):
+        assert o64.nrmse(out, ctx.cs_slice(np.ascontiguousarray(vol[:, z]), m, 12, 0.01)) < 1e-6
+    assert o64.nrmse(i2[1], ctx.cs_slice(k2, m2, 9, 0.02)) < 1e-6
+    assert np.array_equal(d.to_host(), vol)             # the volume is left untouched

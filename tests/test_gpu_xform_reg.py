@@ -91,6 +91,27 @@ def test_column_lanes_forms(ctx, rng, n, lanes):
     assert rel_l2(got, want) < TOL
 
 
+@pytest.mark.parametrize("pf", [0, 1])
+@pytest.mark.parametrize("lanes", [1, 2, 3, 4])
+@pytest.mark.parametrize("n", [n for n in LENGTHS if n != 368])
+def test_column_lanes_pipelined_and_direct(ctx, rng, n, lanes, pf):
+    """The lanes form, software-pipelined (next tile staged in shared memory
+    with cp.async, the default) and direct: several tiles per CTA, a ragged
+    last tile, both directions, and an odd column count (which always takes
+    the direct form)."""
+    for ncols, inverse in ((38, True), (130, False), (7, True)):
+        x = crandn(rng, (3, n, ncols))
+        want = o64.centred_ifft2(x) if inverse else o64.centred_fft2(x)
+        ctx.set_option("xform_lanes", lanes)
+        ctx.set_option("xform_lanes_pf", pf)
+        try:
+            got = ctx.centred_fft2(x, inverse)
+        finally:
+            ctx.set_option("xform_lanes", 0)
+            ctx.set_option("xform_lanes_pf", 1)
+        assert rel_l2(got, want) < TOL
+
+
 @pytest.mark.parametrize("rows,n", [(1, 640), (301, 368), (7, 128), (1001, 320), (64, 512)])
 @pytest.mark.parametrize("inverse,centred", [(0, 1), (1, 1), (0, 0), (1, 0)])
 def test_rows_odd_counts_and_uncentred(ctx, rng, rows, n, inverse, centred):
