@@ -84,7 +84,9 @@ const char* okscuda_version(void);
  *   "prefetch2d"    2-D register passes, the next unit's loads issued
  *                   (cp.async) before the current unit's transforms: bit 0
  *                   column pass with separable masks (default 1), bit 1 row
- *                   pass
+ *                   pass; bit 2 row pass with the next row pair of S, Z~ and
+ *                   X~ staged in shared memory by cp.async.bulk (mbarrier
+ *                   completion, bounded waits)
  *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
  *                   least 12 warps resident per SM, 2 = at least 18,
  *                   0 = registers as needed
@@ -248,28 +250,47 @@ int okscuda_write_nifti(const float* h_vol, int nz, int ny, int nx, const char* 
  * blocks.  Host only (no context). */
 int okscuda_write_png(const uint8_t* h_gray, int width, int height, const char* path);
 
+/* -------------------------------------------------- SENSE unfold (sense) */
+/* sense.rs:64-192 sense_unfold_1d and sense.rs:194-252 sense_gfactor_1d on
+ * the device: per reduced voxel (y0, x), y0 < ny / r, the r x r system
+ * (C^H C + ridge I) rho = r C^H a with C[c][k] = maps[c][y0 + k ny/r][x] and
+ * a[c] = aliased[c][y0][x], solved through the Cholesky factor and its
+ * triangular inverse of prewhiten.rs:148-210, in f32 in the reference's
+ * order (no fused multiply-adds).  d_out[ny, nx] (complex, may be NULL) gets
+ * rho at rows y0 + k ny/r, d_gfactor[ny, nx] (may be NULL) the g-factor;
+ * voxels whose factorisation fails stay zero.  OKS_EINVAL for r < 1
+ * (SenseError::BadAcceleration), OKS_ESHAPE when r does not divide ny
+ * (IndivisibleNy), OKS_ENOTSUP for r > 8. */
+int okscuda_sense_unfold(okscuda_ctx* ctx, const okscuda_c64* d_aliased, const okscuda_c64* d_maps, int nc, int ny,
+                         int nx, int r, float ridge, okscuda_c64* d_out, float* d_gfactor);
+
 /* ------------------------------------------------------- request server */
 /* No counterpart in the reference (which reconstructs one file at a time).
  * A request is one slice (strategy.rs:850-880).  Admission is by an HBM
  * budget and an in-flight limit: okscuda_server_submit returns OKS_EAGAIN
- * when the request does not fit now, and an admitted request is queued.
- * Mode 0 (default, continuous batching): a dispatcher thread takes every
+ * when the request does not fit now.
+ * Mode 0 (default): each admitted request runs its own upload -> FISTA ->
+ * RSS -> download chain on one stream of a pool, so requests that arrive
+ * while others run overlap with them on the GPU.
+ * Mode 1 (continuous batching): the upload of an admitted request starts at
+ * submission on the server's upload stream; a dispatcher thread takes every
  * queued request whenever one of the server's batch slots is free and runs
- * them as one batched pass (okscuda_cs_batch: uploads, readout transforms,
- * one column-engine launch per column length over the (coil, column pair)
- * units of all of them, RSS, downloads) on that slot's streams; requests that
+ * them as one batched pass (okscuda_cs_batch: readout transforms, one
+ * column-engine launch per column length over the (coil, column pair) units
+ * of all of them, RSS, downloads) on that slot's streams; requests that
  * arrive while batches run join the next one, and the slots' batches overlap
- * on the GPU.  Mode 1: each request runs its own upload -> FISTA -> RSS ->
- * download chain on one stream of a pool.  Results are the same in both modes
- * and the same as the request solved alone.  Host buffers of a request must
- * stay valid until it completes (pinned memory keeps the copies
- * asynchronous).  submit / poll / wait / stats are thread-safe. */
+ * on the GPU.  Mode 1 uses the server's context from its own thread: other
+ * work belongs on another context while such a server exists.
+ * Results are the same in both modes and the same as the request solved
+ * alone.  Host buffers of a request must stay valid until it completes
+ * (pinned memory keeps the copies asynchronous).  submit / poll / wait /
+ * stats are thread-safe. */
 typedef struct okscuda_server okscuda_server;
 typedef struct {
     int max_inflight;              /* 0: 32 (queued + running)                 */
     size_t hbm_budget_bytes;       /* 0: half the free device memory           */
-    int n_streams;                 /* 0: 8 (mode 1), 2 batch slots (mode 0)    */
-    int mode;                      /* 0: continuous batching, 1: stream per request */
+    int n_streams;                 /* 0: 12 streams (mode 0), 6 batch slots (mode 1) */
+    int mode;                      /* 0: stream per request, 1: continuous batching */
 } okscuda_server_cfg;
 typedef struct {
     const okscuda_c64* h_kspace;   /* [nc, ny, nx] host k-space, or NULL ...   */

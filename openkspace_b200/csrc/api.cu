@@ -111,7 +111,8 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "occ2d: 0 (1 CTA), 1 (12 warps), 2 (18 warps)");
         ctx->occ2d = (int)value;
     } else if (!std::strcmp(name, "prefetch2d")) {
-        if (value < 0 || value > 3) return set_err(ctx, OKS_EINVAL, "prefetch2d: bit 0 column pass, bit 1 row pass");
+        if (value < 0 || value > 7)
+            return set_err(ctx, OKS_EINVAL, "prefetch2d: bit 0 column pass, bit 1 row pass, bit 2 bulk-copy row pass");
         ctx->prefetch2d = (int)value;
     } else if (!std::strcmp(name, "graph2d")) {
         ctx->graph2d = value != 0;
@@ -414,6 +415,10 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     const bool col_reg = tp.col_engine != 1 && oks::fista2d_reg_supported(ny);
     const bool row_reg = tp.col_engine != 1 && oks::fista2d_reg_supported(nx);
     cudaError_t e = cudaSuccess;
+    if (row_reg && (tp.prefetch2d & 4) && (rc = tc_err_flag(ctx))) {   // the bulk-copy row pass's error word
+        stage_release(ctx, slot);
+        return rc;
+    }
     if ((col_reg || row_reg) && (e = oks::reg_tables_init(&ctx->reg_tables)) != cudaSuccess) {
         stage_release(ctx, slot);
         return cuda_err(ctx, e, "register tables");
@@ -469,6 +474,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             a.persist = tp.persist2d;
             a.occ = tp.occ2d;
             a.prefetch = tp.prefetch2d;
+            a.err = ctx->tc_err;
             auto col = [&](int mode) {
                 if (col_reg) {
                     ProfScope ps(ctx, "k2d_col_reg", st);

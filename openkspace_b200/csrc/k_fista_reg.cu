@@ -429,6 +429,182 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
     if (pf) cp_async_wait_all();
 }
 
+// Row pass with bulk-copy staging (a.prefetch bit 2): one thread of each
+// group copies the group's next row pair of S, Z~ and X~ (three contiguous
+// 2 nx complex64 spans) into a shared-memory staging buffer with
+// cp.async.bulk (no multicast), completing on an mbarrier, while the group
+// transforms the current row pair; the group reads the staged values into
+// registers, releases the buffer and issues the next copies.  The loads
+// then cost no issue slots and no registers while they are in flight.
+// Every mbarrier wait is bounded (about one second of clock cycles): on
+// time-out the group records code 8 in *a.err, waits (bounded again) for
+// the copy in flight and leaves the loop; the decision is uniform per group.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void bar_init1(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool bar_wait_bounded(uint32_t bar, uint32_t parity, long long cycles) {
+    if (bar_try(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!bar_try(bar, parity))
+        if (clock64() - t0 > cycles) return false;
+    return true;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+// true when pred holds in any thread of the group (a warp, or the whole CTA)
+template <class P>
+__device__ __forceinline__ bool group_any(bool pred) {
+    if constexpr (P::T == 32) return __any_sync(0xffffffffu, pred);
+    else return __syncthreads_or(pred) != 0;
+}
+constexpr long long kRowWaitCycles = 2000000000ll;   // about one second at 1.9 GHz
+
+template <class P, int MINB>
+__global__ void __launch_bounds__(P::T * (P::T == 32 ? 4 : 1), MINB)
+k2d_row_tma(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, const float2* __restrict__ groots,
+            int roots_total) {
+    constexpr int E = P::E, TA = P::TA, T = P::T, N = P::N;
+    constexpr int G = (T == 32) ? 4 : 1;
+    constexpr int NTW = Tw<P>::total();
+    static_assert(G == 1 || T == 32, "groups are warps or the whole CTA");
+    extern __shared__ __align__(16) float2 sm[];
+    const int g = threadIdx.x / T, t = threadIdx.x % T;
+    float2* STG = sm + (size_t)g * 6 * N;             // [S row pair | Z~ row pair | X~ row pair]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + (size_t)G * 6 * N);
+    float2* TW = sm + (size_t)G * 6 * N + G;
+    float2* RT = TW + NTW;
+    float2* A = RT + roots_total + g * 2 * P::SMEM_X;
+    float2* B = A + P::SMEM_X;
+    for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    const uint32_t bar = smem_addr(&bars[g]);
+    if (t == 0) {
+        bar_init1(bar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int nrp = a.ny / 2;
+    const bool live = t < TA;
+    const float alpha = mode ? __ldg(a.alpha + it) : 0.f;
+    const float lam = a.lambda;
+    const bool b0 = (t & 1) != 0, b1 = (t & 2) != 0;
+    const long long total = a.nprob * nrp, stride = (long long)gridDim.x * G;
+    constexpr uint32_t kPair = 2u * N * sizeof(float2);   // bytes of one row pair (a multiple of 16)
+    auto issue = [&](long long u) {                         // thread 0 of the group
+        const long long p = u / nrp;
+        const int r0 = 2 * (int)(u - p * nrp);
+        const long long base = p * a.st_stride + (long long)r0 * N;
+        bar_expect_tx(bar, mode ? 3 * kPair : kPair);
+        bulk_g2s(STG, a.S + base, kPair, bar);
+        if (mode) {
+            bulk_g2s(STG + 2 * N, a.Z + base, kPair, bar);
+            bulk_g2s(STG + 4 * N, a.X + base, kPair, bar);
+        }
+    };
+    uint32_t phase = 0;
+    long long unit = (long long)blockIdx.x * G + g;
+    if (t == 0 && unit < total) issue(unit);
+    for (; unit < total; unit += stride) {
+        const bool ok = bar_wait_bounded(bar, phase & 1u, kRowWaitCycles);
+        if (group_any<P>(!ok)) {
+            if (t == 0) {
+                atomicExch(a.err, 8);
+                bar_wait_bounded(bar, phase & 1u, kRowWaitCycles);   // the copy in flight lands first
+            }
+            break;
+        }
+        ++phase;
+        const long long p = unit / nrp;
+        const int r0 = 2 * (int)(unit - p * nrp);
+        const long long mi = (p + a.mask_offset) % a.mask_mod;
+        const uint32_t* cb = a.colbits + mi * a.col_wstride;
+        const long long base = p * a.st_stride + (long long)r0 * N;
+        float2* __restrict__ S = a.S + base;
+        float2* __restrict__ X = a.X + base;
+        float2* __restrict__ Z = a.Z + base;
+        float2 w[E], zo[E], xo[E];
+        uint32_t cm = 0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int q = t + TA * e;
+            const int x = q >> 1;
+            const int off = (q & 1) * N + x;
+            const bool on = live && ((__ldg(cb + (x >> 5)) >> (x & 31)) & 1u) && OKS_IN(off, 2 * N, OKS_B_STAGE);
+            if (on) cm |= 1u << e;
+            w[e] = on ? STG[off] : make_float2(0.f, 0.f);
+            zo[e] = (mode && live) ? STG[2 * N + off] : make_float2(0.f, 0.f);
+            xo[e] = (mode && live) ? STG[4 * N + off] : make_float2(0.f, 0.f);
+        }
+        group_sync<P>();                     // staging read by the group; the last unit's final stage has read A/B
+        if (t == 0 && unit + stride < total) issue(unit + stride);
+        inverse<P>(w, A, B, TW, RT, t);
+        if (mode == 0) {
+            if (live) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int q = t + TA * e;
+                    const long long off = (long long)(q & 1) * N + (q >> 1);
+                    X[off] = w[e];
+                    Z[off] = w[e];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int q = t + TA * e;
+                const long long off = (long long)(q & 1) * N + (q >> 1);
+                const float2 v = zo[e] - w[e];
+                const float2 v1 = shfl_xor2(v, 1);
+                const float2 u = b0 ? (v1 - v) : (v + v1);
+                const float2 u2 = shfl_xor2(u, 2);
+                float2 c = (b1 ? (u2 - u) : (u + u2)) * 0.5f;
+                if (!(b0 && b1)) c = shrink_c(c, lam);   // the demodulated image's LL band: untouched
+                const float2 c1 = shfl_xor2(c, 1);
+                const float2 s2v = b0 ? (c1 - c) : (c + c1);
+                const float2 s2 = shfl_xor2(s2v, 2);
+                const float2 xn = (b1 ? (s2 - s2v) : (s2v + s2)) * 0.5f;
+                const float2 zn = xn + (xn - xo[e]) * alpha;
+                if (live) {
+                    X[off] = xn;
+                    Z[off] = zn;
+                }
+                w[e] = zn;
+            }
+        }
+        group_sync<P>();
+        forward<P>(w, A, B, TW, RT, t);
+        if (live) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                if (!((cm >> e) & 1u)) continue;   // only sampled columns of S are read back
+                const int q = t + TA * e;
+                S[(long long)(q & 1) * N + (q >> 1)] = w[e];
+            }
+        }
+    }
+}
+
 // ------------------------------------------- SENSE mode, register form
 // One image per slice: g = sum_c S_c^* F_y^H m (F_y (S_c z~) - y'_c) per
 // column pair (ky-only mask; maps are diagonal, so they commute with the
@@ -572,6 +748,29 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
     if (pf && MINB > 1 && (base_smem + pf_smem + 1024) * MINB > 220u * 1024u) pf = 0;
     b.prefetch = pf ? (row ? 2 : 1) : 0;   // the kernels test their own bit
     const size_t smem = base_smem + (pf ? pf_smem : 0);
+    if (row && (a.prefetch & 4) && a.err) {
+        // bulk-copy staging: [S | Z~ | X~] row pairs per group, one mbarrier
+        // per group (an 8-byte slot), then the tables and exchange buffers
+        const size_t tsmem = sizeof(float2) * ((size_t)G * 6 * P::N + G + NTW + nrt + (size_t)G * 2 * P::SMEM_X);
+        const void* fn = reinterpret_cast<const void*>(k2d_row_tma<P, MINB>);
+        if ((e = set_smem_attr(fn, tsmem)) != cudaSuccess) return e;
+        long long grid = (units + G - 1) / G;
+        if (a.persist) {
+            static int per_sm = 0, nsm = 0;
+            static std::mutex mu;
+            std::lock_guard<std::mutex> lk(mu);
+            if (!per_sm) {
+                int dev = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2d_row_tma<P, MINB>, P::T * G, tsmem);
+                if (per_sm < 1) per_sm = 1;
+            }
+            if (grid > (long long)per_sm * nsm) grid = (long long)per_sm * nsm;
+        }
+        k2d_row_tma<P, MINB><<<(unsigned)grid, P::T * G, tsmem, st>>>(a, mode, it, tw, rt, nrt);
+        return cudaGetLastError();
+    }
     if (row) e = set_smem_attr(reinterpret_cast<const void*>(k2d_row_reg<P, MINB>), smem);
     else e = set_smem_attr(reinterpret_cast<const void*>(k2d_col_reg<P, MINB>), smem);
     if (e != cudaSuccess) return e;

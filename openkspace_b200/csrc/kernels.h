@@ -185,7 +185,9 @@ struct Fista2dArgs {
     int persist;              // register passes: grid of resident CTAs, units grid-strided
     int occ;                  // register passes: 0 registers as needed, 1 at least 12 warps per SM, 2 at least 18
     int prefetch;             // register passes: next unit's loads in flight (cp.async); bit 0 column
-                              // pass (separable masks), bit 1 row pass
+                              // pass (separable masks), bit 1 row pass; bit 2 row pass with
+                              // bulk-copy (cp.async.bulk) staging of S, Z~, X~
+    int* err;                 // bounded-wait error word (bulk-copy row pass), may be null
 };
 cudaError_t launch_fista2d_col(const Fista2dArgs& a, const DevPlan& py, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_row(const Fista2dArgs& a, const DevPlan& px, int mode, int it, cudaStream_t st);

@@ -264,6 +264,18 @@ class Context:
                                              x.ptr, ctypes.byref(L)))
         return mag.to_host(), x.to_host(), maps.to_host(), L.value
 
+    def sense_unfold(self, aliased, maps, r: int, ridge: float, gfactor: bool = False):
+        """okscuda_sense_unfold (sense.rs:64-252): (unfolded [ny, nx] complex64,
+        g-factor [ny, nx] float32 or None) on the host."""
+        a, _ = self._dev(aliased)
+        m, _ = self._dev(maps)
+        nc, ny, nx = a.shape
+        out = self.empty((ny, nx))
+        g = self.empty((ny, nx), np.float32) if gfactor else None
+        self.check(self.lib.okscuda_sense_unfold(self.handle, a.ptr, m.ptr, nc, ny, nx, int(r), float(ridge), out.ptr,
+                                                 g.ptr if g is not None else None))
+        return out.to_host(), (g.to_host() if g is not None else None)
+
     def set_option(self, name: str, value: int):
         self.check(self.lib.okscuda_set_option(self.handle, name.encode(), int(value)))
 

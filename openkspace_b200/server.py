@@ -24,9 +24,9 @@ class _Req(ctypes.Structure):
 
 
 class Server:
-    """okscuda_server_*: ``mode`` 0 (default) continuous batching (queued
-    requests run together as batched passes on ``n_streams`` batch slots,
-    0 = 2), 1 one stream per request (``n_streams`` streams, 0 = 8)."""
+    """okscuda_server_*: ``mode`` 0 (default) one stream per request
+    (``n_streams`` streams, 0 = 12); 1 continuous batching (queued requests
+    run together as batched passes on ``n_streams`` batch slots, 0 = 6)."""
 
     def __init__(self, ctx, max_inflight: int = 32, hbm_budget_bytes: int = 0, n_streams: int = 0, mode: int = 0):
         self.ctx = ctx

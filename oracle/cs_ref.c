@@ -527,3 +527,115 @@ int csref_ifft1_axis(float *data, long n_outer, int n, long n_inner) {
     plan_free(pl);
     return 0;
 }
+
+/* sense.rs:64-252 sense_unfold_1d / sense_gfactor_1d (f32, the reference's
+ * order; Cholesky and inverse as prewhiten.rs:148-210).  aliased, maps:
+ * [nc, ny, nx]; out [ny, nx] (may be NULL), g [ny, nx] (may be NULL); voxels
+ * whose factorisation fails stay zero.  Returns 1 for R < 1 or ny % R != 0. */
+int csref_sense_unfold(const float *aliased, const float *maps, int nc, int ny, int nx, int r, float ridge,
+                       float *out, float *g) {
+    if (r < 1 || ny % r) return 1;
+    const cf *al = (const cf *)aliased, *mp = (const cf *)maps;
+    cf *o = (cf *)out;
+    const long plane = (long)ny * nx;
+    if (o) memset(o, 0, sizeof(cf) * (size_t)plane);
+    if (g) memset(g, 0, sizeof(float) * (size_t)plane);
+    const int nyr = ny / r;
+    if (nc == 0 || nx == 0 || nyr == 0) return 0;
+    cf *C = (cf *)malloc(sizeof(cf) * (size_t)nc * r);
+    cf *chc = (cf *)malloc(sizeof(cf) * (size_t)r * r);
+    cf *l = (cf *)malloc(sizeof(cf) * (size_t)r * r);
+    cf *inv = (cf *)malloc(sizeof(cf) * (size_t)r * r);
+    cf *rhs = (cf *)malloc(sizeof(cf) * (size_t)r);
+    cf *tmp = (cf *)malloc(sizeof(cf) * (size_t)r);
+    for (int x = 0; x < nx; ++x)
+        for (int y0 = 0; y0 < nyr; ++y0) {
+            for (int c = 0; c < nc; ++c)
+                for (int k = 0; k < r; ++k) C[c * r + k] = mp[c * plane + (long)(y0 + k * nyr) * nx + x];
+            for (int a = 0; a < r; ++a)
+                for (int b = 0; b < r; ++b) {
+                    cf acc = {0.f, 0.f};
+                    for (int c = 0; c < nc; ++c) {
+                        cf ca = C[c * r + a], cc = {ca.re, -ca.im};
+                        acc = cadd(acc, cmul(cc, C[c * r + b]));
+                    }
+                    if (a == b) { cf rd = {ridge, 0.f}; acc = cadd(acc, rd); }
+                    chc[a * r + b] = acc;
+                }
+            for (int a = 0; a < r; ++a) {
+                cf acc = {0.f, 0.f};
+                for (int c = 0; c < nc; ++c) {
+                    cf ca = C[c * r + a], cc = {ca.re, -ca.im};
+                    acc = cadd(acc, cmul(cc, al[c * plane + (long)y0 * nx + x]));
+                }
+                cf rr = {(float)r, 0.f};
+                rhs[a] = cmul(acc, rr);
+            }
+            int bad = 0;
+            memset(l, 0, sizeof(cf) * (size_t)r * r);
+            for (int i = 0; i < r && !bad; ++i) {
+                cf diag = chc[i * r + i];
+                for (int k = 0; k < i; ++k) {
+                    cf lk = l[i * r + k], ck = {lk.re, -lk.im};
+                    diag = csub(diag, cmul(lk, ck));
+                }
+                float d_re = diag.re;
+                if (!isfinite(d_re) || d_re <= 0.0f) { bad = 1; break; }
+                float lii = sqrtf(d_re);
+                l[i * r + i].re = lii; l[i * r + i].im = 0.f;
+                cf iv = {1.0f / lii, 0.f};
+                for (int j = i + 1; j < r; ++j) {
+                    cf s = chc[j * r + i];
+                    for (int k = 0; k < i; ++k) {
+                        cf lik = l[i * r + k], c2 = {lik.re, -lik.im};
+                        s = csub(s, cmul(l[j * r + k], c2));
+                    }
+                    l[j * r + i] = cmul(s, iv);
+                }
+            }
+            if (bad) continue;
+            memset(inv, 0, sizeof(cf) * (size_t)r * r);
+            for (int col = 0; col < r && !bad; ++col)
+                for (int i = 0; i < r; ++i) {
+                    cf s = {i == col ? 1.f : 0.f, 0.f};
+                    for (int j = 0; j < i; ++j) s = csub(s, cmul(l[i * r + j], inv[j * r + col]));
+                    cf d = l[i * r + i];
+                    if (fabsf(d.re) < 1.1920929e-7f && fabsf(d.im) < 1.1920929e-7f) { bad = 1; break; }
+                    float den = d.re * d.re + d.im * d.im;
+                    cf q = {(s.re * d.re + s.im * d.im) / den, (s.im * d.re - s.re * d.im) / den};
+                    inv[i * r + col] = q;
+                }
+            if (bad) continue;
+            for (int i = 0; i < r; ++i)
+                for (int j = i + 1; j < r; ++j) { inv[i * r + j].re = 0.f; inv[i * r + j].im = 0.f; }
+            if (o) {
+                for (int i = 0; i < r; ++i) {
+                    cf acc = {0.f, 0.f};
+                    for (int j = 0; j <= i; ++j) acc = cadd(acc, cmul(inv[i * r + j], rhs[j]));
+                    tmp[i] = acc;
+                }
+                for (int i = 0; i < r; ++i) {
+                    cf acc = {0.f, 0.f};
+                    for (int j = i; j < r; ++j) {
+                        cf v = inv[j * r + i], vc = {v.re, -v.im};
+                        acc = cadd(acc, cmul(vc, tmp[j]));
+                    }
+                    o[(long)(y0 + i * nyr) * nx + x] = acc;
+                }
+            }
+            if (g)
+                for (int k = 0; k < r; ++k) {
+                    float inv_diag = 0.f;
+                    for (int j = k; j < r; ++j) {
+                        cf v = inv[j * r + k];
+                        inv_diag += v.re * v.re + v.im * v.im;
+                    }
+                    float cd = chc[k * r + k].re;
+                    if (!(cd > 0.f)) cd = (cd != cd) ? 0.f : (cd > 0.f ? cd : 0.f);
+                    float p = inv_diag * cd;
+                    g[(long)(y0 + k * nyr) * nx + x] = sqrtf(p > 0.f ? p : 0.f);
+                }
+        }
+    free(C); free(chc); free(l); free(inv); free(rhs); free(tmp);
+    return 0;
+}

@@ -45,6 +45,8 @@ def lib():
         L.csref_prewhiten_apply.argtypes = [_f, _f, ctypes.c_long, ctypes.c_int, ctypes.c_int]
         L.csref_os_apply.argtypes = [_f, _f, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.csref_ifft1_axis.argtypes = [_f, ctypes.c_long, ctypes.c_int, ctypes.c_long]
+        L.csref_sense_unfold.argtypes = [_f, _f, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_float, _f, _f]
         _lib = L
     return _lib
 
@@ -158,3 +160,17 @@ def ifft1_axis(data, axis) -> np.ndarray:
     inner = int(np.prod(a.shape[axis + 1:]))
     lib().csref_ifft1_axis(_fp(a), outer, n, inner)
     return a
+
+
+def sense_unfold(aliased, maps, r, ridge, gfactor=False):
+    """sense.rs:64-252 in f32: (unfolded [ny, nx] complex64, g-factor [ny, nx]
+    float32 or None)."""
+    a, m = _c64(aliased), _c64(maps)
+    nc, ny, nx = a.shape
+    out = np.zeros((ny, nx), np.complex64)
+    g = np.zeros((ny, nx), np.float32) if gfactor else None
+    rc = lib().csref_sense_unfold(_fp(a), _fp(m), nc, ny, nx, int(r), float(ridge), _fp(out),
+                                  g.ctypes.data_as(_f) if g is not None else None)
+    if rc:
+        raise ValueError("SENSE: bad R")
+    return out, g

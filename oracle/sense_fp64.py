@@ -124,3 +124,35 @@ def sense_fista(kspace, maps, mask, iters, lam, L):
         z = x_new + float(alpha) * (x_new - x)
         x = x_new
     return x
+
+
+def sense_unfold_1d(aliased, maps, r: int, ridge: float, gfactor: bool = False):
+    """sense.rs:64-252 in FP64: rho = (C^H C + ridge I)^-1 C^H (R a) per
+    reduced voxel through the prewhiten.rs Cholesky and triangular inverse;
+    voxels whose factorisation fails stay zero.  Returns (unfolded [ny, nx],
+    g-factor [ny, nx] or None)."""
+    a = np.asarray(aliased, dtype=np.complex128)
+    m = np.asarray(maps, dtype=np.complex128)
+    nc, ny, nx = a.shape
+    if r < 1 or ny % r:
+        raise ValueError("SENSE: bad R")
+    nyr = ny // r
+    out = np.zeros((ny, nx), np.complex128)
+    g = np.zeros((ny, nx), np.float64) if gfactor else None
+    for x in range(nx):
+        for y0 in range(nyr):
+            C = m[:, y0 + nyr * np.arange(r), x]                 # [nc, r]
+            chc = C.conj().T @ C + ridge * np.eye(r)
+            rhs = (C.conj().T @ a[:, y0, x]) * r
+            low = o64.cholesky_lower(chc)
+            if low is None:
+                continue
+            inv = o64.invert_lower_triangular(low)
+            if inv is None:
+                continue
+            rho = inv.conj().T @ (inv @ rhs)
+            out[y0 + nyr * np.arange(r), x] = rho
+            if g is not None:
+                inv_diag = np.sum(np.abs(inv) ** 2, axis=0)
+                g[y0 + nyr * np.arange(r), x] = np.sqrt(np.maximum(inv_diag * np.maximum(chc.diagonal().real, 0), 0))
+    return out, g

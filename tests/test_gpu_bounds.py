@@ -64,7 +64,8 @@ with Context(0) as ctx:
             if o64.nrmse(got, want) > 1e-4:
                 out["errors"].append(f"column engine {n} variant {var}")
     forms = [dict(occ2d=1, prefetch2d=1), dict(occ2d=1, prefetch2d=0), dict(occ2d=1, prefetch2d=3),
-             dict(occ2d=2, prefetch2d=3), dict(occ2d=0, prefetch2d=0, persist2d=0)]
+             dict(occ2d=2, prefetch2d=3), dict(occ2d=0, prefetch2d=0, persist2d=0), dict(occ2d=1, prefetch2d=5),
+             dict(occ2d=0, prefetch2d=4, persist2d=0)]
     default = dict(occ2d=1, prefetch2d=1, persist2d=1)
     for ny, nx in ((368, 640), (256, 192), (384, 320), (128, 512)):   # 2-D engine, partial rows
         m = np.zeros((ny, nx), bool)

@@ -123,7 +123,10 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=0),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=3),
              dict(mask_bits=1, occ2d=2, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=1),
-             dict(mask_bits=1, occ2d=2, persist2d=1, fista2d_streams=1, fista2d_chunk=2, prefetch2d=3)]
+             dict(mask_bits=1, occ2d=2, persist2d=1, fista2d_streams=1, fista2d_chunk=2, prefetch2d=3),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=5),
+             dict(mask_bits=1, occ2d=1, persist2d=0, fista2d_streams=1, fista2d_chunk=3, prefetch2d=4),
+             dict(mask_bits=0, occ2d=2, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=5)]
     default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0, prefetch2d=1)
     results = []
     try:
@@ -137,6 +140,7 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
     for r in results:
         assert rel_l2(r, results[0]) < 1e-6
         assert rel_l2(r, want) < TOL_CS
+    assert ctx.tc_status() == 0                  # no bounded wait of the bulk-copy row pass ran out
     mr = ragged_row_mask(rng, ny, nx)
     kr = np.where(mr[None], crandn(rng, (2, ny, nx)), 0).astype(np.complex64)
     assert rel_l2(ctx.fista_cs(kr, mr, iters, 0.02), o64.fista_cs_single_coil(kr, mr, iters, 0.02)) < TOL_CS

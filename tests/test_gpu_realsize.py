@@ -83,28 +83,30 @@ def test_cartesian3d_subvolume_32_coils(ctx):
     assert o64.nrmse(got, want) < TOL_CS
 
 
-def test_cartesian3d_slices_through_the_server(ctx):
+@pytest.mark.parametrize("mode", [0, 1])
+def test_cartesian3d_slices_through_the_server(ctx, mode):
     """Configuration 4's path through the request server: the kz-decoupled
-    32-coil 256 x 256 x 8 volume's slices submitted in place beside serving
-    requests, under an HBM budget that refuses some submissions; each slice
-    equals the CsRss 3-D path's slice, and each serving request its result
-    alone."""
+    32-coil 256 x 256 x 8 volume's slices submitted in place, back to back,
+    under an HBM budget that holds 2.5 of them (so admission refuses some),
+    then serving requests beside them; each slice equals the CsRss 3-D
+    path's slice, and each serving request its result alone."""
     from openkspace_b200 import Context
     k, m = synth.volume_3d(nc=32, nz=8, ny=256, nx=256)
     want = CsRss(iters=80, lambda_=0.01).reconstruct(ctx, cartesian3d_acquisitions(k, m)).data
-    reqs = synth.uneven_requests(n=4, workload=3, iter_range=(15, 25))
+    reqs = synth.uneven_requests(n=4, workload=3, sizes=((256, 256), (320, 320)), coil_range=(8, 12),
+                                 iter_range=(15, 25))
     masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in reqs]
     alone = [ctx.cs_slice(r.kspace, mk, r.iters, r.lam) for r, mk in zip(reqs, masks)]
+    nc, nz, ny, nx = k.shape
+    slice_need = 4 * nc * ny * nx * 8 + ny * nx * 4          # work copy + RSS + worst-case 2-D scratch
+    refused = 0
     with Context(0) as sctx:
         d = sctx.to_device(k)
-        nc, nz, ny, nx = k.shape
         sctx.check(sctx.lib.okscuda_ifft1_kz(sctx.handle, d.ptr, nc, nz, ny, nx))
         m2 = np.repeat(m[:, None], nx, 1)
-        refused = 0
-        with Server(sctx, max_inflight=6, hbm_budget_bytes=400 << 20) as srv:
+        with Server(sctx, max_inflight=16, hbm_budget_bytes=int(2.5 * slice_need), mode=mode) as srv:
             ids, sids = [], []
             todo = [("v", z) for z in range(nz)] + [("r", i) for i in range(len(reqs))]
-            todo = [todo[i] for i in (0, 8, 1, 9, 2, 10, 3, 11, 4, 5, 6, 7)]
             for kind, i in todo:
                 while True:
                     try:
@@ -116,7 +118,7 @@ def test_cartesian3d_slices_through_the_server(ctx):
                     except OksError as e:
                         assert e.code == _lib.OKS_EAGAIN
                         refused += 1
-                        time.sleep(0.001)
+                        time.sleep(0.0005)
             for _, (rid, _) in ids + sids:
                 srv.wait(rid, 120000)
     assert refused > 0                                   # the budget did push back

@@ -17,13 +17,13 @@ TOL_CS = 1e-4
 
 @pytest.mark.parametrize("mode", [0, 1])
 def test_mix_equals_alone(ctx, mode):
-    """Mode 0 merges the queued requests into batched passes, mode 1 runs one
-    chain per request: every result equals the request solved alone."""
+    """Mode 0 runs one chain per request, mode 1 merges the queued requests
+    into batched passes: every result equals the request solved alone."""
     reqs = synth.uneven_requests(n=12, sizes=((256, 256), (320, 320), (368, 64), (64, 48)), coil_range=(2, 6),
                                  iter_range=(5, 25))
     masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in reqs]
     alone = [ctx.cs_slice(r.kspace, m, r.iters, r.lam) for r, m in zip(reqs, masks)]
-    with Server(ctx, max_inflight=8, n_streams=4 if mode else 2, mode=mode) as srv:
+    with Server(ctx, max_inflight=8, n_streams=4, mode=mode) as srv:
         pending = list(range(len(reqs)))
         ids = {}
         while pending:                       # submit everything, resubmitting refused requests

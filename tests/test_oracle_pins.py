@@ -333,3 +333,57 @@ def test_phasecorr_binning_rules():
     got = o64.phase_correct_apply(corr, line, 5, 3)          # slice 5 has no bin: the (65535, 3) one
     assert np.allclose(got[:, :4], line[:, :4] * corr[(65535, 3)]) and np.array_equal(got[:, 4:], line[:, 4:])
     assert np.array_equal(o64.phase_correct_apply(corr, line, 0, 7), line)
+
+
+# ----------------------------------------------------------------- sense.rs
+def _sense_r2_case():
+    """sense.rs:262-341: 4 Gaussian coils at the corners, a rectangle with a
+    dot, every other ky line kept (plain FFT along y)."""
+    nc, ny, nx, r = 4, 32, 24, 2
+    truth = np.zeros((ny, nx), np.float32)
+    truth[6:26, 4:20] = 1.0
+    truth[14:18, 10:14] = 0.3
+    maps = np.zeros((nc, ny, nx), np.complex64)
+    yy, xx = np.meshgrid(np.arange(ny, dtype=np.float32), np.arange(nx, dtype=np.float32), indexing="ij")
+    for c, (fy, fx) in enumerate([(0.25, 0.25), (0.25, 0.75), (0.75, 0.25), (0.75, 0.75)]):
+        mag = np.exp(-((yy - fy * ny) ** 2 + (xx - fx * nx) ** 2) / 200.0)
+        maps[c] = mag * np.exp(1j * 0.2 * c)
+    k = np.fft.fft(maps * truth, axis=1)
+    k[:, np.arange(ny) % r != 0, :] = 0
+    aliased = np.fft.ifft(k, axis=1).astype(np.complex64)
+    return truth, maps, aliased, r
+
+
+def test_sense_unfold_r2_phantom_both_oracles():
+    from oracle import sense_fp64 as sref
+    truth, maps, aliased, r = _sense_r2_case()
+    assert np.sqrt(np.sum(np.abs(aliased[:, 0] - aliased[:, 32 // r]) ** 2)) < 1e-3
+    for out in (sref.sense_unfold_1d(aliased, maps, r, 1e-5)[0], csref.sense_unfold(aliased, maps, r, 1e-5)[0]):
+        m = np.abs(out)
+        assert np.sqrt(np.sum((truth - m) ** 2) / np.sum(truth ** 2)) < 0.1
+
+
+def test_sense_r1_passthrough_and_unit_gfactor():
+    from oracle import sense_fp64 as sref
+    nc, ny, nx = 2, 8, 6                                 # sense.rs:353-393
+    maps = np.ones((nc, ny, nx), np.complex64)
+    y, x = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    aliased = np.stack([np.sin(y * 0.1 + x * 0.05 + c) for c in range(nc)]).astype(np.complex64)
+    for out in (sref.sense_unfold_1d(aliased, maps, 1, 0.0)[0], csref.sense_unfold(aliased, maps, 1, 0.0)[0]):
+        assert np.abs(out - aliased.mean(0)).max() < 1e-4
+    maps3 = np.ones((3, 6, 5), np.complex64)              # sense.rs:398-421: g = 1 with R = 1
+    for g in (sref.sense_unfold_1d(np.zeros_like(maps3), maps3, 1, 0.0, gfactor=True)[1],
+              csref.sense_unfold(np.zeros_like(maps3), maps3, 1, 0.0, gfactor=True)[1]):
+        assert np.abs(g - 1.0).max() < 1e-5
+
+
+def test_sense_fp32_restatement_matches_fp64():
+    from oracle import sense_fp64 as sref
+    rng = np.random.default_rng(8)
+    nc, ny, nx, r = 6, 24, 10, 3
+    maps = (rng.standard_normal((nc, ny, nx)) + 1j * rng.standard_normal((nc, ny, nx))).astype(np.complex64)
+    al = (rng.standard_normal((nc, ny, nx)) + 1j * rng.standard_normal((nc, ny, nx))).astype(np.complex64)
+    o32, g32 = csref.sense_unfold(al, maps, r, 1e-3, gfactor=True)
+    o64, g64 = sref.sense_unfold_1d(al, maps, r, 1e-3, gfactor=True)
+    assert np.linalg.norm(o32 - o64) / np.linalg.norm(o64) < 1e-5
+    assert np.linalg.norm(g32 - g64) / np.linalg.norm(g64) < 1e-5
