@@ -108,6 +108,9 @@ const char* okscuda_version(void);
  *                   (192, 256, 320, 384, 512, 640), 1-4 a (columns, threads per column)
  *                   form (16,32) (16,64) (8,64) (8,32) for every length but 368,
  *                   -1 never
+ *   "xform_row_variant" register row transform: 0 (default) the fastest plan
+ *                   per length; 1 the E = 8 plans for 192 (8·3·8) and 320
+ *                   (8·5·8); 2 the 96-thread plan 4·12·4 for 192 (measurement)
  *   "xform_lanes_pf" lanes form: 1 (default) = software-pipelined (the next
  *                   tile is copied into shared memory with cp.async while the
  *                   current one is transformed; even nx and 16-byte aligned
@@ -416,6 +419,27 @@ size_t okscuda_acq_set_size(void);
  * (phasecorr.rs:61-169, strategy.rs:807-815). */
 int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, const okscuda_acq_set* acqs,
                               float* h_out, long long out_cap, int* out_dims);
+
+/* ------------------------------------------------ acquisition ingest */
+/* IsmrmrdFile::open + the rows of /dataset/data (reader.rs:15-24, 47-76;
+ * acquisition.rs:33-95; header.rs) without HDF5: the same rows serialised
+ * as an acquisition stream file --
+ *   "OKSACQ1\0", u32 xml_len, the ISMRMRD XML header, u64 n_acq, then per
+ *   acquisition the packed 340-byte little-endian AcquisitionHeader (field
+ *   order of acquisition.rs:33-59), f32 traj[trajectory_dimensions *
+ *   number_of_samples], f32 data[2 * active_channels * number_of_samples].
+ * okscuda_raw_open reads the headers, then the samples straight into one
+ * pinned host buffer (ordinary memory when no device is present), and parses
+ * the XML for the encoded / recon matrix sizes and the ky / kz encoding
+ * centres (header.rs:128-206 tag-path rules).  OKS_EINVAL for an unreadable
+ * or malformed file (IoError).  Host only (no context). */
+typedef struct okscuda_raw okscuda_raw;
+int okscuda_raw_open(const char* path, okscuda_raw** out);
+/* The okscuda_acq_set of an open file (valid until okscuda_raw_close). */
+int okscuda_raw_acq_set(const okscuda_raw* raw, okscuda_acq_set* out);
+/* acquisitionSystemInformation/receiverChannels and the XML length. */
+int okscuda_raw_info(const okscuda_raw* raw, int* receiver_channels, int* xml_len);
+void okscuda_raw_close(okscuda_raw* raw);
 
 /* ------------------------------------------------------------- profiling */
 /* No reference counterpart (the reference has no timing hooks).  When

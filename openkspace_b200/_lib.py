@@ -69,6 +69,10 @@ SIGNATURES = {
     "okscuda_cs_batch": (_i, [_vp, _vp, _i]),
     "okscuda_sense_cs": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _i, _i, _i, _vp, _vp, _vp,
                               _c.POINTER(_c.c_double)]),
+    "okscuda_raw_open": (_i, [_c.c_char_p, _c.POINTER(_vp)]),
+    "okscuda_raw_acq_set": (_i, [_vp, _vp]),
+    "okscuda_raw_info": (_i, [_vp, _c.POINTER(_i), _c.POINTER(_i)]),
+    "okscuda_raw_close": (None, [_vp]),
     "okscuda_sense_unfold": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _f, _vp, _vp]),
     "okscuda_percentile": (_i, [_vp, _vp, _c.c_longlong, _f, _c.POINTER(_f)]),
     "okscuda_window_u8": (_i, [_vp, _vp, _c.c_longlong, _f, _f, _i, _vp]),

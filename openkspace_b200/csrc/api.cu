@@ -135,6 +135,9 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value != 0 && value != 2 && value != 4 && value != 8)
             return set_err(ctx, OKS_EINVAL, "xform_tile: 0 (by length), 2, 4 or 8 column pairs");
         ctx->xform_tile = (int)value;
+    } else if (!std::strcmp(name, "xform_row_variant")) {
+        if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");
+        ctx->xform_row_variant = (int)value;
     } else if (!std::strcmp(name, "xform_lanes_pf")) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "xform_lanes_pf: 0 or 1");
         ctx->xform_lanes_pf = (int)value;
@@ -240,6 +243,7 @@ int okscuda_centred_fft2(okscuda_ctx* ctx, okscuda_c64* d_data, int batch, int n
     float2* d = reinterpret_cast<float2*>(d_data);
     oks::RowXformArgs ra{};
     ra.reg = ctx->xform_reg;
+    ra.variant = ctx->xform_row_variant;
     ra.in = d; ra.out = d; ra.nrows = (long long)batch * ny; ra.ld_in = nx; ra.ld_out = nx;
     ra.sign = inverse ? +1 : -1; ra.centred = 1; ra.scale = 1.0f; ra.rows_per_prob = ny;
     {

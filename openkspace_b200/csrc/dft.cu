@@ -18,6 +18,7 @@ extern "C" int okscuda_dft_rows(okscuda_ctx* ctx, const okscuda_c64* d_in, okscu
         if (rc) return rc;
         oks::RowXformArgs ra{};
         ra.reg = ctx->xform_reg;
+        ra.variant = ctx->xform_row_variant;
         ra.in = reinterpret_cast<const float2*>(d_in);
         ra.out = reinterpret_cast<float2*>(d_out);
         ra.nrows = nrows;

@@ -547,18 +547,26 @@ bool xform_reg_supported(int n) {
 }
 
 namespace reg {
-// Row plan for 192: 4·12·4 on 96 threads (every lane active; the 8·3·8 plan
-// leaves 16 of 64 idle): 4.17 against 3.64 TB/s on B200.  Measured and not
-// taken: 640 = 4·4·10·4 (3.84 against 4.73), 320 = 4·5·4·4 (4.14 against
-// 4.40), 368 on 184 threads (2.91 against 2.93).
+// Row plans for 192 measured on B200 (GB/s of the row pass, 1 GiB of
+// planes): 12·4·4 on 32 threads, four row pairs per CTA (P192), 5610; 4·12·4
+// on 96 threads (R192), 4445; 8·3·8 on 48 of 64 threads (S192), 3864.  P192
+// is the default.  Measured and not taken elsewhere: 640 = 4·4·10·4 (3.84
+// against 4.73 TB/s), 320 = 4·5·4·4 (4.14 against 4.40) and 8·5·8 on 80 of 96
+// threads (3.97 against 4.04), 368 on 184 threads (2.91 against 2.93).
 using R192 = Plan<192, 96, 4, 12, 4>;
 }  // namespace reg
 
 cudaError_t launch_row_xform_reg(const RowXformArgs& a, int n, cudaStream_t st) {
     if (a.nrows <= 0) return cudaSuccess;
+    // alternative row plans (option xform_row_variant), for measurement
+    if (a.variant == 1 && !a.tables) {
+        if (n == 192) return reg::row_p<reg::S192>(a, st);    // 8·3·8 on 48 of 64 threads
+        if (n == 320) return reg::row_p<reg::V320>(a, st);    // 8·5·8 on 80 of 96 threads
+    }
+    if (a.variant == 2 && !a.tables && n == 192) return reg::row_p<reg::R192>(a, st);   // 4·12·4 on 96 threads
     switch (n) {
         case 128: return reg::row_p<reg::S128>(a, st);
-        case 192: return reg::row_p<reg::R192>(a, st);
+        case 192: return reg::row_p<reg::P192>(a, st);
         case 256: return reg::row_p<reg::S256>(a, st);
         case 320: return reg::row_p<reg::S320>(a, st);
         case 368: return reg::row_p<reg::S368>(a, st);
@@ -581,7 +589,7 @@ static int row_tables_p(float2* h, int cap, int* nroots) {
 int row_xform_reg_tables(int n, float2* h, int cap, int* nroots) {
     switch (n) {
         case 128: return reg::row_tables_p<reg::S128>(h, cap, nroots);
-        case 192: return reg::row_tables_p<reg::R192>(h, cap, nroots);
+        case 192: return reg::row_tables_p<reg::P192>(h, cap, nroots);
         case 256: return reg::row_tables_p<reg::S256>(h, cap, nroots);
         case 320: return reg::row_tables_p<reg::S320>(h, cap, nroots);
         case 368: return reg::row_tables_p<reg::S368>(h, cap, nroots);

@@ -69,6 +69,7 @@ struct RowXformArgs {
     // layout); null: the tables the library builds on first use
     const float2* tables = nullptr;
     int tables_nroots = 0;
+    int variant = 0;     // register kernel: 0 the default plan per length, 1 / 2 alternatives (192, 320)
 };
 cudaError_t launch_row_xform(const RowXformArgs& a, const DevPlan& pl, cudaStream_t st);
 

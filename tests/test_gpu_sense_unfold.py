@@ -51,10 +51,10 @@ def test_reference_cases_on_the_device(ctx):
 def test_walsh_maps_then_unfold(ctx):
     """The sense strategy's chain on a synthetic slice: Walsh maps of the
     device SENSE path, aliased images of a regular R = 2 mask, unfold."""
-    s = synth.make_slice(64, 48, 6, 4.0, 12, seed=3)
+    s = synth.make_slice(128, 48, 6, 4.0, 12, seed=3)
     _, _, maps, _ = ctx.sense_cs(s.kspace, s.mask2d, 1, 0.0)
     k = np.array(s.kspace)
-    m = np.zeros(64, bool)
+    m = np.zeros(128, bool)
     m[::2] = True
     k[:, ~m, :] = 0
     al = np.fft.ifft(k, axis=1).astype(np.complex64)

@@ -151,3 +151,17 @@ def test_fista_prep_rows_same_on_both_engines(ctx, rng):
     want = o64.fista_cs_single_coil(k, m, 20, 0.01)
     assert o64.nrmse(reg, want) < 1e-4
     assert o64.nrmse(reg, gen) < 1e-5
+
+
+@pytest.mark.parametrize("n,variant", [(192, 1), (192, 2), (320, 1)])
+def test_row_plan_variants(ctx, rng, n, variant):
+    """The alternative register row plans (option xform_row_variant)."""
+    x = crandn(rng, (3, 40, n))
+    ctx.set_option("xform_row_variant", variant)
+    try:
+        got = ctx.centred_fft2(x, False)
+        got_i = ctx.dft_rows(x.reshape(-1, n), inverse=True, centred=True, engine=0)
+    finally:
+        ctx.set_option("xform_row_variant", 0)
+    assert rel_l2(got, o64.centred_fft2(x)) < TOL
+    assert rel_l2(got_i, ref_rows(x.reshape(-1, n), 1, 1)) < TOL
