@@ -108,7 +108,8 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
     } else if (!std::strcmp(name, "mask_bits")) {
         ctx->mask_bits = value != 0;
     } else if (!std::strcmp(name, "occ2d")) {
-        if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "occ2d: 0 (1 CTA), 1 (12 warps), 2 (18 warps)");
+        if (value < 0 || value > 3)
+            return set_err(ctx, OKS_EINVAL, "occ2d: 0 (1 CTA), 1 (12 warps), 2 (18 warps), 3 (15 warps)");
         ctx->occ2d = (int)value;
     } else if (!std::strcmp(name, "prefetch2d")) {
         if (value < 0 || value > 7)
@@ -135,6 +136,9 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value != 0 && value != 2 && value != 4 && value != 8)
             return set_err(ctx, OKS_EINVAL, "xform_tile: 0 (by length), 2, 4 or 8 column pairs");
         ctx->xform_tile = (int)value;
+    } else if (!std::strcmp(name, "col2d_lanes")) {
+        if (value < 0 || value > 6) return set_err(ctx, OKS_EINVAL, "col2d_lanes: 0 off, 1 to 6 a lanes form");
+        ctx->col2d_lanes = (int)value;
     } else if (!std::strcmp(name, "xform_row_variant")) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");
         ctx->xform_row_variant = (int)value;
@@ -142,7 +146,7 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "xform_lanes_pf: 0 or 1");
         ctx->xform_lanes_pf = (int)value;
     } else if (!std::strcmp(name, "xform_lanes")) {
-        if (value < -1 || value > 4) return set_err(ctx, OKS_EINVAL, "xform_lanes: -1 off, 0 by length, 1 to 4");
+        if (value < -1 || value > 6) return set_err(ctx, OKS_EINVAL, "xform_lanes: -1 off, 0 by length, 1 to 6");
         ctx->xform_lanes = (int)value;
     } else if (!std::strcmp(name, "fista2d_streams")) {
         if (value < 1 || value > 8) return set_err(ctx, OKS_EINVAL, "fista2d_streams: 1 to 8");
@@ -479,6 +483,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             a.occ = tp.occ2d;
             a.prefetch = tp.prefetch2d;
             a.err = ctx->tc_err;
+            a.col_lanes = ctx->col2d_lanes;
             auto col = [&](int mode) {
                 if (col_reg) {
                     ProfScope ps(ctx, "k2d_col_reg", st);
@@ -562,10 +567,10 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     const size_t data_bytes = sizeof(float2) * (size_t)nprob * N;
     if (ctx->graph2d && !use_tc) {
         char kb[320];
-        std::snprintf(kb, sizeof kb, "%d/%d/%lld/%d/%d/%08x/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%zu/%d", ny, nx, nprob, nmask, iters,
-                      [&] { uint32_t u; std::memcpy(&u, &lambda, 4); return u; }(), chunk, ns, (int)col_reg,
+        std::snprintf(kb, sizeof kb, "%d/%d/%lld/%d/%d/%08x/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%zu/%d/%d", ny, nx, nprob, nmask,
+                      iters, [&] { uint32_t u; std::memcpy(&u, &lambda, 4); return u; }(), chunk, ns, (int)col_reg,
                       (int)row_reg, tp.persist2d, tp.occ2d, tp.prefetch2d, (int)separable, ctx->mask_bits, up.size(),
-                      ctx->device);
+                      ctx->device, ctx->col2d_lanes);
         const std::string key(kb);
         auto it = ctx->g2d.find(key);
         if (it == ctx->g2d.end()) {

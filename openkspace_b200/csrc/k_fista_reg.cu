@@ -798,8 +798,17 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
     return cudaGetLastError();
 }
 
+// The 15-warp form (a.occ = 3): between the two above (the 368 column pass
+// at 5 CTAs of 96 threads per SM, 136 registers).
+template <class P>
+constexpr int occ_blocks_mid() {
+    constexpr int threads = P::T * (P::T == 32 ? 4 : 1);
+    return (15 * 32 + threads - 1) / threads;
+}
+
 template <class P>
 static cudaError_t launch_2d(const Fista2dArgs& a, long long units, cudaStream_t st, int mode, int it, bool row) {
+    if (a.occ == 3) return launch_2d_k<P, occ_blocks_mid<P>()>(a, units, st, mode, it, row);
     if (a.occ == 2) return launch_2d_k<P, occ_blocks_hi<P>()>(a, units, st, mode, it, row);
     if (a.occ) return launch_2d_k<P, occ_blocks<P>()>(a, units, st, mode, it, row);
     return launch_2d_k<P, 1>(a, units, st, mode, it, row);
@@ -808,6 +817,8 @@ static cudaError_t launch_2d(const Fista2dArgs& a, long long units, cudaStream_t
 template <class P>
 static cudaError_t col2d(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st) {
     (void)tabs;
+    if (a.col_lanes > 0 && (a.nx % 2) == 0 && (reinterpret_cast<uintptr_t>(a.S) & 15) == 0)
+        return launch_fista2d_col_lanes(a, a.col_lanes, mode, st);
     return launch_2d<P>(a, a.nprob * (a.nx / 2), st, mode, 0, false);
 }
 template <class P>

@@ -16,6 +16,8 @@
 // pair per thread group.  The tile arrives through the same kind of staging
 // buffer in whole 2G * 8-byte row segments; results go back through the
 // groups' exchange buffers so that the CTA writes whole row segments too.
+#include <type_traits>
+
 #include "reg_fft.cuh"
 
 namespace oks {
@@ -250,21 +252,88 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
 // writes).  Twiddles depend on the row only: one broadcast per half-warp.
 // PF: stage 0 reads its inputs from the staging tile ST ([N][CW], filled by
 // cp.async while the previous tile was transformed) instead of global memory.
+// Output pairs Q, Q + 1, ..., (R - 1) / 2 of a large odd-radix butterfly
+// (symmetric form, compile-time roots) stored to the lanes tile.
+template <int SIGN, int R, int Q, int CW>
+__device__ __forceinline__ void lanes_odd_pairs(const float2* a, const float2* b, float2 x0, float2* D, int ob,
+                                                int p, int c) {
+    if constexpr (Q <= (R - 1) / 2) {
+        float2 re = x0, im = make_float2(0.f, 0.f);
+        odd_acc<R, Q, 1>(a, b, re, im);
+        const float2 si = mul_si<SIGN>(im);
+        D[(ob + Q * p) * CW + c] = re + si;
+        D[(ob + (R - Q) * p) * CW + c] = re - si;
+        lanes_odd_pairs<SIGN, R, Q + 1, CW>(a, b, x0, D, ob, p, c);
+    }
+}
+
 // After every thread has read ST, refill() issues the next tile's copies.
 struct NoRefill {
     __device__ void operator()() const {}
 };
-template <class P, int SIGN, int CW, int TPC, int s, bool PF = false, class F = NoRefill>
+// Last-stage output: NoOut writes the column to global memory (centring
+// sign and scale applied); any other functor receives (row, value).
+struct NoOut {
+    __device__ void operator()(int, float2) const {}
+};
+template <class P, int SIGN, int CW, int TPC, int s, bool PF = false, class F = NoRefill, class Out = NoOut>
 __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2* __restrict__ TW,
                                             const float2* __restrict__ RT, float2* __restrict__ col, int nx,
                                             bool on, bool centred, float sc, int c, int tc,
-                                            const float2* __restrict__ ST = nullptr, const F& refill = F()) {
+                                            const float2* __restrict__ ST = nullptr, const F& refill = F(),
+                                            const Out& out = Out()) {
     constexpr int S = P::S, N = P::N;
     constexpr int R = SIGN < 0 ? P::R[s] : P::R[S - 1 - s];
     constexpr int p = SIGN < 0 ? P::prod(s) : P::rprod(s);
     constexpr int off = SIGN < 0 ? Tw<P>::fwd(s) : Tw<P>::inv(s);
     constexpr int NB = N / R;
     constexpr int BPT = (NB + TPC - 1) / TPC;   // butterflies per thread
+    if constexpr (R % 2 == 1 && R > 5) {
+        // Large odd radix (the middle stage of 368 = 4·23·4): each thread folds
+        // its butterflies' inputs, a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j}
+        // (twiddled), and after the barrier forms the output pairs with
+        // compile-time roots; one thread per butterfly, no repeated folds.
+        static_assert(s > 0 && s < S - 1, "the large odd radix is a middle stage");
+        constexpr int H = (R - 1) / 2;
+        float2 x0[BPT], fa[BPT][H], fb[BPT][H];
+#pragma unroll
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (NB % TPC != 0 && b >= NB) break;
+            const int k = b % p;
+            x0[bb] = OKS_IN(b * CW + c, N * CW, OKS_B_TILE) ? D[b * CW + c] : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 1; j <= H; ++j) {
+                float2 u = D[(b + j * NB) * CW + c];
+                float2 w = D[(b + (R - j) * NB) * CW + c];
+                if (p > 1) {
+                    u = twmul<SIGN>(u, TW[off + k * (R - 1) + j - 1]);
+                    w = twmul<SIGN>(w, TW[off + k * (R - 1) + R - j - 1]);
+                }
+                fa[bb][j - 1] = u + w;
+                fb[bb][j - 1] = u - w;
+            }
+        }
+        __syncthreads();                                  // in place: all inputs read before any output lands
+#pragma unroll
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (NB % TPC != 0 && b >= NB) break;
+            const int k = b % p;
+            const int ob = (b - k) * R + k;
+            float2 y0 = x0[bb];
+#pragma unroll
+            for (int j = 0; j < H; ++j) y0 = y0 + fa[bb][j];
+            if (OKS_IN((ob + (R - 1) * p) * CW + c, N * CW, OKS_B_TILE)) {
+                D[ob * CW + c] = y0;
+                lanes_odd_pairs<SIGN, R, 1, CW>(fa[bb], fb[bb], x0[bb], D, ob, p, c);
+            }
+        }
+        __syncthreads();
+        lanes_stage<P, SIGN, CW, TPC, s + 1, false, NoRefill, Out>(D, TW, RT, col, nx, on, centred, sc, c, tc, nullptr,
+                                                                  NoRefill(), out);
+        return;
+    } else {
     float2 v[BPT][R];
 #pragma unroll
     for (int bb = 0; bb < BPT; ++bb) {
@@ -304,7 +373,11 @@ __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2
         for (int j = 0; j < R; ++j) {
             const int o = ob + j * p;
             if constexpr (s == S - 1) {
-                if (on) col[o * nx] = v[bb][j] * ((centred && (o & 1)) ? -sc : sc);
+                if constexpr (std::is_same<Out, NoOut>::value) {
+                    if (on) col[o * nx] = v[bb][j] * ((centred && (o & 1)) ? -sc : sc);
+                } else {
+                    out(o, v[bb][j]);
+                }
             } else if (OKS_IN(o * CW + c, N * CW, OKS_B_TILE)) {
                 D[o * CW + c] = v[bb][j];
             }
@@ -312,7 +385,9 @@ __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2
     }
     if constexpr (s < S - 1) {
         __syncthreads();
-        lanes_stage<P, SIGN, CW, TPC, s + 1>(D, TW, RT, col, nx, on, centred, sc, c, tc);
+        lanes_stage<P, SIGN, CW, TPC, s + 1, false, NoRefill, Out>(D, TW, RT, col, nx, on, centred, sc, c, tc, nullptr,
+                                                                  NoRefill(), out);
+    }
     }
 }
 
@@ -511,11 +586,17 @@ constexpr int lanes_default() {
 // (lanes 1..4: (16, 32), (16, 64), (8, 64), (8, 32)).
 template <class P>
 static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) {
-    switch (lanes) {
-        case 2: return col_lanes_k<P, 16, 64>(a, st);
-        case 3: return col_lanes_k<P, 8, 64>(a, st);
-        case 4: return col_lanes_k<P, 8, 32>(a, st);
-        default: return col_lanes_k<P, 16, 32>(a, st);
+    if constexpr (big_odd_plan<P>()) {
+        // 16 threads per column: one per radix-23 butterfly (368 / 23 = 16)
+        if (lanes == 6) return col_lanes_k<P, 8, 16>(a, st);
+        return col_lanes_k<P, 16, 16>(a, st);
+    } else {
+        switch (lanes) {
+            case 2: return col_lanes_k<P, 16, 64>(a, st);
+            case 3: return col_lanes_k<P, 8, 64>(a, st);
+            case 4: return col_lanes_k<P, 8, 32>(a, st);
+            default: return col_lanes_k<P, 16, 32>(a, st);
+        }
     }
 }
 
@@ -523,10 +604,15 @@ static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) 
 // CTA (1024 threads, 64 registers each) and one SM's shared memory, else 4.
 template <class P>
 static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
-    if constexpr (!big_odd_plan<P>()) {
+    {
         // columns across the lanes (in-problem offsets in 32 bits) where that
-        // form measured faster than the tiles: 192, 256, 320, 384, 512, 640
-        const int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
+        // form measured faster than the tiles: 192, 256, 320, 384, 512, 640;
+        // 368 takes the forms 5 and 6 (16 threads per column), others 1-4
+        int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
+        if (lanes > 0) {
+            if constexpr (big_odd_plan<P>()) lanes = lanes < 5 ? 5 : lanes;
+            else lanes = lanes > 4 ? 1 : lanes;
+        }
         if (a.tile == 0 && lanes > 0 && (long long)P::N * a.nx < (1ll << 31)) return col_lanes<P>(a, lanes, st);
     }
     constexpr bool g8 = P::N <= 512 && P::T * 8 <= 1024 && !big_odd_plan<P>();
@@ -537,7 +623,131 @@ static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
     return col_pg<P, 2>(a, st);
 }
 
+// 2-D-mask engine, column pass in the lanes form: one CTA per tile of CW
+// columns of one problem (tiles without a sampled column are skipped).  The
+// S tile comes in whole row segments (16-byte cp.async) into ST; the forward
+// transform runs in place in D with the lanes across the columns, and its
+// last stage writes the data residual m' (F S - y') back into ST; the
+// inverse transform reads ST and its last stage writes S.  Same arithmetic
+// as k2d_col_reg (plain DFTs of the modulated state, y' signed by
+// (-1)^(r + x) and scaled by ysc); mode 0 forms S = F^H (m' y').
+template <class P, int CW, int TPC>
+__global__ void __launch_bounds__(CW * TPC, xform_min_blocks<CW * TPC, lanes_regs<P, TPC>()>())
+k2d_col_lanes(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float2* __restrict__ groots,
+              int roots_total) {
+    constexpr int N = P::N;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* D = sm;                                  // [N][CW] transform stages
+    float2* ST = sm + N * CW;                        // [N][CW] S tile, then the residual
+    float2* TWs = ST + N * CW;                       // both directions' twiddles
+    float2* RT = TWs + Tw<P>::total();
+    for (int q = threadIdx.x; q < Tw<P>::total(); q += blockDim.x) TWs[q] = gtw[q];
+    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    const int c = threadIdx.x % CW, tc = threadIdx.x / CW;
+    const int nx = a.nx;
+    const int ntx = (nx + CW - 1) / CW;
+    const long long total = a.nprob * ntx;
+    const float minv = a.minv, ysc = a.ysc;
+    for (long long u = blockIdx.x; u < total; u += gridDim.x) {
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const long long mi = (p + a.mask_offset) % a.mask_mod;
+        const uint32_t* cb = a.colbits + mi * a.col_wstride;
+        bool any = false;                            // the same answer in every thread
+        for (int cc = 0; cc < CW; ++cc) {
+            const int xx = x0 + cc;
+            if (xx < nx && ((__ldg(cb + (xx >> 5)) >> (xx & 31)) & 1u)) any = true;
+        }
+        if (!any) continue;                          // S there is never read
+        const int x = x0 + c;
+        const bool on = x < nx;
+        const bool colon = on && ((__ldg(cb + (x >> 5)) >> (x & 31)) & 1u);
+        const uint32_t* rb = a.rowbits + mi * a.row_wstride;
+        const uint8_t* mk = a.mask + mi * a.mask_stride;
+        float2* S = a.S + p * a.st_stride;
+        const float2* y = a.y + p * a.y_stride;
+        auto sampled = [&](int r) {
+            return colon && (a.separable ? ((__ldg(rb + (r >> 5)) >> (r & 31)) & 1u) != 0 : mk[(long long)r * nx + x] != 0);
+        };
+        auto yprime = [&](int r) { return y[(long long)r * nx + x] * (((r + x) & 1) ? -ysc : ysc); };
+        __syncthreads();                             // tables loaded; the last tile's inverse has read ST and D
+        if (mode) {
+            for (int k = threadIdx.x; k < N * (CW / 2); k += CW * TPC) {
+                const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+                const bool onj = x0 + j < nx;
+                if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                    cp_async16(ST + r * CW + j, onj ? S + (long long)r * nx + x0 + j : S, onj ? 16u : 0u);
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncthreads();
+            auto resid = [&](int o, float2 v) {
+                const bool m = sampled(o);
+                ST[o * CW + c] = m ? (v - yprime(o)) * minv : make_float2(0.f, 0.f);
+            };
+            lanes_stage<P, -1, CW, TPC, 0, true, NoRefill, decltype(resid)>(D, TWs, RT, nullptr, nx, on, false, 1.f,
+                                                                           c, tc, ST, NoRefill(), resid);
+        } else {
+            for (int r = tc; r < N; r += TPC) ST[r * CW + c] = sampled(r) ? yprime(r) * minv : make_float2(0.f, 0.f);
+        }
+        __syncthreads();                             // the residual tile is complete
+        auto store = [&](int o, float2 v) {
+            if (on) S[(long long)o * nx + x] = v;
+        };
+        lanes_stage<P, +1, CW, TPC, 0, true, NoRefill, decltype(store)>(D, TWs, RT, nullptr, nx, on, false, 1.f, c,
+                                                                       tc, ST, NoRefill(), store);
+    }
+}
+
+template <class P, int CW, int TPC>
+static cudaError_t col2d_lanes_k(const Fista2dArgs& a, int mode, cudaStream_t st) {
+    const float2 *tw, *rt;
+    int nrt;
+    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)2 * P::N * CW + Tw<P>::total() + nrt);
+    const void* fn = reinterpret_cast<const void*>(k2d_col_lanes<P, CW, TPC>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = a.nprob * ((a.nx + CW - 1) / CW);
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, CW * TPC, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    k2d_col_lanes<P, CW, TPC><<<(unsigned)grid, CW * TPC, smem, st>>>(a, mode, tw, rt, nrt);
+    return cudaGetLastError();
+}
+
+template <class P>
+static cudaError_t col2d_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st) {
+    if constexpr (big_odd_plan<P>()) {
+        if (form == 6) return col2d_lanes_k<P, 8, 16>(a, mode, st);
+        return col2d_lanes_k<P, 16, 16>(a, mode, st);
+    } else {
+        switch (form) {
+            case 2: return col2d_lanes_k<P, 16, 64>(a, mode, st);
+            case 3: return col2d_lanes_k<P, 8, 64>(a, mode, st);
+            case 4: return col2d_lanes_k<P, 8, 32>(a, mode, st);
+            default: return col2d_lanes_k<P, 16, 32>(a, mode, st);
+        }
+    }
+}
+
 }  // namespace reg
+
+cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st) {
+    if (a.nprob <= 0) return cudaSuccess;
+    if (a.nx % 2 || (reinterpret_cast<uintptr_t>(a.S) & 15)) return cudaErrorInvalidValue;
+    switch (a.ny) {
+        case 128: return reg::col2d_lanes<reg::S128>(a, form, mode, st);
+        case 192: return reg::col2d_lanes<reg::S192>(a, form, mode, st);
+        case 256: return reg::col2d_lanes<reg::S256>(a, form, mode, st);
+        case 320: return reg::col2d_lanes<reg::S320>(a, form, mode, st);
+        case 368: return reg::col2d_lanes<reg::S368>(a, form, mode, st);
+        case 384: return reg::col2d_lanes<reg::S384>(a, form, mode, st);
+        case 512: return reg::col2d_lanes<reg::S512>(a, form, mode, st);
+        case 640: return reg::col2d_lanes<reg::P640>(a, form, mode, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
 
 bool xform_reg_supported(int n) {
     switch (n) {

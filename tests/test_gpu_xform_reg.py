@@ -165,3 +165,21 @@ def test_row_plan_variants(ctx, rng, n, variant):
         ctx.set_option("xform_row_variant", 0)
     assert rel_l2(got, o64.centred_fft2(x)) < TOL
     assert rel_l2(got_i, ref_rows(x.reshape(-1, n), 1, 1)) < TOL
+
+
+@pytest.mark.parametrize("pf", [0, 1])
+@pytest.mark.parametrize("lanes", [5, 6])
+def test_column_lanes_368(ctx, rng, lanes, pf):
+    """The 368-point lanes forms (16 threads per column, one per radix-23
+    butterfly), pipelined and direct, ragged and odd column counts."""
+    for ncols, inverse in ((38, True), (130, False), (7, True)):
+        x = crandn(rng, (2, 368, ncols))
+        want = o64.centred_ifft2(x) if inverse else o64.centred_fft2(x)
+        ctx.set_option("xform_lanes", lanes)
+        ctx.set_option("xform_lanes_pf", pf)
+        try:
+            got = ctx.centred_fft2(x, inverse)
+        finally:
+            ctx.set_option("xform_lanes", 0)
+            ctx.set_option("xform_lanes_pf", 1)
+        assert rel_l2(got, want) < TOL
