@@ -90,7 +90,7 @@ const char* okscuda_version(void);
  *   "col2d_lanes"   2-D-mask engine column pass: 0 (default) one column pair
  *                   per thread group; 1-6 the lanes form (tiles of 8 or 16
  *                   columns in shared memory, lanes across the columns; the
- *                   forms of "xform_lanes", 5-6 for 368)
+ *                   forms of "xform_lanes", 5-8 for 368)
  *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
  *                   least 12 warps resident per SM, 2 = at least 18, 3 = at
  *                   least 15, 0 = registers as needed
@@ -111,8 +111,9 @@ const char* okscuda_version(void);
  *                   memory): 0 (default) for the lengths where it is faster
  *                   (192, 256, 320, 384, 512, 640), 1-4 a (columns, threads per column)
  *                   form (16,32) (16,64) (8,64) (8,32) for every length but 368,
- *                   5-6 the 368 forms (16,16) (8,16) with one thread per
- *                   radix-23 butterfly, -1 never
+ *                   5-8 the 368 forms (16,16) (8,16) (16,32) (8,32), 16
+ *                   threads per column being one per radix-23 butterfly,
+ *                   -1 never
  *   "xform_row_variant" register row transform: 0 (default) the fastest plan
  *                   per length; 1 the E = 8 plans for 192 (8·3·8) and 320
  *                   (8·5·8); 2 the 96-thread plan 4·12·4 for 192 (measurement)

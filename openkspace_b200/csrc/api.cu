@@ -137,7 +137,7 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
             return set_err(ctx, OKS_EINVAL, "xform_tile: 0 (by length), 2, 4 or 8 column pairs");
         ctx->xform_tile = (int)value;
     } else if (!std::strcmp(name, "col2d_lanes")) {
-        if (value < 0 || value > 6) return set_err(ctx, OKS_EINVAL, "col2d_lanes: 0 off, 1 to 6 a lanes form");
+        if (value < 0 || value > 8) return set_err(ctx, OKS_EINVAL, "col2d_lanes: 0 off, 1 to 8 a lanes form");
         ctx->col2d_lanes = (int)value;
     } else if (!std::strcmp(name, "xform_row_variant")) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");
@@ -146,7 +146,7 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "xform_lanes_pf: 0 or 1");
         ctx->xform_lanes_pf = (int)value;
     } else if (!std::strcmp(name, "xform_lanes")) {
-        if (value < -1 || value > 6) return set_err(ctx, OKS_EINVAL, "xform_lanes: -1 off, 0 by length, 1 to 6");
+        if (value < -1 || value > 8) return set_err(ctx, OKS_EINVAL, "xform_lanes: -1 off, 0 by length, 1 to 8");
         ctx->xform_lanes = (int)value;
     } else if (!std::strcmp(name, "fista2d_streams")) {
         if (value < 1 || value > 8) return set_err(ctx, OKS_EINVAL, "fista2d_streams: 1 to 8");

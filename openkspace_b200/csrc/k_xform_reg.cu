@@ -587,8 +587,11 @@ constexpr int lanes_default() {
 template <class P>
 static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) {
     if constexpr (big_odd_plan<P>()) {
-        // 16 threads per column: one per radix-23 butterfly (368 / 23 = 16)
+        // 16 threads per column: one per radix-23 butterfly (368 / 23 = 16);
+        // 32: half of them idle in that stage, fewer butterflies each in the others
         if (lanes == 6) return col_lanes_k<P, 8, 16>(a, st);
+        if (lanes == 7) return col_lanes_k<P, 16, 32>(a, st);
+        if (lanes == 8) return col_lanes_k<P, 8, 32>(a, st);
         return col_lanes_k<P, 16, 16>(a, st);
     } else {
         switch (lanes) {
@@ -610,7 +613,7 @@ static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
         // 368 takes the forms 5 and 6 (16 threads per column), others 1-4
         int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
         if (lanes > 0) {
-            if constexpr (big_odd_plan<P>()) lanes = lanes < 5 ? 5 : lanes;
+            if constexpr (big_odd_plan<P>()) lanes = lanes < 5 ? 5 : lanes;   // 5-8
             else lanes = lanes > 4 ? 1 : lanes;
         }
         if (a.tile == 0 && lanes > 0 && (long long)P::N * a.nx < (1ll << 31)) return col_lanes<P>(a, lanes, st);
@@ -638,8 +641,9 @@ k2d_col_lanes(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const flo
     constexpr int N = P::N;
     extern __shared__ __align__(16) float2 sm[];
     float2* D = sm;                                  // [N][CW] transform stages
-    float2* ST = sm + N * CW;                        // [N][CW] S tile, then the residual
-    float2* TWs = ST + N * CW;                       // both directions' twiddles
+    float2* ST = sm + N * CW;                        // [N][CW] S tile (the next one lands here early)
+    float2* RS = ST + N * CW;                        // [N][CW] F S, then the residual
+    float2* TWs = RS + N * CW;                       // both directions' twiddles
     float2* RT = TWs + Tw<P>::total();
     for (int q = threadIdx.x; q < Tw<P>::total(); q += blockDim.x) TWs[q] = gtw[q];
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
@@ -648,17 +652,43 @@ k2d_col_lanes(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const flo
     const int ntx = (nx + CW - 1) / CW;
     const long long total = a.nprob * ntx;
     const float minv = a.minv, ysc = a.ysc;
-    for (long long u = blockIdx.x; u < total; u += gridDim.x) {
+    // tiles with a sampled column (the same answer in every thread)
+    auto has_sample = [&](long long u) {
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const uint32_t* cb = a.colbits + ((p + a.mask_offset) % a.mask_mod) * a.col_wstride;
+        for (int cc = 0; cc < CW; ++cc) {
+            const int xx = x0 + cc;
+            if (xx < nx && ((__ldg(cb + (xx >> 5)) >> (xx & 31)) & 1u)) return true;
+        }
+        return false;
+    };
+    auto next_tile = [&](long long u) {
+        for (; u < total; u += gridDim.x)
+            if (has_sample(u)) break;
+        return u;
+    };
+    // the S tile of unit u into ST: whole row segments, 16-byte cp.async
+    auto issue = [&](long long u) {
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const float2* S = a.S + p * a.st_stride;
+        for (int k = threadIdx.x; k < N * (CW / 2); k += CW * TPC) {
+            const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+            const bool onj = x0 + j < nx;
+            if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                cp_async16(ST + r * CW + j, onj ? S + (long long)r * nx + x0 + j : S, onj ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    long long u = next_tile(blockIdx.x);
+    if (mode && u < total) issue(u);
+    while (u < total) {
+        const long long un = next_tile(u + gridDim.x);
         const long long p = u / ntx;
         const int x0 = (int)(u - p * ntx) * CW;
         const long long mi = (p + a.mask_offset) % a.mask_mod;
         const uint32_t* cb = a.colbits + mi * a.col_wstride;
-        bool any = false;                            // the same answer in every thread
-        for (int cc = 0; cc < CW; ++cc) {
-            const int xx = x0 + cc;
-            if (xx < nx && ((__ldg(cb + (xx >> 5)) >> (xx & 31)) & 1u)) any = true;
-        }
-        if (!any) continue;                          // S there is never read
         const int x = x0 + c;
         const bool on = x < nx;
         const bool colon = on && ((__ldg(cb + (x >> 5)) >> (x & 31)) & 1u);
@@ -670,33 +700,36 @@ k2d_col_lanes(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const flo
             return colon && (a.separable ? ((__ldg(rb + (r >> 5)) >> (r & 31)) & 1u) != 0 : mk[(long long)r * nx + x] != 0);
         };
         auto yprime = [&](int r) { return y[(long long)r * nx + x] * (((r + x) & 1) ? -ysc : ysc); };
-        __syncthreads();                             // tables loaded; the last tile's inverse has read ST and D
         if (mode) {
-            for (int k = threadIdx.x; k < N * (CW / 2); k += CW * TPC) {
-                const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
-                const bool onj = x0 + j < nx;
-                if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
-                    cp_async16(ST + r * CW + j, onj ? S + (long long)r * nx + x0 + j : S, onj ? 16u : 0u);
-            }
-            cp_async_commit();
             cp_async_wait_all();
-            __syncthreads();
-            auto resid = [&](int o, float2 v) {
-                const bool m = sampled(o);
-                ST[o * CW + c] = m ? (v - yprime(o)) * minv : make_float2(0.f, 0.f);
+            __syncthreads();                         // ST holds this tile; the last tile's inverse is done with D, RS
+            // once the forward's first stage has read ST, the next tile's S
+            // copy goes into it, in flight during both transforms
+            auto refill = [&]() {
+                if (un < total) issue(un);
             };
-            lanes_stage<P, -1, CW, TPC, 0, true, NoRefill, decltype(resid)>(D, TWs, RT, nullptr, nx, on, false, 1.f,
-                                                                           c, tc, ST, NoRefill(), resid);
+            float2* RSc = RS + c;
+            auto keep = [RSc](int o, float2 v) { RSc[o * CW] = v; };
+            lanes_stage<P, -1, CW, TPC, 0, true, decltype(refill), decltype(keep)>(D, TWs, RT, nullptr, nx, on, false,
+                                                                                  1.f, c, tc, ST, refill, keep);
+            __syncthreads();
+            // the residual m' (F S - y') in place, each thread on its own column's rows
+            for (int r = tc; r < N; r += TPC)
+                RS[r * CW + c] = sampled(r) ? (RS[r * CW + c] - yprime(r)) * minv : make_float2(0.f, 0.f);
         } else {
-            for (int r = tc; r < N; r += TPC) ST[r * CW + c] = sampled(r) ? yprime(r) * minv : make_float2(0.f, 0.f);
+            __syncthreads();                         // tables loaded; the last tile's inverse has read RS and D
+            for (int r = tc; r < N; r += TPC) RS[r * CW + c] = sampled(r) ? yprime(r) * minv : make_float2(0.f, 0.f);
         }
         __syncthreads();                             // the residual tile is complete
-        auto store = [&](int o, float2 v) {
-            if (on) S[(long long)o * nx + x] = v;
+        float2* Sc = S + (on ? x : 0);
+        auto store = [Sc, on, nx](int o, float2 v) {
+            if (on) Sc[(long long)o * nx] = v;
         };
         lanes_stage<P, +1, CW, TPC, 0, true, NoRefill, decltype(store)>(D, TWs, RT, nullptr, nx, on, false, 1.f, c,
-                                                                       tc, ST, NoRefill(), store);
+                                                                       tc, RS, NoRefill(), store);
+        u = un;
     }
+    cp_async_wait_all();
 }
 
 template <class P, int CW, int TPC>
@@ -705,7 +738,7 @@ static cudaError_t col2d_lanes_k(const Fista2dArgs& a, int mode, cudaStream_t st
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(float2) * ((size_t)2 * P::N * CW + Tw<P>::total() + nrt);
+    const size_t smem = sizeof(float2) * ((size_t)3 * P::N * CW + Tw<P>::total() + nrt);
     const void* fn = reinterpret_cast<const void*>(k2d_col_lanes<P, CW, TPC>);
     if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
     const long long tiles = a.nprob * ((a.nx + CW - 1) / CW);
@@ -720,6 +753,8 @@ template <class P>
 static cudaError_t col2d_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st) {
     if constexpr (big_odd_plan<P>()) {
         if (form == 6) return col2d_lanes_k<P, 8, 16>(a, mode, st);
+        if (form == 7) return col2d_lanes_k<P, 16, 32>(a, mode, st);
+        if (form == 8) return col2d_lanes_k<P, 8, 32>(a, mode, st);
         return col2d_lanes_k<P, 16, 16>(a, mode, st);
     } else {
         switch (form) {

@@ -41,7 +41,7 @@ with Context(0) as ctx:
             want = o64.centred_ifft2(x) if inv else o64.centred_fft2(x)
             if rel(got, want) > 1e-5:
                 out["errors"].append(f"fft2 {n} inv={inv}")
-        for opt, vals in (("xform_tile", (2, 4, 8)), ("xform_lanes", (1, 2, 3, 4) if n != 368 else (5, 6))):
+        for opt, vals in (("xform_tile", (2, 4, 8)), ("xform_lanes", (1, 2, 3, 4) if n != 368 else (5, 6, 7, 8))):
             for v in vals:
                 for pf in ((0, 1) if opt == "xform_lanes" else (0,)):
                     ctx.set_option(opt, v)
@@ -65,7 +65,7 @@ with Context(0) as ctx:
                 out["errors"].append(f"column engine {n} variant {var}")
     forms = [dict(occ2d=1, prefetch2d=1), dict(occ2d=1, prefetch2d=0), dict(occ2d=1, prefetch2d=3),
              dict(occ2d=2, prefetch2d=3), dict(occ2d=0, prefetch2d=0, persist2d=0), dict(occ2d=1, prefetch2d=5),
-             dict(occ2d=0, prefetch2d=4, persist2d=0), dict(col2d_lanes=5), dict(col2d_lanes=6), dict(col2d_lanes=1),
+             dict(occ2d=0, prefetch2d=4, persist2d=0), dict(col2d_lanes=5), dict(col2d_lanes=6), dict(col2d_lanes=7), dict(col2d_lanes=8), dict(col2d_lanes=1),
              dict(col2d_lanes=3)]
     default = dict(occ2d=1, prefetch2d=1, persist2d=1, col2d_lanes=0)
     for ny, nx in ((368, 640), (256, 192), (384, 320), (128, 512)):   # 2-D engine, partial rows

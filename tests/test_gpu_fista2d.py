@@ -130,6 +130,8 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
              dict(mask_bits=1, occ2d=3, persist2d=1, fista2d_streams=2, fista2d_chunk=2, prefetch2d=1),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=5),
              dict(mask_bits=0, occ2d=1, persist2d=1, fista2d_streams=1, fista2d_chunk=3, col2d_lanes=6),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=7),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=3, col2d_lanes=8),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=1),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=4)]
     default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0, prefetch2d=1, col2d_lanes=0)

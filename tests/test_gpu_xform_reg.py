@@ -168,7 +168,7 @@ def test_row_plan_variants(ctx, rng, n, variant):
 
 
 @pytest.mark.parametrize("pf", [0, 1])
-@pytest.mark.parametrize("lanes", [5, 6])
+@pytest.mark.parametrize("lanes", [5, 6, 7, 8])
 def test_column_lanes_368(ctx, rng, lanes, pf):
     """The 368-point lanes forms (16 threads per column, one per radix-23
     butterfly), pipelined and direct, ragged and odd column counts."""
