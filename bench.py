@@ -477,6 +477,39 @@ def fft_stages(ctx, shapes=((368, 640), (256, 256), (320, 320), (384, 384), (512
     return out
 
 
+def prewhiten_stage(ctx, nc=15, ns=1280, target=1 << 30, reps=5):
+    """HBM rate of the prewhitening apply (prewhiten.rs:118-142) on about 1 GiB
+    of raw lines [n][nc][ns] (the precision workload's channel count and
+    oversampled readout length): the bulk-copy staged kernel against the
+    plain-load one, 16 B per sample per channel (read and write in place)."""
+    import torch
+    hbm, kind = peaks()
+    nacq = max(1, target // (nc * ns * 8))
+    d = torch.zeros((nacq, nc, ns), dtype=torch.complex64, device="cuda")
+    w = torch.tril(torch.randn((nc, nc), dtype=torch.complex64, device="cuda", generator=torch.Generator(
+        device="cuda").manual_seed(3)))
+    torch.cuda.synchronize()
+    out = {"peak_gbs": hbm, "peak_kind": kind, "acquisitions": nacq, "channels": nc, "samples": ns,
+           "bytes_model": "16 B per sample per channel"}
+    for bulk, name in ((1, "k_prewhiten_bulk"), (0, "k_prewhiten_apply")):
+        ctx.set_option("prewhiten_bulk", bulk)
+        for _ in range(2):
+            ctx.check(ctx.lib.okscuda_prewhiten_apply(ctx.handle, w.data_ptr(), d.data_ptr(), nacq, nc, ns))
+        ctx.profile(True)
+        for _ in range(reps):
+            ctx.check(ctx.lib.okscuda_prewhiten_apply(ctx.handle, w.data_ptr(), d.data_ptr(), nacq, nc, ns))
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        ms, n = prof[name]
+        gbs = 16.0 * nacq * nc * ns / (ms / n / 1e3) / 1e9
+        out[name] = {"us_per_launch": 1e3 * ms / n, "achieved_gbs": gbs, "frac": gbs / hbm}
+    ctx.set_option("prewhiten_bulk", 1)
+    out["tc_status"] = ctx.tc_status()
+    del d
+    torch.cuda.synchronize()
+    return out
+
+
 WORKLOADS = {"plain": lambda: PlainWorkload(1), "volume": lambda: PlainWorkload(36),
              "precision": lambda: PrecisionWorkload(36), "batched": lambda: BatchedWorkload(64),
              "volume3d": lambda: Volume3dWorkload(),
@@ -1040,6 +1073,7 @@ def main():
         # the FFT stages on their own: row and column passes of the centred
         # 2-D FFT at the configuration's lengths, against the HBM roofline
         line["fft_stages"] = fft_stages(ctx)
+        line["prewhiten_stage"] = prewhiten_stage(ctx)
         # configurations 0, 2 and 4, each a short device + end-to-end measurement
         configs = {}
         pw = PlainWorkload(1)

@@ -109,7 +109,7 @@ const char* okscuda_version(void);
  *   "xform_lanes"   register column transform with the lanes across the
  *                   columns (whole row segments straight from and to global
  *                   memory): 0 (default) for the lengths where it is faster
- *                   (192, 256, 320, 384, 512, 640), 1-4 a (columns, threads per column)
+ *                   (192, 256, 320, 368, 384, 512, 640), 1-4 a (columns, threads per column)
  *                   form (16,32) (16,64) (8,64) (8,32) for every length but 368,
  *                   5-8 the 368 forms (16,16) (8,16) (16,32) (8,32), 16
  *                   threads per column being one per radix-23 butterfly,
@@ -121,6 +121,11 @@ const char* okscuda_version(void);
  *                   tile is copied into shared memory with cp.async while the
  *                   current one is transformed; even nx and 16-byte aligned
  *                   data), 0 = stage 0 reads global memory directly
+ *   "prewhiten_bulk" prewhitening: 1 (default) = tiles of 128 samples of
+ *                   every channel staged in shared memory by bulk copies
+ *                   (cp.async.bulk, two stages) for nc <= 32, even ns and
+ *                   16-byte aligned data, a time-out of its bounded copy
+ *                   waits reported as 9 by okscuda_tc_status; 0 = plain loads
  * Any other name returns OKS_EINVAL. */
 int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value);
 /* Autotuner (no reference counterpart): times the plan and launch-shape

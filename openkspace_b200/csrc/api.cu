@@ -142,6 +142,9 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
     } else if (!std::strcmp(name, "xform_row_variant")) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");
         ctx->xform_row_variant = (int)value;
+    } else if (!std::strcmp(name, "prewhiten_bulk")) {
+        if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "prewhiten_bulk: 0 or 1");
+        ctx->prewhiten_bulk = (int)value;
     } else if (!std::strcmp(name, "xform_lanes_pf")) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "xform_lanes_pf: 0 or 1");
         ctx->xform_lanes_pf = (int)value;

@@ -147,6 +147,24 @@ __global__ void k_chol_inv(const double2* __restrict__ partial, int nparts, int 
 
 // ------------------------------------------------------- prewhiten apply
 // data [nacq][nc][ns]: every sample column s -> W s (lower triangular).
+// One column through W, with its nc samples in registers: out_i =
+// sum_{j <= i} W_ij s_j in j order (prewhiten.rs:126-135).  Both apply
+// kernels call this, so they round identically.
+template <int NCMAX, class LD, class ST>
+__device__ __forceinline__ void whiten_column(const float2* __restrict__ W, int wstride, int nc, LD ld, ST st) {
+    float2 s[NCMAX];
+#pragma unroll
+    for (int j = 0; j < NCMAX; ++j) s[j] = (j < nc) ? ld(j) : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < NCMAX; ++i) {
+        if (i >= nc) break;
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j <= i; ++j) acc = acc + cmul(W[i * wstride + j], s[j]);
+        st(i, acc);
+    }
+}
+
 template <int NCMAX>
 __global__ void k_prewhiten_apply(float2* __restrict__ data, const float2* __restrict__ Wg, long long nacq, int nc,
                                   int ns, const int* __restrict__ status) {
@@ -162,24 +180,170 @@ __global__ void k_prewhiten_apply(float2* __restrict__ data, const float2* __res
         const long long a = t / ns;
         const int n = (int)(t - a * ns);
         float2* col = data + a * nc * (long long)ns + n;
-        float2 s[NCMAX];
-#pragma unroll
-        for (int j = 0; j < NCMAX; ++j) s[j] = (j < nc) ? col[(long long)j * ns] : make_float2(0.f, 0.f);
-#pragma unroll
-        for (int i = 0; i < NCMAX; ++i) {
-            if (i >= nc) break;
-            float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int j = 0; j <= i; ++j) acc = acc + cmul(W[i * NCMAX + j], s[j]);
-            col[(long long)i * ns] = acc;
-        }
+        whiten_column<NCMAX>(
+            W, NCMAX, nc, [&](int j) { return col[(long long)j * ns]; },
+            [&](int i, float2 v) { col[(long long)i * ns] = v; });
     }
 }
 
+// Bulk-copy staged prewhitening.  A CTA of TS threads loops over tiles of
+// (acquisition a, samples [s0, s0 + TS)).  Lane c < nc of warp 0 copies
+// channel c's row segment (8 len contiguous bytes) into a shared stage with
+// cp.async.bulk, completing on the stage's mbarrier; with two stages the next
+// tile's copies are in flight while this one is computed, and they cost no
+// issue slots or registers.  Thread s reads its sample column from the stage,
+// applies W (whiten_column) and writes the result back into the stage; after
+// a proxy fence and a CTA barrier the same lanes store the segments with
+// cp.async.bulk (shared to global).  A stage is refilled only after the lane's
+// own stores from it have been read (cp.async.bulk.wait_group.read).
+// The launcher takes this kernel only for ns even and a 16-byte aligned data
+// pointer: every segment then starts on a 16-byte boundary and is a multiple
+// of 16 bytes long.  Each mbarrier wait is bounded (about one second of clock
+// cycles); on time-out the CTA records 9 in *err, waits (bounded again) for
+// its loads in flight and for its stores, and returns.
+__device__ __forceinline__ uint32_t pw_smem(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ bool pw_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool pw_wait(uint32_t bar, uint32_t parity) {
+    constexpr long long kCycles = 2000000000ll;   // about one second at 1.9 GHz
+    if (pw_try(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!pw_try(bar, parity))
+        if (clock64() - t0 > kCycles) return false;
+    return true;
+}
+
+template <int NCMAX, int TS>
+__global__ void __launch_bounds__(TS) k_prewhiten_bulk(float2* __restrict__ data, const float2* __restrict__ Wg,
+                                                       long long nacq, int nc, int ns, const int* __restrict__ status,
+                                                       int* __restrict__ err) {
+    if (status && *status != 0) return;
+    extern __shared__ __align__(16) float2 pw_sm[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(pw_sm);   // two stage barriers (16 bytes)
+    float2* W = pw_sm + 2;                                 // [nc][nc]
+    float2* stg0 = W + ((nc * nc + 1) & ~1);               // two stages [nc][TS], 16-byte aligned
+    const int tid = threadIdx.x;
+    const bool issuer = tid < nc;                          // nc <= 32: lanes of warp 0
+    for (int q = tid; q < nc * nc; q += TS) W[q] = Wg[q];
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pw_smem(&bars[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pw_smem(&bars[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const long long tiles_per = (ns + TS - 1) / TS;
+    const long long total = nacq * tiles_per;
+    // tile u -> (acquisition, first sample, length); the caller of issue is lane c
+    auto tile_of = [&](long long u, long long& a, int& s0, int& len) {
+        a = u / tiles_per;
+        s0 = (int)(u - a * tiles_per) * TS;
+        len = min(TS, ns - s0);
+    };
+    auto issue_load = [&](long long u, int b) {   // warp 0 only
+        long long a;
+        int s0, len;
+        tile_of(u, a, s0, len);
+        const uint32_t bar = pw_smem(&bars[b]);
+        if (tid == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"((uint32_t)(nc * len * 8))
+                         : "memory");
+        __syncwarp();
+        if (issuer) {
+            // this lane's stores from the stage must have read it first
+            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+            const float2* src = data + (a * nc + tid) * (long long)ns + s0;
+            float2* dst = stg0 + ((size_t)b * nc + tid) * TS;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             pw_smem(dst)),
+                         "l"(src), "r"((uint32_t)(len * 8)), "r"(bar)
+                         : "memory");
+        }
+    };
+    long long u = blockIdx.x;
+    if (tid < 32 && u < total) issue_load(u, 0);
+    uint32_t use0 = 0u, use1 = 0u;   // completed waits per stage: the parity of its next phase
+    int it = 0;
+    for (; u < total; u += gridDim.x, ++it) {
+        const int b = it & 1;
+        const long long un = u + gridDim.x;
+        const bool pending_next = un < total;
+        if (tid < 32 && pending_next) issue_load(un, b ^ 1);
+        const uint32_t par = (b ? use1 : use0) & 1u, par_next = (b ? use0 : use1) & 1u;
+        const bool ok = pw_wait(pw_smem(&bars[b]), par);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(err, 9);
+                pw_wait(pw_smem(&bars[b]), par);                       // copies in flight land first
+                if (pending_next) pw_wait(pw_smem(&bars[b ^ 1]), par_next);
+            }
+            break;
+        }
+        if (b) ++use1;
+        else ++use0;
+        long long a;
+        int s0, len;
+        tile_of(u, a, s0, len);
+        float2* stg = stg0 + (size_t)b * nc * TS;
+        if (tid < len)
+            whiten_column<NCMAX>(
+                W, nc, nc, [&](int j) { return stg[j * TS + tid]; }, [&](int i, float2 v) { stg[i * TS + tid] = v; });
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (issuer) {
+            float2* dst = data + (a * nc + tid) * (long long)ns + s0;
+            asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                         "r"(pw_smem(stg + (size_t)tid * TS)), "r"((uint32_t)(len * 8))
+                         : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+    }
+    if (issuer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");   // stores done before the CTA leaves
+}
+
+bool prewhiten_bulk_eligible(const float2* data, int nc, int ns, const int* err, int bulk) {
+    return bulk && err && nc >= 1 && nc <= 32 && ns > 0 && (ns % 2) == 0 &&
+           (reinterpret_cast<uintptr_t>(data) % 16) == 0;
+}
+
+template <int NCMAX, int TS>
+static cudaError_t launch_bulk(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st,
+                               const int* status, int* err) {
+    const size_t smem = 16 + sizeof(float2) * (size_t)(((nc * nc + 1) & ~1) + 2 * nc * TS);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_prewhiten_bulk<NCMAX, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_prewhiten_bulk<NCMAX, TS>, TS, smem);
+    const long long tiles = nacq * ((ns + TS - 1) / TS);
+    long long blocks = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    if (blocks > tiles) blocks = tiles;
+    k_prewhiten_bulk<NCMAX, TS><<<(unsigned)blocks, TS, smem, st>>>(data, W, nacq, nc, ns, status, err);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st,
-                                   const int* status) {
+                                   const int* status, int* err, int bulk) {
     const long long total = nacq * ns;
     if (total <= 0 || nc <= 0) return cudaSuccess;
+    if (prewhiten_bulk_eligible(data, nc, ns, err, bulk)) {
+        if (nc <= 8) return launch_bulk<8, 128>(data, W, nacq, nc, ns, st, status, err);
+        if (nc <= 16) return launch_bulk<16, 128>(data, W, nacq, nc, ns, st, status, err);
+        return launch_bulk<32, 128>(data, W, nacq, nc, ns, st, status, err);
+    }
     long long blocks = (total + 255) / 256;
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (nc <= 8) k_prewhiten_apply<8><<<(unsigned)blocks, 256, 0, st>>>(data, W, nacq, nc, ns, status);

@@ -575,11 +575,17 @@ static cudaError_t col_lanes_k(const ColXformArgs& a, cudaStream_t st) {
 // threads) choice / direct lanes form / tiles): 192 5074 / 4346 / 3368 (form
 // 4), 256 5065 / 4807 / 4535 (form 4), 320 4528 / 3514 / 3177 (form 1), 384
 // 4581 / 3782 / 4063 (form 3), 512 4805 / 4154 / 4144 (form 1), 640 4078 /
-// 2784 / 3689 (form 2).  The tiles stay at 128 (5043 / 3907 against the direct
-// lanes form) and at 368, whose radix-23 plan has no lanes form.
+// 2784 / 3689 (form 2), 368 4158 / 2750 / 2624 (form 8, (8, 32): 32 threads
+// per column, the radix-23 stage on 16 of them, one butterfly each).  The
+// tiles stay at 128 (5043 / 3907 against the direct lanes form).
 template <class P>
 constexpr int lanes_default() {
-    return (P::N == 192 || P::N == 256) ? 4 : (P::N == 320 || P::N == 512) ? 1 : P::N == 384 ? 3 : P::N == 640 ? 2 : 0;
+    return (P::N == 192 || P::N == 256) ? 4
+           : (P::N == 320 || P::N == 512) ? 1
+           : P::N == 384 ? 3
+           : P::N == 640 ? 2
+           : P::N == 368 ? 8
+                         : 0;
 }
 
 // Columns across the lanes: tile width CW and threads per column TPC
@@ -609,8 +615,8 @@ template <class P>
 static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
     {
         // columns across the lanes (in-problem offsets in 32 bits) where that
-        // form measured faster than the tiles: 192, 256, 320, 384, 512, 640;
-        // 368 takes the forms 5 and 6 (16 threads per column), others 1-4
+        // form measured faster than the tiles: 192, 256, 320, 368, 384, 512,
+        // 640; 368 takes the forms 5-8, the other lengths 1-4
         int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
         if (lanes > 0) {
             if constexpr (big_odd_plan<P>()) lanes = lanes < 5 ? 5 : lanes;   // 5-8

@@ -93,9 +93,14 @@ int okscuda_prewhiten_apply(okscuda_ctx* ctx, const okscuda_c64* d_W, okscuda_c6
     if (!d_W || (!d_data && nacq > 0) || nacq < 0 || nc <= 0 || ns < 0)
         return set_err(ctx, OKS_EINVAL, "prewhiten_apply: bad arguments");
     if (nc > 64) return set_err(ctx, OKS_ENOTSUP, "prewhiten_apply: nc=%d above 64", nc);
-    ProfScope ps(ctx, "k_prewhiten_apply");
+    int rc;
+    if (ctx->prewhiten_bulk && (rc = tc_err_flag(ctx))) return rc;
+    ProfScope ps(ctx, oks::prewhiten_bulk_eligible(reinterpret_cast<float2*>(d_data), nc, ns, ctx->tc_err,
+                                                   ctx->prewhiten_bulk)
+                          ? "k_prewhiten_bulk"
+                          : "k_prewhiten_apply");
     OKS_CUDA(oks::launch_prewhiten_apply(reinterpret_cast<float2*>(d_data), reinterpret_cast<const float2*>(d_W),
-                                         nacq, nc, ns, ctx->stream));
+                                         nacq, nc, ns, ctx->stream, nullptr, ctx->tc_err, ctx->prewhiten_bulk));
     return OKS_OK;
 }
 
@@ -381,9 +386,16 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
         // preprocess: W s (prewhiten.rs:118-124 skips other channel counts), then OS removal
         if (have_w && gnc == w_nc) {
             if (gnc > 64) return set_err(ctx, OKS_ENOTSUP, "prewhiten_apply: nc=%d above 64", gnc);
-            ProfScope ps(ctx, "k_prewhiten_apply");
+            if (ctx->prewhiten_bulk) {
+                const int rc = tc_err_flag(ctx);
+                if (rc) return rc;
+            }
+            ProfScope ps(ctx, oks::prewhiten_bulk_eligible(raw.as<float2>(), gnc, gns, ctx->tc_err,
+                                                           ctx->prewhiten_bulk)
+                                  ? "k_prewhiten_bulk"
+                                  : "k_prewhiten_apply");
             OKS_CUDA(oks::launch_prewhiten_apply(raw.as<float2>(), dW.as<float2>(), ng, gnc, gns, ctx->stream,
-                                                 dWstat.as<int>()));
+                                                 dWstat.as<int>(), ctx->tc_err, ctx->prewhiten_bulk));
         }
         // navigator phasors (phasecorr.rs:141-168), before oversampling removal
         if (!pc_bins.empty()) {
