@@ -503,7 +503,7 @@ def prewhiten_stage(ctx, nc=15, ns=1280, target=1 << 30, reps=5):
         ms, n = prof[name]
         gbs = 16.0 * nacq * nc * ns / (ms / n / 1e3) / 1e9
         out[name] = {"us_per_launch": 1e3 * ms / n, "achieved_gbs": gbs, "frac": gbs / hbm}
-    ctx.set_option("prewhiten_bulk", 1)
+    ctx.set_option("prewhiten_bulk", -1)
     out["tc_status"] = ctx.tc_status()
     del d
     torch.cuda.synchronize()

@@ -87,10 +87,15 @@ const char* okscuda_version(void);
  *                   pass; bit 2 row pass with the next row pair of S, Z~ and
  *                   X~ staged in shared memory by cp.async.bulk (mbarrier
  *                   completion, bounded waits)
- *   "col2d_lanes"   2-D-mask engine column pass: 0 (default) one column pair
- *                   per thread group; 1-6 the lanes form (tiles of 8 or 16
+ *   "col2d_lanes"   2-D-mask engine column pass: 0 (default) by length (form 9
+ *                   at ny = 368, else -1); -1 one column pair
+ *                   per thread group; 1-8 the lanes form (tiles of 8 or 16
  *                   columns in shared memory, lanes across the columns; the
- *                   forms of "xform_lanes", 5-8 for 368)
+ *                   forms of "xform_lanes", 5-8 for 368); 9-12 for ny = 368
+ *                   and separable masks, the lanes form pruned to the
+ *                   sampled rows (radix-23 output pairs and input pairs that
+ *                   only unsampled rows reach are left out), (columns,
+ *                   threads per column) (8,16) (8,32) (16,16) (16,32)
  *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
  *                   least 12 warps resident per SM, 2 = at least 18, 3 = at
  *                   least 15, 0 = registers as needed
@@ -121,11 +126,13 @@ const char* okscuda_version(void);
  *                   tile is copied into shared memory with cp.async while the
  *                   current one is transformed; even nx and 16-byte aligned
  *                   data), 0 = stage 0 reads global memory directly
- *   "prewhiten_bulk" prewhitening: 1 (default) = tiles of 128 samples of
- *                   every channel staged in shared memory by bulk copies
+ *   "prewhiten_bulk" prewhitening: 1 = tiles of 128 samples of every
+ *                   channel staged in shared memory by bulk copies
  *                   (cp.async.bulk, two stages) for nc <= 32, even ns and
  *                   16-byte aligned data, a time-out of its bounded copy
- *                   waits reported as 9 by okscuda_tc_status; 0 = plain loads
+ *                   waits reported as 9 by okscuda_tc_status; 0 = plain
+ *                   loads; -1 (default) = the bulk copies for nc <= 8, plain
+ *                   loads above (the faster of the two on B200)
  * Any other name returns OKS_EINVAL. */
 int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value);
 /* Autotuner (no reference counterpart): times the plan and launch-shape

@@ -137,13 +137,15 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
             return set_err(ctx, OKS_EINVAL, "xform_tile: 0 (by length), 2, 4 or 8 column pairs");
         ctx->xform_tile = (int)value;
     } else if (!std::strcmp(name, "col2d_lanes")) {
-        if (value < 0 || value > 8) return set_err(ctx, OKS_EINVAL, "col2d_lanes: 0 off, 1 to 8 a lanes form");
+        if (value < -1 || value > 12)
+            return set_err(ctx, OKS_EINVAL,
+                           "col2d_lanes: -1 column pairs, 0 by length, 1 to 8 a lanes form, 9 to 12 the pruned 368 forms");
         ctx->col2d_lanes = (int)value;
     } else if (!std::strcmp(name, "xform_row_variant")) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");
         ctx->xform_row_variant = (int)value;
     } else if (!std::strcmp(name, "prewhiten_bulk")) {
-        if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "prewhiten_bulk: 0 or 1");
+        if (value < -1 || value > 1) return set_err(ctx, OKS_EINVAL, "prewhiten_bulk: -1, 0 or 1");
         ctx->prewhiten_bulk = (int)value;
     } else if (!std::strcmp(name, "xform_lanes_pf")) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "xform_lanes_pf: 0 or 1");
@@ -486,7 +488,10 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             a.occ = tp.occ2d;
             a.prefetch = tp.prefetch2d;
             a.err = ctx->tc_err;
-            a.col_lanes = ctx->col2d_lanes;
+            // 0: by length -- the pruned lanes form (8, 16) at ny = 368 (it
+            // takes the iteration passes of separable masks; the rest stay on
+            // the column-pair pass), the column-pair pass elsewhere
+            a.col_lanes = ctx->col2d_lanes > 0 ? ctx->col2d_lanes : (ctx->col2d_lanes == 0 && ny == 368 ? 9 : 0);
             auto col = [&](int mode) {
                 if (col_reg) {
                     ProfScope ps(ctx, "k2d_col_reg", st);

@@ -83,8 +83,8 @@ struct okscuda_ctx {
     int xform_lanes = 0;                  // lanes-across-columns form of it: 0 by length, 1..4, -1 off
     int xform_lanes_pf = 1;               // lanes form: 1 = next tile staged in shared memory while transforming
     int xform_row_variant = 0;            // register row transform: alternative plans for 192 and 320
-    int col2d_lanes = 0;                  // 2-D engine column pass: 0 column pairs, 1-6 the lanes form
-    int prewhiten_bulk = 1;               // prewhitening: 1 bulk-copy staged kernel where eligible, 0 plain loads
+    int col2d_lanes = 0;                  // 2-D engine column pass: 0 by length, -1 column pairs, 1-12 a lanes form
+    int prewhiten_bulk = -1;              // prewhitening: -1 by channel count, 1 bulk-copy staged kernel, 0 plain loads
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)
     cudaEvent_t fork_ev = nullptr;

@@ -23,10 +23,11 @@ cudaError_t launch_noise_fit(const float2* noise, int nc, long long ns, double d
 // status (nullable): device result word of the noise fit; when it is not 0
 // the kernel leaves the data unchanged (no host round trip to decide)
 // err (nullable): the context's device error word.  With err given, ns even
-// and data on a 16-byte boundary, the bulk-copy staged kernel runs (unless
-// bulk is 0); it records 9 in *err if a bounded copy wait runs out.
+// and data on a 16-byte boundary, the bulk-copy staged kernel runs for
+// bulk > 0, or for bulk < 0 and nc <= 8; it records 9 in *err if a bounded
+// copy wait runs out.
 cudaError_t launch_prewhiten_apply(float2* data, const float2* W, long long nacq, int nc, int ns, cudaStream_t st,
-                                   const int* status = nullptr, int* err = nullptr, int bulk = 1);
+                                   const int* status = nullptr, int* err = nullptr, int bulk = -1);
 // true when launch_prewhiten_apply takes the bulk-copy kernel for these arguments
 bool prewhiten_bulk_eligible(const float2* data, int nc, int ns, const int* err, int bulk);
 cudaError_t launch_os_remove(const float2* in, float2* out, long long nlines, const DevPlan& pe, const DevPlan& pr,

@@ -192,15 +192,16 @@ __global__ void k_prewhiten_apply(float2* __restrict__ data, const float2* __res
 // cp.async.bulk, completing on the stage's mbarrier; with two stages the next
 // tile's copies are in flight while this one is computed, and they cost no
 // issue slots or registers.  Thread s reads its sample column from the stage,
-// applies W (whiten_column) and writes the result back into the stage; after
-// a proxy fence and a CTA barrier the same lanes store the segments with
-// cp.async.bulk (shared to global).  A stage is refilled only after the lane's
-// own stores from it have been read (cp.async.bulk.wait_group.read).
+// applies W (whiten_column) and stores the results straight to global memory
+// (consecutive threads, consecutive samples of a channel row); the barrier at
+// the end of the tile frees the stage for the copies issued one tile later.
+// (Staging the results for bulk stores as well measured slower on B200: the
+// refill of a stage then waits for its stores to have been read.)
 // The launcher takes this kernel only for ns even and a 16-byte aligned data
 // pointer: every segment then starts on a 16-byte boundary and is a multiple
 // of 16 bytes long.  Each mbarrier wait is bounded (about one second of clock
 // cycles); on time-out the CTA records 9 in *err, waits (bounded again) for
-// its loads in flight and for its stores, and returns.
+// its loads in flight and returns.
 __device__ __forceinline__ uint32_t pw_smem(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -261,8 +262,6 @@ __global__ void __launch_bounds__(TS) k_prewhiten_bulk(float2* __restrict__ data
                          : "memory");
         __syncwarp();
         if (issuer) {
-            // this lane's stores from the stage must have read it first
-            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
             const float2* src = data + (a * nc + tid) * (long long)ns + s0;
             float2* dst = stg0 + ((size_t)b * nc + tid) * TS;
             asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -295,25 +294,21 @@ __global__ void __launch_bounds__(TS) k_prewhiten_bulk(float2* __restrict__ data
         long long a;
         int s0, len;
         tile_of(u, a, s0, len);
-        float2* stg = stg0 + (size_t)b * nc * TS;
+        const float2* stg = stg0 + (size_t)b * nc * TS;
+        float2* out = data + a * nc * (long long)ns + s0 + tid;
         if (tid < len)
             whiten_column<NCMAX>(
-                W, nc, nc, [&](int j) { return stg[j * TS + tid]; }, [&](int i, float2 v) { stg[i * TS + tid] = v; });
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (issuer) {
-            float2* dst = data + (a * nc + tid) * (long long)ns + s0;
-            asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-                         "r"(pw_smem(stg + (size_t)tid * TS)), "r"((uint32_t)(len * 8))
-                         : "memory");
-            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-        }
+                W, nc, nc, [&](int j) { return stg[j * TS + tid]; },
+                [&](int i, float2 v) { out[(long long)i * ns] = v; });
+        __syncthreads();                                   // stage b read by every thread: free for a refill
     }
-    if (issuer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");   // stores done before the CTA leaves
 }
 
 bool prewhiten_bulk_eligible(const float2* data, int nc, int ns, const int* err, int bulk) {
-    return bulk && err && nc >= 1 && nc <= 32 && ns > 0 && (ns % 2) == 0 &&
+    // bulk < 0 (the default): by channel count, the bulk copies for nc <= 8,
+    // where they measured faster on B200 than the plain loads (at 15 and 32
+    // channels the plain kernel was faster)
+    return (bulk > 0 || (bulk < 0 && nc <= 8)) && err && nc >= 1 && nc <= 32 && ns > 0 && (ns % 2) == 0 &&
            (reinterpret_cast<uintptr_t>(data) % 16) == 0;
 }
 

@@ -817,7 +817,11 @@ static cudaError_t launch_2d(const Fista2dArgs& a, long long units, cudaStream_t
 template <class P>
 static cudaError_t col2d(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st) {
     (void)tabs;
-    if (a.col_lanes > 0 && (a.nx % 2) == 0 && (reinterpret_cast<uintptr_t>(a.S) & 15) == 0)
+    // the pruned 368 forms (9-12) take the iteration passes of separable
+    // masks; the init pass and other masks stay on the register pass
+    const bool pruned = a.col_lanes >= 9;
+    if (a.col_lanes > 0 && (a.nx % 2) == 0 && (reinterpret_cast<uintptr_t>(a.S) & 15) == 0 &&
+        (!pruned || (mode == 1 && a.separable && a.ny == 368)))
         return launch_fista2d_col_lanes(a, a.col_lanes, mode, st);
     return launch_2d<P>(a, a.nprob * (a.nx / 2), st, mode, 0, false);
 }

@@ -772,11 +772,350 @@ static cudaError_t col2d_lanes(const Fista2dArgs& a, int form, int mode, cudaStr
     }
 }
 
+
+// 2-D-mask engine, column pass at ny = 368 for separable masks, pruned to
+// the sampled rows (forms 9-12).  The plan is 368 = 4 · 23 · 4 (Stockham,
+// the inverse in reversed order).  With need[i] = "one of the rows i,
+// i + 92, i + 184, i + 276 is sampled" (i < 92):
+//  - forward: output o = ob + 4 j of radix-23 butterfly b (k = b mod 4) is
+//    read only by last-stage butterfly o mod 92 = k + 4 j, whose outputs are
+//    exactly those four rows.  Output pairs (j, 23 - j) with need[k + 4 j]
+//    and need[k + 92 - 4 j] both clear are not formed, and the last stage
+//    skips the butterflies i with need[i] clear (their rows are unsampled:
+//    the residual there is zero and is written by the inverse's first stage);
+//  - inverse: the residual is zero off the sampled rows, so first-stage
+//    butterfly i has only zero inputs when need[i] is clear (it writes
+//    zeros), and input pair (j, 23 - j) of radix-23 butterfly b is zero when
+//    need[b/4 + 4 j] and need[b/4 + 92 - 4 j] are clear: its fold and its
+//    terms are left out (each would add an exact zero).
+// Both tests depend on the butterfly only through its class (b mod 4
+// forward, b / 4 inverse).  The forward maps thread tc < 16 to butterfly
+// 4 (tc mod 4) + tc / 4 and the inverse to butterfly tc, so in both the
+// class is tc / 4 and every warp's branches are uniform.  Tiles of CW
+// columns with the lanes across the columns as in k2d_col_lanes; the S tile
+// of the next unit is staged by 16-byte cp.async into ST once the forward's
+// first stage has read it; D holds every stage in place.  Same arithmetic
+// per formed output as the full transform.
+template <int CW, int SIGN, int Q>
+__device__ __forceinline__ void p368_pairs_fwd(const float2* fa, const float2* fb, float2 x0, float2* D, int ob,
+                                               int c, uint32_t pm) {
+    if constexpr (Q <= 11) {
+        if ((pm >> Q) & 1u) {
+            float2 re = x0, im = make_float2(0.f, 0.f);
+            odd_acc<23, Q, 1>(fa, fb, re, im);
+            const float2 si = mul_si<SIGN>(im);
+            D[(ob + 4 * Q) * CW + c] = re + si;
+            D[(ob + 4 * (23 - Q)) * CW + c] = re - si;
+        }
+        p368_pairs_fwd<CW, SIGN, Q + 1>(fa, fb, x0, D, ob, c, pm);
+    }
+}
+// re += sum a_j cos(2 pi j Q / 23), im += sum b_j sin(...), over the j with pm bit j
+template <int Q, int J>
+__device__ __forceinline__ void p368_acc_masked(const float2* a, const float2* b, float2& re, float2& im,
+                                                uint32_t pm) {
+    if constexpr (J <= 11) {
+        if ((pm >> J) & 1u) {
+            constexpr int M = (J * Q) % 23;
+            re.x = fmaf(a[J - 1].x, RootRM<23, M>::c, re.x);
+            re.y = fmaf(a[J - 1].y, RootRM<23, M>::c, re.y);
+            im.x = fmaf(b[J - 1].x, RootRM<23, M>::s, im.x);
+            im.y = fmaf(b[J - 1].y, RootRM<23, M>::s, im.y);
+        }
+        p368_acc_masked<Q, J + 1>(a, b, re, im, pm);
+    }
+}
+template <int CW, int SIGN, int Q>
+__device__ __forceinline__ void p368_pairs_inv(const float2* fa, const float2* fb, float2 x0, float2* D, int ob,
+                                               int c, uint32_t pm) {
+    if constexpr (Q <= 11) {
+        float2 re = x0, im = make_float2(0.f, 0.f);
+        p368_acc_masked<Q, 1>(fa, fb, re, im, pm);
+        const float2 si = mul_si<SIGN>(im);
+        D[(ob + 4 * Q) * CW + c] = re + si;
+        D[(ob + 4 * (23 - Q)) * CW + c] = re - si;
+        p368_pairs_inv<CW, SIGN, Q + 1>(fa, fb, x0, D, ob, c, pm);
+    }
+}
+
+template <int CW, int TPC>
+__global__ void __launch_bounds__(CW * TPC, 512 / (CW * TPC) > 0 ? 512 / (CW * TPC) : 1)   // 128 registers
+k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
+    using P = S368;
+    constexpr int N = 368, NB4 = 92, H = 11;
+    constexpr int BPT = (NB4 + TPC - 1) / TPC;   // radix-4 butterflies per thread
+    static_assert(TPC >= 16 && CW * TPC >= 96, "16 radix-23 butterflies; 3 warps build the need bits");
+    constexpr int F1 = Tw<P>::fwd(1), F2 = Tw<P>::fwd(2), I1 = Tw<P>::inv(1), I2 = Tw<P>::inv(2);
+    extern __shared__ __align__(16) float2 sm[];
+    float2* D = sm;                                           // [N][CW] every stage, in place
+    float2* ST = sm + N * CW;                                 // [N][CW] staged S tile
+    float2* TWs = ST + N * CW;                                // both directions' twiddles
+    uint32_t* NEED = reinterpret_cast<uint32_t*>(TWs + Tw<P>::total());   // 3 words: need[0..92)
+    for (int q = threadIdx.x; q < Tw<P>::total(); q += blockDim.x) TWs[q] = gtw[q];
+    const int tid = threadIdx.x, c = tid % CW, tc = tid / CW, lane = tid & 31;
+    const int cls = (tc >> 2) & 3;                            // this thread's radix-23 class (tc < 16)
+    const int nx = a.nx;
+    const int ntx = (nx + CW - 1) / CW;
+    const long long total = a.nprob * ntx;
+    const float minv = a.minv, ysc = a.ysc;
+    auto has_sample = [&](long long u) {
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const uint32_t* cb = a.colbits + ((p + a.mask_offset) % a.mask_mod) * a.col_wstride;
+        for (int cc = 0; cc < CW; ++cc) {
+            const int xx = x0 + cc;
+            if (xx < nx && ((__ldg(cb + (xx >> 5)) >> (xx & 31)) & 1u)) return true;
+        }
+        return false;
+    };
+    auto next_tile = [&](long long u) {
+        for (; u < total; u += gridDim.x)
+            if (has_sample(u)) break;
+        return u;
+    };
+    auto issue = [&](long long u) {
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const float2* S = a.S + p * a.st_stride;
+        for (int k = tid; k < N * (CW / 2); k += CW * TPC) {
+            const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+            const bool onj = x0 + j < nx;
+            if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                cp_async16(ST + r * CW + j, onj ? S + (long long)r * nx + x0 + j : S, onj ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    auto need = [&](int i) { return (NEED[i >> 5] >> (i & 31)) & 1u; };
+    long long u = next_tile(blockIdx.x);
+    if (u < total) issue(u);
+    while (u < total) {
+        const long long un = next_tile(u + gridDim.x);
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const long long mi = (p + a.mask_offset) % a.mask_mod;
+        const uint32_t* rb = a.rowbits + mi * a.row_wstride;
+        const int x = x0 + c;
+        const bool on = x < nx;
+        const bool colon = on && ((__ldg(a.colbits + mi * a.col_wstride + (x >> 5)) >> (x & 31)) & 1u);
+        auto rowbit = [&](int r) { return (__ldg(rb + (r >> 5)) >> (r & 31)) & 1u; };
+        cp_async_wait_all();
+        __syncthreads();                                      // ST holds this tile; the last tile is done with D, NEED
+        if (tid < 96) {
+            const int i = tid;
+            const bool bit = i < NB4 && (rowbit(i) | rowbit(i + 92) | rowbit(i + 184) | rowbit(i + 276));
+            const uint32_t w = __ballot_sync(0xffffffffu, bit);
+            if (lane == 0) NEED[tid >> 5] = w;
+        }
+        // forward stage 0 (radix 4, p = 1): inputs b + 92 j from ST
+        float2 v[BPT][4];
+#pragma unroll
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (NB4 % TPC != 0 && b >= NB4) break;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int r = b + NB4 * j;
+                v[bb][j] = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? ST[r * CW + c] : make_float2(0.f, 0.f);
+            }
+        }
+        __syncthreads();                                      // ST read by every thread; NEED complete
+        if (un < total) issue(un);                            // in flight during both transforms
+        // pair masks of this thread's class (bit 0: the DC input / output)
+        uint32_t pm;
+        {
+            const int q = lane < 12 ? lane : 0;
+            const bool bit = lane < 12 && (q == 0 ? need(cls) : (need(cls + 4 * q) | need(cls + 92 - 4 * q)));
+            pm = __ballot_sync(0xffffffffu, bit);
+        }
+#pragma unroll
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (NB4 % TPC != 0 && b >= NB4) break;
+            bfly4<-1>(v[bb]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (OKS_IN((4 * b + j) * CW + c, N * CW, OKS_B_TILE)) D[(4 * b + j) * CW + c] = v[bb][j];
+        }
+        __syncthreads();
+        // forward stage 1 (radix 23, p = 4): butterfly 4 (tc mod 4) + tc / 4
+        {
+            float2 x0v = make_float2(0.f, 0.f), fa[H], fb[H];
+            int ob = 0;
+            const bool act = tc < 16;
+            if (act) {
+                const int b = 4 * (tc & 3) + (tc >> 2), k = b & 3;
+                ob = (b - k) * 23 + k;
+                x0v = D[b * CW + c];
+#pragma unroll
+                for (int j = 1; j <= H; ++j) {
+                    const float2 uu = twmul<-1>(D[(b + 16 * j) * CW + c], TWs[F1 + k * 22 + j - 1]);
+                    const float2 ww = twmul<-1>(D[(b + 16 * (23 - j)) * CW + c], TWs[F1 + k * 22 + 22 - j]);
+                    fa[j - 1] = uu + ww;
+                    fb[j - 1] = uu - ww;
+                }
+            }
+            __syncthreads();                                  // in place: every input read
+            if (act && OKS_IN((ob + 88) * CW + c, N * CW, OKS_B_TILE)) {
+                if (pm & 1u) {
+                    float2 y0 = x0v;
+#pragma unroll
+                    for (int j = 0; j < H; ++j) y0 = y0 + fa[j];
+                    D[ob * CW + c] = y0;
+                }
+                p368_pairs_fwd<CW, -1, 1>(fa, fb, x0v, D, ob, c, pm);
+            }
+        }
+        __syncthreads();
+        // forward stage 2 (radix 4, p = 92) and the residual m' (F S - y'),
+        // each butterfly in place on its own four rows
+        {
+            const float2* y = a.y + p * a.y_stride;
+#pragma unroll
+            for (int bb = 0; bb < BPT; ++bb) {
+                const int b = tc + TPC * bb;
+                if (NB4 % TPC != 0 && b >= NB4) break;
+                if (!need(b)) continue;
+                float2 yv[4];
+                bool sm4[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int r = b + NB4 * j;
+                    sm4[j] = colon && rowbit(r);
+                    yv[j] = sm4[j] ? y[(long long)r * nx + x] * (((r + x) & 1) ? -ysc : ysc) : make_float2(0.f, 0.f);
+                }
+                float2 w4[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int r = b + NB4 * j;
+                    float2 t = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? D[r * CW + c] : make_float2(0.f, 0.f);
+                    if (j > 0) t = twmul<-1>(t, TWs[F2 + b * 3 + j - 1]);
+                    w4[j] = t;
+                }
+                bfly4<-1>(w4);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int r = b + NB4 * j;
+                    if (OKS_IN(r * CW + c, N * CW, OKS_B_TILE))
+                        D[r * CW + c] = sm4[j] ? (w4[j] - yv[j]) * minv : make_float2(0.f, 0.f);
+                }
+            }
+        }
+        __syncthreads();
+        // inverse stage 0 (radix 4, p = 1): inputs b + 92 j, outputs 4 b + j
+#pragma unroll
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (NB4 % TPC != 0 && b >= NB4) break;
+            const bool nz = need(b) != 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int r = b + NB4 * j;
+                v[bb][j] = (nz && OKS_IN(r * CW + c, N * CW, OKS_B_TILE)) ? D[r * CW + c] : make_float2(0.f, 0.f);
+            }
+        }
+        __syncthreads();                                      // in place: every input read
+#pragma unroll
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (NB4 % TPC != 0 && b >= NB4) break;
+            if (need(b)) bfly4<+1>(v[bb]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (OKS_IN((4 * b + j) * CW + c, N * CW, OKS_B_TILE)) D[(4 * b + j) * CW + c] = v[bb][j];
+        }
+        __syncthreads();
+        // inverse stage 1 (radix 23, p = 4): butterfly tc, zero input pairs left out
+        {
+            float2 x0v = make_float2(0.f, 0.f), fa[H], fb[H];
+            int ob = 0;
+            const bool act = tc < 16;
+            if (act) {
+                const int b = tc, k = b & 3;
+                ob = (b - k) * 23 + k;
+                x0v = D[b * CW + c];
+#pragma unroll
+                for (int j = 1; j <= H; ++j) {
+                    if ((pm >> j) & 1u) {
+                        const float2 uu = twmul<+1>(D[(b + 16 * j) * CW + c], TWs[I1 + k * 22 + j - 1]);
+                        const float2 ww = twmul<+1>(D[(b + 16 * (23 - j)) * CW + c], TWs[I1 + k * 22 + 22 - j]);
+                        fa[j - 1] = uu + ww;
+                        fb[j - 1] = uu - ww;
+                    } else {
+                        fa[j - 1] = make_float2(0.f, 0.f);
+                        fb[j - 1] = make_float2(0.f, 0.f);
+                    }
+                }
+            }
+            __syncthreads();                                  // in place: every input read
+            if (act && OKS_IN((ob + 88) * CW + c, N * CW, OKS_B_TILE)) {
+                float2 y0 = x0v;
+#pragma unroll
+                for (int j = 1; j <= H; ++j)
+                    if ((pm >> j) & 1u) y0 = y0 + fa[j - 1];
+                D[ob * CW + c] = y0;
+                p368_pairs_inv<CW, +1, 1>(fa, fb, x0v, D, ob, c, pm);
+            }
+        }
+        __syncthreads();
+        // inverse stage 2 (radix 4, p = 92): rows b + 92 j of S
+        {
+            float2* Sc = a.S + p * a.st_stride + (on ? x : 0);
+#pragma unroll
+            for (int bb = 0; bb < BPT; ++bb) {
+                const int b = tc + TPC * bb;
+                if (NB4 % TPC != 0 && b >= NB4) break;
+                float2 w4[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int r = b + NB4 * j;
+                    float2 t = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? D[r * CW + c] : make_float2(0.f, 0.f);
+                    if (j > 0) t = twmul<+1>(t, TWs[I2 + b * 3 + j - 1]);
+                    w4[j] = t;
+                }
+                bfly4<+1>(w4);
+                if (on) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) Sc[(long long)(b + NB4 * j) * nx] = w4[j];
+                }
+            }
+        }
+        u = un;
+    }
+    cp_async_wait_all();
+}
+
+template <int CW, int TPC>
+static cudaError_t col2d_p368_k(const Fista2dArgs& a, cudaStream_t st) {
+    using P = S368;
+    const float2 *tw, *rt;
+    int nrt;
+    cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)2 * P::N * CW + Tw<P>::total()) + 4 * sizeof(uint32_t);
+    const void* fn = reinterpret_cast<const void*>(k2d_col_p368<CW, TPC>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = a.nprob * ((a.nx + CW - 1) / CW);
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, CW * TPC, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    k2d_col_p368<CW, TPC><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw);
+    return cudaGetLastError();
+}
 }  // namespace reg
 
 cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st) {
     if (a.nprob <= 0) return cudaSuccess;
     if (a.nx % 2 || (reinterpret_cast<uintptr_t>(a.S) & 15)) return cudaErrorInvalidValue;
+    if (form >= 9) {
+        // the pruned 368 forms: separable masks, the iteration pass (mode 1)
+        if (a.ny != 368 || !a.separable || mode != 1) return cudaErrorInvalidValue;
+        switch (form) {
+            case 10: return reg::col2d_p368_k<8, 32>(a, st);
+            case 11: return reg::col2d_p368_k<16, 16>(a, st);
+            case 12: return reg::col2d_p368_k<16, 32>(a, st);
+            default: return reg::col2d_p368_k<8, 16>(a, st);
+        }
+    }
     switch (a.ny) {
         case 128: return reg::col2d_lanes<reg::S128>(a, form, mode, st);
         case 192: return reg::col2d_lanes<reg::S192>(a, form, mode, st);

@@ -189,7 +189,8 @@ struct Fista2dArgs {
                               // pass (separable masks), bit 1 row pass; bit 2 row pass with
                               // bulk-copy (cp.async.bulk) staging of S, Z~, X~
     int* err;                 // bounded-wait error word (bulk-copy row pass), may be null
-    int col_lanes;            // column pass in the lanes form: 0 off, else the form (1-6)
+    int col_lanes;            // column pass in the lanes form: 0 off, else the form (1-8); 9-12
+                              // the pruned 368 forms (separable masks, iteration passes)
 };
 cudaError_t launch_fista2d_col(const Fista2dArgs& a, const DevPlan& py, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_row(const Fista2dArgs& a, const DevPlan& px, int mode, int it, cudaStream_t st);
@@ -199,7 +200,9 @@ bool fista2d_reg_supported(int n);
 cudaError_t launch_fista2d_col_reg(const Fista2dArgs& a, RegTables& tabs, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_row_reg(const Fista2dArgs& a, RegTables& tabs, int mode, int it, cudaStream_t st);
 // Column pass in the lanes form (k_xform_reg.cu): form 1-4 (16,32) (16,64)
-// (8,64) (8,32) columns x threads per column, 5-6 the 368 forms (16,16) (8,16).
+// (8,64) (8,32) columns x threads per column, 5-8 the 368 forms (16,16) (8,16)
+// (16,32) (8,32); 9-12 the 368 forms pruned to the sampled rows, (8,16) (8,32)
+// (16,16) (16,32), for separable masks and mode 1 only.
 cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_demod(const float2* X, float2* out, long long nprob, int ny, int nx, long long in_stride,
                                  long long out_stride, cudaStream_t st);

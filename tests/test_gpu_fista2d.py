@@ -133,7 +133,12 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=7),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=3, col2d_lanes=8),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=1),
-             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=4)]
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=4),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=-1),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=9),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=3, col2d_lanes=10),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=1, fista2d_chunk=2, col2d_lanes=11),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=12)]
     default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0, prefetch2d=1, col2d_lanes=0)
     results = []
     try:
@@ -151,6 +156,65 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
     mr = ragged_row_mask(rng, ny, nx)
     kr = np.where(mr[None], crandn(rng, (2, ny, nx)), 0).astype(np.complex64)
     assert rel_l2(ctx.fista_cs(kr, mr, iters, 0.02), o64.fista_cs_single_coil(kr, mr, iters, 0.02)) < TOL_CS
+
+
+def row_set_mask(ny, nx, rows):
+    """Separable mask: the given ky rows over the central half of kx."""
+    m = np.zeros((ny, nx), bool)
+    m[np.asarray(rows, int), nx // 4:nx // 4 + nx // 2] = True
+    return m
+
+
+@pytest.mark.parametrize("rows", ["r4_centre", "r4_offset", "r3", "random20", "one_row", "all", "class_edge"])
+@pytest.mark.parametrize("form", [9, 10, 11, 12])
+def test_pruned_368_column_pass(ctx, rng, rows, form):
+    """The 368 column pass pruned to the sampled rows (col2d_lanes 9-12)
+    against the full register pass and FP64, for row sets that exercise
+    every pruning case: R = 4 plus a centre block (the precision workload's
+    pattern, dense class and sparse classes), R = 4 shifted by one row, R = 3
+    (every class partly sampled), random rows, a single row (one need bit),
+    every row (nothing pruned), and rows at the ends of the 92-row blocks."""
+    ny, nx, iters = 368, 96, 6
+    rset = {"r4_centre": list(range(0, ny, 4)) + list(range(ny // 2 - 15, ny // 2 + 15)),
+            "r4_offset": list(range(1, ny, 4)) + [ny // 2],
+            "r3": list(range(2, ny, 3)),
+            "random20": list(np.flatnonzero(rng.random(ny) < 0.2)) + [ny // 2],
+            "one_row": [ny // 2 + 5],
+            "all": list(range(ny)),
+            "class_edge": [0, 91, 92, 183, 276, 367, 3, 95]}[rows]
+    m = row_set_mask(ny, nx, sorted(set(rset)))
+    k = np.where(m[None], crandn(rng, (3, ny, nx)), 0).astype(np.complex64)
+    ctx.set_option("col2d_lanes", -1)
+    base = ctx.fista_cs(k, m, iters, 0.02)
+    ctx.set_option("col2d_lanes", form)
+    try:
+        got = ctx.fista_cs(k, m, iters, 0.02)
+    finally:
+        ctx.set_option("col2d_lanes", 0)
+    assert rel_l2(got, base) < 1e-5
+    assert rel_l2(got, o64.fista_cs_single_coil(k, m, iters, 0.02)) < TOL_CS
+
+
+def test_pruned_368_column_pass_full_width(ctx, rng):
+    """The precision workload's grid (368 x 640, R = 4 plus 8 % centre over
+    the central half of kx) through the pruned form (the default at ny = 368)
+    against the column-pair pass, with the CUDA graph
+    (second call of a shape) and two chunks in flight, for two row offsets."""
+    ny, nx, iters = 368, 640, 5
+    for off in (0, 2):
+        rows = sorted(set(range(off, ny, 4)) | set(range(ny // 2 - 15, ny // 2 + 15)))
+        m = row_set_mask(ny, nx, rows)
+        k = np.where(m[None], crandn(rng, (5, ny, nx)), 0).astype(np.complex64)
+        ctx.set_option("col2d_lanes", -1)
+        base = ctx.fista_cs(k, m, iters, 0.02)
+        ctx.set_option("col2d_lanes", 0)
+        try:
+            got = [ctx.fista_cs(k, m, iters, 0.02) for _ in range(3)]   # direct, captured, replayed
+        finally:
+            ctx.set_option("col2d_lanes", 0)
+        for g in got:
+            assert rel_l2(g, base) < 1e-5
+        assert rel_l2(got[-1], o64.fista_cs_single_coil(k, m, iters, 0.02)) < TOL_CS
 
 
 def test_graph_replay_matches_direct_launches(ctx, rng):

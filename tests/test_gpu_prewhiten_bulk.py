@@ -1,5 +1,5 @@
 """Prewhitening apply (prewhiten.rs:118-142) through the bulk-copy staged
-kernel (option prewhiten_bulk = 1, the default) against the plain-load kernel
+kernel (option prewhiten_bulk = 1; the default -1 takes it for nc <= 8) against the plain-load kernel
 (prewhiten_bulk = 0) and the FP64 oracle.  Both kernels share the per-column
 arithmetic, so their outputs must be bit-identical; against the oracle the
 tolerance is 1e-5 relative L2.  The shapes cover ragged last tiles (ns not a
@@ -34,7 +34,7 @@ def apply(ctx, w, data, bulk, offset=0):
     try:
         ctx.check(ctx.lib.okscuda_prewhiten_apply(ctx.handle, dw.ptr, d.ptr + 8 * offset, nacq, nc, ns))
     finally:
-        ctx.set_option("prewhiten_bulk", 1)
+        ctx.set_option("prewhiten_bulk", -1)
     return d.to_host()[offset:].reshape(data.shape)
 
 
