@@ -95,7 +95,8 @@ const char* okscuda_version(void);
  *                   and separable masks, the lanes form pruned to the
  *                   sampled rows (radix-23 output pairs and input pairs that
  *                   only unsampled rows reach are left out), (columns,
- *                   threads per column) (8,16) (8,32) (16,16) (16,32)
+ *                   threads per column) (8,16) (8,32) (16,16) (16,32); 13 =
+ *                   (8,16) with the row slots swizzled against bank conflicts
  *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
  *                   least 12 warps resident per SM, 2 = at least 18, 3 = at
  *                   least 15, 0 = registers as needed

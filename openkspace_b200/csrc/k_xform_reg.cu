@@ -796,7 +796,18 @@ static cudaError_t col2d_lanes(const Fista2dArgs& a, int form, int mode, cudaStr
 // of the next unit is staged by 16-byte cp.async into ST once the forward's
 // first stage has read it; D holds every stage in place.  Same arithmetic
 // per formed output as the full transform.
-template <int CW, int SIGN, int Q>
+// D row slot of row r in k2d_col_p368.  SW (form 13): rows r and r ^ 1 trade
+// places when bit 2 of r is set, so the strided row sets of the stages fall on
+// both halves of the banks (a permutation inside each row pair: the slots stay
+// in [0, N)).  On B200 it removed 84 % of the shared-memory bank conflicts but
+// added 16 % instructions; the forms 9-12 keep the rows in order.
+template <bool SW>
+__device__ __forceinline__ int p368_slot(int r) {
+    if constexpr (SW) return r ^ ((r >> 2) & 1);
+    else return r;
+}
+
+template <int CW, bool SW, int SIGN, int Q>
 __device__ __forceinline__ void p368_pairs_fwd(const float2* fa, const float2* fb, float2 x0, float2* D, int ob,
                                                int c, uint32_t pm) {
     if constexpr (Q <= 11) {
@@ -804,10 +815,10 @@ __device__ __forceinline__ void p368_pairs_fwd(const float2* fa, const float2* f
             float2 re = x0, im = make_float2(0.f, 0.f);
             odd_acc<23, Q, 1>(fa, fb, re, im);
             const float2 si = mul_si<SIGN>(im);
-            D[(ob + 4 * Q) * CW + c] = re + si;
-            D[(ob + 4 * (23 - Q)) * CW + c] = re - si;
+            D[p368_slot<SW>(ob + 4 * Q) * CW + c] = re + si;
+            D[p368_slot<SW>(ob + 4 * (23 - Q)) * CW + c] = re - si;
         }
-        p368_pairs_fwd<CW, SIGN, Q + 1>(fa, fb, x0, D, ob, c, pm);
+        p368_pairs_fwd<CW, SW, SIGN, Q + 1>(fa, fb, x0, D, ob, c, pm);
     }
 }
 // re += sum a_j cos(2 pi j Q / 23), im += sum b_j sin(...), over the j with pm bit j
@@ -825,32 +836,34 @@ __device__ __forceinline__ void p368_acc_masked(const float2* a, const float2* b
         p368_acc_masked<Q, J + 1>(a, b, re, im, pm);
     }
 }
-template <int CW, int SIGN, int Q>
+template <int CW, bool SW, int SIGN, int Q>
 __device__ __forceinline__ void p368_pairs_inv(const float2* fa, const float2* fb, float2 x0, float2* D, int ob,
                                                int c, uint32_t pm) {
     if constexpr (Q <= 11) {
         float2 re = x0, im = make_float2(0.f, 0.f);
         p368_acc_masked<Q, 1>(fa, fb, re, im, pm);
         const float2 si = mul_si<SIGN>(im);
-        D[(ob + 4 * Q) * CW + c] = re + si;
-        D[(ob + 4 * (23 - Q)) * CW + c] = re - si;
-        p368_pairs_inv<CW, SIGN, Q + 1>(fa, fb, x0, D, ob, c, pm);
+        D[p368_slot<SW>(ob + 4 * Q) * CW + c] = re + si;
+        D[p368_slot<SW>(ob + 4 * (23 - Q)) * CW + c] = re - si;
+        p368_pairs_inv<CW, SW, SIGN, Q + 1>(fa, fb, x0, D, ob, c, pm);
     }
 }
 
-template <int CW, int TPC>
+template <int CW, int TPC, bool SW>
 __global__ void __launch_bounds__(CW * TPC, 512 / (CW * TPC) > 0 ? 512 / (CW * TPC) : 1)   // 128 registers
 k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
     using P = S368;
     constexpr int N = 368, NB4 = 92, H = 11;
     constexpr int BPT = (NB4 + TPC - 1) / TPC;   // radix-4 butterflies per thread
-    static_assert(TPC >= 16 && CW * TPC >= 96, "16 radix-23 butterflies; 3 warps build the need bits");
+    static_assert(TPC >= 16 && CW * TPC >= 108, "16 radix-23 butterflies; 3 warps build the need bits");
+    static_assert(CW % 2 == 0, "16-byte copies of column pairs");
     constexpr int F1 = Tw<P>::fwd(1), F2 = Tw<P>::fwd(2), I1 = Tw<P>::inv(1), I2 = Tw<P>::inv(2);
     extern __shared__ __align__(16) float2 sm[];
-    float2* D = sm;                                           // [N][CW] every stage, in place
-    float2* ST = sm + N * CW;                                 // [N][CW] staged S tile
+    float2* D = sm;                                           // [N][CW] every stage, in place (row slots swizzled)
+    float2* ST = sm + N * CW;                                 // [N][CW] S tile, then y' on the sampled rows
     float2* TWs = ST + N * CW;                                // both directions' twiddles
     uint32_t* NEED = reinterpret_cast<uint32_t*>(TWs + Tw<P>::total());   // 3 words: need[0..92)
+    uint32_t* ROWS = NEED + 4;                                // 12 words: the tile's sampled rows
     for (int q = threadIdx.x; q < Tw<P>::total(); q += blockDim.x) TWs[q] = gtw[q];
     const int tid = threadIdx.x, c = tid % CW, tc = tid / CW, lane = tid & 31;
     const int cls = (tc >> 2) & 3;                            // this thread's radix-23 class (tc < 16)
@@ -858,6 +871,7 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
     const int ntx = (nx + CW - 1) / CW;
     const long long total = a.nprob * ntx;
     const float minv = a.minv, ysc = a.ysc;
+    auto dr = [](int r) { return p368_slot<SW>(r) * CW; };
     auto has_sample = [&](long long u) {
         const long long p = u / ntx;
         const int x0 = (int)(u - p * ntx) * CW;
@@ -873,7 +887,8 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
             if (has_sample(u)) break;
         return u;
     };
-    auto issue = [&](long long u) {
+    // the S tile of unit u into ST: whole row segments, 16-byte cp.async
+    auto issue_s = [&](long long u) {
         const long long p = u / ntx;
         const int x0 = (int)(u - p * ntx) * CW;
         const float2* S = a.S + p * a.st_stride;
@@ -886,8 +901,9 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
         cp_async_commit();
     };
     auto need = [&](int i) { return (NEED[i >> 5] >> (i & 31)) & 1u; };
+    auto rowbit = [&](int r) { return (ROWS[r >> 5] >> (r & 31)) & 1u; };
     long long u = next_tile(blockIdx.x);
-    if (u < total) issue(u);
+    if (u < total) issue_s(u);
     while (u < total) {
         const long long un = next_tile(u + gridDim.x);
         const long long p = u / ntx;
@@ -897,14 +913,16 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
         const int x = x0 + c;
         const bool on = x < nx;
         const bool colon = on && ((__ldg(a.colbits + mi * a.col_wstride + (x >> 5)) >> (x & 31)) & 1u);
-        auto rowbit = [&](int r) { return (__ldg(rb + (r >> 5)) >> (r & 31)) & 1u; };
         cp_async_wait_all();
-        __syncthreads();                                      // ST holds this tile; the last tile is done with D, NEED
+        __syncthreads();                                      // ST holds this tile; the last tile is done with D, NEED, ROWS
         if (tid < 96) {
             const int i = tid;
-            const bool bit = i < NB4 && (rowbit(i) | rowbit(i + 92) | rowbit(i + 184) | rowbit(i + 276));
+            auto rbit = [&](int r) { return (__ldg(rb + (r >> 5)) >> (r & 31)) & 1u; };
+            const bool bit = i < NB4 && (rbit(i) | rbit(i + 92) | rbit(i + 184) | rbit(i + 276));
             const uint32_t w = __ballot_sync(0xffffffffu, bit);
             if (lane == 0) NEED[tid >> 5] = w;
+        } else if (tid < 108) {
+            ROWS[tid - 96] = __ldg(rb + (tid - 96));
         }
         // forward stage 0 (radix 4, p = 1): inputs b + 92 j from ST
         float2 v[BPT][4];
@@ -918,8 +936,7 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
                 v[bb][j] = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? ST[r * CW + c] : make_float2(0.f, 0.f);
             }
         }
-        __syncthreads();                                      // ST read by every thread; NEED complete
-        if (un < total) issue(un);                            // in flight during both transforms
+        __syncthreads();                                      // ST read by every thread; NEED and ROWS complete
         // pair masks of this thread's class (bit 0: the DC input / output)
         uint32_t pm;
         {
@@ -934,7 +951,20 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
             bfly4<-1>(v[bb]);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (OKS_IN((4 * b + j) * CW + c, N * CW, OKS_B_TILE)) D[(4 * b + j) * CW + c] = v[bb][j];
+                if (OKS_IN(dr(4 * b + j) + c, N * CW, OKS_B_TILE)) D[dr(4 * b + j) + c] = v[bb][j];
+        }
+        {
+            // y' on the sampled rows into ST (16-byte cp.async, column pairs),
+            // in flight during the forward's radix-23 stage
+            const float2* y = a.y + p * a.y_stride;
+            for (int k = tid; k < N * (CW / 2); k += CW * TPC) {
+                const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+                if (!rowbit(r)) continue;
+                const bool onj = x0 + j < nx;
+                if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                    cp_async16(ST + r * CW + j, onj ? y + (long long)r * nx + x0 + j : y, onj ? 16u : 0u);
+            }
+            cp_async_commit();
         }
         __syncthreads();
         // forward stage 1 (radix 23, p = 4): butterfly 4 (tc mod 4) + tc / 4
@@ -945,11 +975,11 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
             if (act) {
                 const int b = 4 * (tc & 3) + (tc >> 2), k = b & 3;
                 ob = (b - k) * 23 + k;
-                x0v = D[b * CW + c];
+                x0v = D[dr(b) + c];
 #pragma unroll
                 for (int j = 1; j <= H; ++j) {
-                    const float2 uu = twmul<-1>(D[(b + 16 * j) * CW + c], TWs[F1 + k * 22 + j - 1]);
-                    const float2 ww = twmul<-1>(D[(b + 16 * (23 - j)) * CW + c], TWs[F1 + k * 22 + 22 - j]);
+                    const float2 uu = twmul<-1>(D[dr(b + 16 * j) + c], TWs[F1 + k * 22 + j - 1]);
+                    const float2 ww = twmul<-1>(D[dr(b + 16 * (23 - j)) + c], TWs[F1 + k * 22 + 22 - j]);
                     fa[j - 1] = uu + ww;
                     fb[j - 1] = uu - ww;
                 }
@@ -960,47 +990,40 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
                     float2 y0 = x0v;
 #pragma unroll
                     for (int j = 0; j < H; ++j) y0 = y0 + fa[j];
-                    D[ob * CW + c] = y0;
+                    D[dr(ob) + c] = y0;
                 }
-                p368_pairs_fwd<CW, -1, 1>(fa, fb, x0v, D, ob, c, pm);
+                p368_pairs_fwd<CW, SW, -1, 1>(fa, fb, x0v, D, ob, c, pm);
             }
         }
+        cp_async_wait_all();                                  // this thread's y' copies
         __syncthreads();
         // forward stage 2 (radix 4, p = 92) and the residual m' (F S - y'),
         // each butterfly in place on its own four rows
-        {
-            const float2* y = a.y + p * a.y_stride;
 #pragma unroll
-            for (int bb = 0; bb < BPT; ++bb) {
-                const int b = tc + TPC * bb;
-                if (NB4 % TPC != 0 && b >= NB4) break;
-                if (!need(b)) continue;
-                float2 yv[4];
-                bool sm4[4];
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (NB4 % TPC != 0 && b >= NB4) break;
+            if (!need(b)) continue;
+            float2 w4[4];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int r = b + NB4 * j;
-                    sm4[j] = colon && rowbit(r);
-                    yv[j] = sm4[j] ? y[(long long)r * nx + x] * (((r + x) & 1) ? -ysc : ysc) : make_float2(0.f, 0.f);
-                }
-                float2 w4[4];
+            for (int j = 0; j < 4; ++j) {
+                const int r = b + NB4 * j;
+                float2 t = OKS_IN(dr(r) + c, N * CW, OKS_B_TILE) ? D[dr(r) + c] : make_float2(0.f, 0.f);
+                if (j > 0) t = twmul<-1>(t, TWs[F2 + b * 3 + j - 1]);
+                w4[j] = t;
+            }
+            bfly4<-1>(w4);
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int r = b + NB4 * j;
-                    float2 t = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? D[r * CW + c] : make_float2(0.f, 0.f);
-                    if (j > 0) t = twmul<-1>(t, TWs[F2 + b * 3 + j - 1]);
-                    w4[j] = t;
-                }
-                bfly4<-1>(w4);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int r = b + NB4 * j;
-                    if (OKS_IN(r * CW + c, N * CW, OKS_B_TILE))
-                        D[r * CW + c] = sm4[j] ? (w4[j] - yv[j]) * minv : make_float2(0.f, 0.f);
-                }
+            for (int j = 0; j < 4; ++j) {
+                const int r = b + NB4 * j;
+                const bool smp = colon && rowbit(r);
+                const float2 yv = smp ? ST[r * CW + c] * (((r + x) & 1) ? -ysc : ysc) : make_float2(0.f, 0.f);
+                if (OKS_IN(dr(r) + c, N * CW, OKS_B_TILE))
+                    D[dr(r) + c] = smp ? (w4[j] - yv) * minv : make_float2(0.f, 0.f);
             }
         }
-        __syncthreads();
+        __syncthreads();                                      // ST (y') read by every thread
+        if (un < total) issue_s(un);                          // the next S tile, in flight during the inverse
         // inverse stage 0 (radix 4, p = 1): inputs b + 92 j, outputs 4 b + j
 #pragma unroll
         for (int bb = 0; bb < BPT; ++bb) {
@@ -1010,7 +1033,7 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int r = b + NB4 * j;
-                v[bb][j] = (nz && OKS_IN(r * CW + c, N * CW, OKS_B_TILE)) ? D[r * CW + c] : make_float2(0.f, 0.f);
+                v[bb][j] = (nz && OKS_IN(dr(r) + c, N * CW, OKS_B_TILE)) ? D[dr(r) + c] : make_float2(0.f, 0.f);
             }
         }
         __syncthreads();                                      // in place: every input read
@@ -1021,7 +1044,7 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
             if (need(b)) bfly4<+1>(v[bb]);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (OKS_IN((4 * b + j) * CW + c, N * CW, OKS_B_TILE)) D[(4 * b + j) * CW + c] = v[bb][j];
+                if (OKS_IN(dr(4 * b + j) + c, N * CW, OKS_B_TILE)) D[dr(4 * b + j) + c] = v[bb][j];
         }
         __syncthreads();
         // inverse stage 1 (radix 23, p = 4): butterfly tc, zero input pairs left out
@@ -1032,12 +1055,12 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
             if (act) {
                 const int b = tc, k = b & 3;
                 ob = (b - k) * 23 + k;
-                x0v = D[b * CW + c];
+                x0v = D[dr(b) + c];
 #pragma unroll
                 for (int j = 1; j <= H; ++j) {
                     if ((pm >> j) & 1u) {
-                        const float2 uu = twmul<+1>(D[(b + 16 * j) * CW + c], TWs[I1 + k * 22 + j - 1]);
-                        const float2 ww = twmul<+1>(D[(b + 16 * (23 - j)) * CW + c], TWs[I1 + k * 22 + 22 - j]);
+                        const float2 uu = twmul<+1>(D[dr(b + 16 * j) + c], TWs[I1 + k * 22 + j - 1]);
+                        const float2 ww = twmul<+1>(D[dr(b + 16 * (23 - j)) + c], TWs[I1 + k * 22 + 22 - j]);
                         fa[j - 1] = uu + ww;
                         fb[j - 1] = uu - ww;
                     } else {
@@ -1052,8 +1075,8 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
 #pragma unroll
                 for (int j = 1; j <= H; ++j)
                     if ((pm >> j) & 1u) y0 = y0 + fa[j - 1];
-                D[ob * CW + c] = y0;
-                p368_pairs_inv<CW, +1, 1>(fa, fb, x0v, D, ob, c, pm);
+                D[dr(ob) + c] = y0;
+                p368_pairs_inv<CW, SW, +1, 1>(fa, fb, x0v, D, ob, c, pm);
             }
         }
         __syncthreads();
@@ -1068,7 +1091,7 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int r = b + NB4 * j;
-                    float2 t = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? D[r * CW + c] : make_float2(0.f, 0.f);
+                    float2 t = OKS_IN(dr(r) + c, N * CW, OKS_B_TILE) ? D[dr(r) + c] : make_float2(0.f, 0.f);
                     if (j > 0) t = twmul<+1>(t, TWs[I2 + b * 3 + j - 1]);
                     w4[j] = t;
                 }
@@ -1084,21 +1107,21 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
     cp_async_wait_all();
 }
 
-template <int CW, int TPC>
+template <int CW, int TPC, bool SW = false>
 static cudaError_t col2d_p368_k(const Fista2dArgs& a, cudaStream_t st) {
     using P = S368;
     const float2 *tw, *rt;
     int nrt;
     cudaError_t e = plan_tables<P>(&tw, &rt, &nrt);
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(float2) * ((size_t)2 * P::N * CW + Tw<P>::total()) + 4 * sizeof(uint32_t);
-    const void* fn = reinterpret_cast<const void*>(k2d_col_p368<CW, TPC>);
+    const size_t smem = sizeof(float2) * ((size_t)2 * P::N * CW + Tw<P>::total()) + 16 * sizeof(uint32_t);
+    const void* fn = reinterpret_cast<const void*>(k2d_col_p368<CW, TPC, SW>);
     if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
     const long long tiles = a.nprob * ((a.nx + CW - 1) / CW);
     long long grid = tiles;
     const long long cap = (long long)ctas_per_sm(fn, CW * TPC, smem) * sm_count();
     if (grid > cap) grid = cap;
-    k2d_col_p368<CW, TPC><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw);
+    k2d_col_p368<CW, TPC, SW><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw);
     return cudaGetLastError();
 }
 }  // namespace reg
@@ -1113,6 +1136,7 @@ cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, c
             case 10: return reg::col2d_p368_k<8, 32>(a, st);
             case 11: return reg::col2d_p368_k<16, 16>(a, st);
             case 12: return reg::col2d_p368_k<16, 32>(a, st);
+            case 13: return reg::col2d_p368_k<8, 16, true>(a, st);
             default: return reg::col2d_p368_k<8, 16>(a, st);
         }
     }

@@ -166,9 +166,9 @@ def row_set_mask(ny, nx, rows):
 
 
 @pytest.mark.parametrize("rows", ["r4_centre", "r4_offset", "r3", "random20", "one_row", "all", "class_edge"])
-@pytest.mark.parametrize("form", [9, 10, 11, 12])
+@pytest.mark.parametrize("form", [9, 10, 11, 12, 13])
 def test_pruned_368_column_pass(ctx, rng, rows, form):
-    """The 368 column pass pruned to the sampled rows (col2d_lanes 9-12)
+    """The 368 column pass pruned to the sampled rows (col2d_lanes 9-13)
     against the full register pass and FP64, for row sets that exercise
     every pruning case: R = 4 plus a centre block (the precision workload's
     pattern, dense class and sparse classes), R = 4 shifted by one row, R = 3
