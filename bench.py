@@ -556,15 +556,18 @@ def serving_measure(ctx, rates, seconds, max_requests, mode=0, n_streams=0, volu
     masks = [np.repeat(r.mask_rows[:, None], r.kspace.shape[2], 1) for r in pool]
     for k, m, r in zip(pinned, masks, pool):                 # warm-up: every size, iteration count (plans, tables)
         ctx.cs_slice(k, m, r.iters, r.lam)
-    # plain per-slice drop-in
-    lat = []
-    t0 = time.perf_counter()
-    for k, m, r in zip(pinned, masks, pool):
-        a = time.perf_counter()
-        ctx.cs_slice(k, m, r.iters, r.lam)
-        lat.append(time.perf_counter() - a)
-    plain_rate = len(pool) / (time.perf_counter() - t0)
-    plain = {"slices_per_s": plain_rate, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+    # plain per-slice drop-in: three passes over the pool, the median pass rate
+    # (one slow host call in a 32-call pass moves a single pass's rate a lot)
+    lat, pass_rates = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        for k, m, r in zip(pinned, masks, pool):
+            a = time.perf_counter()
+            ctx.cs_slice(k, m, r.iters, r.lam)
+            lat.append(time.perf_counter() - a)
+        pass_rates.append(len(pool) / (time.perf_counter() - t0))
+    plain_rate = float(np.median(pass_rates))
+    plain = {"slices_per_s": plain_rate, "pass_rates": pass_rates, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
              "p99_ms": 1e3 * float(np.percentile(lat, 99))}
     out, vol_rec = {}, None
     rng = np.random.default_rng(7)
