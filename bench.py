@@ -761,7 +761,7 @@ def precision_kernel_roofline(ctx, wl, hbm, peak_kind):
         ctx.set_option("graph2d", 1)
         ctx.set_option("fista2d_streams", 2)
     kernels = {}
-    step_ms = sum(v[0] for v in prof.values())
+    step_ms = sum(v[0] for v in prof.values() if v[1] > 0)   # kernels only (copy scopes count no launch)
     for k, b in model.items():
         ms, n = prof.get(k, (0.0, 0))
         if n == 0 or ms <= 0:

@@ -97,6 +97,10 @@ const char* okscuda_version(void);
  *                   only unsampled rows reach are left out), (columns,
  *                   threads per column) (8,16) (8,32) (16,16) (16,32); 13 =
  *                   (8,16) with the row slots swizzled against bank conflicts
+ *   "row2d_ctas", "col2d_ctas" 2-D engine: at most this many CTAs per SM for
+ *                   the persistent row pass / the pruned 368 column pass, so
+ *                   the other stream's pass finds room on every SM; 0
+ *                   (default) = every resident slot
  *   "occ2d"         2-D register passes: 1 = launch bounds that keep at
  *                   least 12 warps resident per SM, 2 = at least 18, 3 = at
  *                   least 15, 0 = registers as needed

@@ -142,8 +142,14 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
                            "col2d_lanes: -1 column pairs, 0 by length, 1 to 8 a lanes form, 9 to 13 the pruned 368 forms");
         ctx->col2d_lanes = (int)value;
     } else if (!std::strcmp(name, "xform_row_variant")) {
-        if (value < 0 || value > 5) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0 to 5");
+        if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");
         ctx->xform_row_variant = (int)value;
+    } else if (!std::strcmp(name, "row2d_ctas")) {
+        if (value < 0 || value > 16) return set_err(ctx, OKS_EINVAL, "row2d_ctas: 0 to 16");
+        ctx->row2d_ctas = (int)value;
+    } else if (!std::strcmp(name, "col2d_ctas")) {
+        if (value < 0 || value > 16) return set_err(ctx, OKS_EINVAL, "col2d_ctas: 0 to 16");
+        ctx->col2d_ctas = (int)value;
     } else if (!std::strcmp(name, "prewhiten_bulk")) {
         if (value < -1 || value > 1) return set_err(ctx, OKS_EINVAL, "prewhiten_bulk: -1, 0 or 1");
         ctx->prewhiten_bulk = (int)value;
@@ -492,6 +498,8 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             // takes the iteration passes of separable masks; the rest stay on
             // the column-pair pass), the column-pair pass elsewhere
             a.col_lanes = ctx->col2d_lanes > 0 ? ctx->col2d_lanes : (ctx->col2d_lanes == 0 && ny == 368 ? 9 : 0);
+            a.row_ctas = ctx->row2d_ctas;
+            a.col_ctas = ctx->col2d_ctas;
             auto col = [&](int mode) {
                 if (col_reg) {
                     ProfScope ps(ctx, "k2d_col_reg", st);
@@ -575,10 +583,10 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     const size_t data_bytes = sizeof(float2) * (size_t)nprob * N;
     if (ctx->graph2d && !use_tc) {
         char kb[320];
-        std::snprintf(kb, sizeof kb, "%d/%d/%lld/%d/%d/%08x/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%zu/%d/%d", ny, nx, nprob, nmask,
+        std::snprintf(kb, sizeof kb, "%d/%d/%lld/%d/%d/%08x/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%zu/%d/%d/%d/%d", ny, nx, nprob, nmask,
                       iters, [&] { uint32_t u; std::memcpy(&u, &lambda, 4); return u; }(), chunk, ns, (int)col_reg,
                       (int)row_reg, tp.persist2d, tp.occ2d, tp.prefetch2d, (int)separable, ctx->mask_bits, up.size(),
-                      ctx->device, ctx->col2d_lanes);
+                      ctx->device, ctx->col2d_lanes, ctx->row2d_ctas, ctx->col2d_ctas);
         const std::string key(kb);
         auto it = ctx->g2d.find(key);
         if (it == ctx->g2d.end()) {

@@ -789,7 +789,9 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
             else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0][pf], k2d_col_reg<P, MINB>, P::T * G, smem);
             if (per_sm[row][pf] < 1) per_sm[row][pf] = 1;
         }
-        if (grid > (long long)per_sm[row][pf] * nsm) grid = (long long)per_sm[row][pf] * nsm;
+        int per = per_sm[row][pf];
+        if (row && a.row_ctas > 0 && a.row_ctas < per) per = a.row_ctas;
+        if (grid > (long long)per * nsm) grid = (long long)per * nsm;
     }
     if (row)
         k2d_row_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(b, mode, it, tw, rt, nrt);

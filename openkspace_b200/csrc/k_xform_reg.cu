@@ -250,9 +250,8 @@ k_col_xform_reg(ColXformArgs a, const float2* __restrict__ gtw, const float2* __
 // middle stages work in place on one [N][CW] shared-memory tile (each thread
 // reads all its butterflies' inputs before the barrier that precedes the
 // writes).  Twiddles depend on the row only: one broadcast per half-warp.
-// PF: stage 0 reads its inputs from the staging tile ST ([N][STS], STS >= CW,
-// filled by cp.async while the previous tile was transformed) instead of
-// global memory.
+// PF: stage 0 reads its inputs from the staging tile ST ([N][CW], filled by
+// cp.async while the previous tile was transformed) instead of global memory.
 // Output pairs Q, Q + 1, ..., (R - 1) / 2 of a large odd-radix butterfly
 // (symmetric form, compile-time roots) stored to the lanes tile.
 template <int SIGN, int R, int Q, int CW>
@@ -277,8 +276,7 @@ struct NoRefill {
 struct NoOut {
     __device__ void operator()(int, float2) const {}
 };
-template <class P, int SIGN, int CW, int TPC, int s, bool PF = false, class F = NoRefill, class Out = NoOut,
-          int STS = CW>
+template <class P, int SIGN, int CW, int TPC, int s, bool PF = false, class F = NoRefill, class Out = NoOut>
 __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2* __restrict__ TW,
                                             const float2* __restrict__ RT, float2* __restrict__ col, int nx,
                                             bool on, bool centred, float sc, int c, int tc,
@@ -346,7 +344,7 @@ __device__ __forceinline__ void lanes_stage(float2* __restrict__ D, const float2
             const int r = b + j * NB;
             if constexpr (s == 0) {
                 float2 x;
-                if constexpr (PF) x = OKS_IN(r * STS + c, N * STS, OKS_B_TILE) ? ST[r * STS + c] : make_float2(0.f, 0.f);
+                if constexpr (PF) x = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? ST[r * CW + c] : make_float2(0.f, 0.f);
                 else x = on ? col[r * nx] : make_float2(0.f, 0.f);   // N nx < 2^31 (launcher)
                 if (centred && (r & 1)) x = make_float2(-x.x, -x.y);
                 v[bb][j] = x;
@@ -521,115 +519,6 @@ static cudaError_t row_p(const RowXformArgs& a, cudaStream_t st) {
     if (a.sign < 0) k_row_xform_reg<P, -1><<<(unsigned)grid, P::T * G, smem, st>>>(b, tw, rt, nrt);
     else k_row_xform_reg<P, +1><<<(unsigned)grid, P::T * G, smem, st>>>(b, tw, rt, nrt);
     return cudaGetLastError();
-}
-
-
-// Row transform with the lanes across RW rows (the lanes form of k_col_lanes
-// turned on its side).  A CTA takes a tile of RW consecutive rows: the rows
-// are copied element by element (8-byte cp.async, consecutive threads on
-// consecutive elements of one row) into the staging tile ST, transposed to
-// [N][RW + 1] (the odd stride spreads the transposed writes over the banks),
-// while the previous tile is transformed.  Thread (c, tc) = (tid % RW,
-// tid / RW) then owns row c of the tile and the butterflies tc, tc + TPR, ...
-// of every stage, exactly as the column form owns a column: stage 0 reads
-// ST, the middle stages run in place on D = [N][RW], and the last stage
-// stores element o of row c straight to global memory (four lanes of a row
-// write one 32-byte sector).  The large odd radix of 368 gets one thread per
-// butterfly, as in the column form.  Same arithmetic per element as the
-// column form; centring signs, scale, rowsign and kept rows as in
-// k_row_xform_reg.
-template <class P, int SIGN, int RW, int TPR>
-__global__ void __launch_bounds__(RW * TPR,
-                                  xform_min_blocks<RW * TPR, big_odd_plan<P>() ? 128 : lanes_regs<P, TPR>()>())
-k_row_lanes(RowXformArgs a, const float2* __restrict__ gtw, const float2* __restrict__ groots, int roots_total) {
-    constexpr int N = P::N, STS = RW + 1;
-    extern __shared__ __align__(16) float2 sm[];
-    float2* D = sm;                                  // [N][RW]
-    float2* ST = D + N * RW;                         // [N][RW + 1]
-    float2* TWs = ST + N * STS;
-    float2* RT = TWs + tw_half<P>();
-    const float2* TW = load_twiddles<P, SIGN>(TWs, gtw);
-    for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
-    const int c = threadIdx.x % RW, tc = threadIdx.x / RW;
-    const long long ntiles = (a.nrows + RW - 1) / RW;
-    auto row_kept = [&](long long row) {
-        if (row >= a.nrows) return false;
-        return !a.use_keep || row_on(a.keep, row / a.rows_per_prob, (int)(row % a.rows_per_prob));
-    };
-    auto issue = [&](long long u) {
-        for (int k = threadIdx.x; k < RW * N; k += RW * TPR) {
-            const int r = k / N, n = k - r * N;
-            const long long row = u * RW + r;
-            const bool on = row_kept(row);
-            if (OKS_IN(n * STS + r, N * STS, OKS_B_STAGE))
-                cp_async8(ST + n * STS + r, on ? a.in + row * a.ld_in + n : a.in, on ? 8u : 0u);
-        }
-        cp_async_commit();
-    };
-    const float sc_n2 = (a.centred && ((N / 2) & 1)) ? -a.scale : a.scale;
-    long long u = blockIdx.x;
-    if (u < ntiles) issue(u);
-    for (; u < ntiles; u += gridDim.x) {
-        const long long row = u * RW + c;
-        const bool on = row < a.nrows;
-        float s = sc_n2;
-        if (a.rowsign && ((row % a.rows_per_prob) & 1)) s = -s;
-        float2* o = a.out + (on ? row : 0) * a.ld_out;
-        const bool centred = a.centred != 0;
-        cp_async_wait_all();
-        __syncthreads();                             // ST holds tile u; the last tile's final stage has read D
-        const long long un = u + gridDim.x;
-        auto refill = [&]() {
-            if (un < ntiles) issue(un);
-        };
-        auto store = [o, on, s, centred](int k, float2 v) {
-            if (on) o[k] = v * ((centred && (k & 1)) ? -s : s);
-        };
-        lanes_stage<P, SIGN, RW, TPR, 0, true, decltype(refill), decltype(store), STS>(
-            D, TW, RT, nullptr, 0, on, centred, 1.f, c, tc, ST, refill, store);
-    }
-    cp_async_wait_all();
-}
-
-template <class P, int RW, int TPR>
-static cudaError_t row_lanes_k(const RowXformArgs& a, cudaStream_t st) {
-    const float2 *tw, *rt;
-    int nrt;
-    cudaError_t e = cudaSuccess;
-    if (a.tables) {   // caller-owned tables: nothing is allocated here
-        tw = a.tables;
-        rt = a.tables + Tw<P>::total();
-        nrt = a.tables_nroots;
-    } else if ((e = plan_tables<P>(&tw, &rt, &nrt)) != cudaSuccess) {
-        return e;
-    }
-    const size_t smem = sizeof(float2) * ((size_t)P::N * (2 * RW + 1) + tw_half<P>() + nrt);
-    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_row_lanes<P, -1, RW, TPR>)
-                                : reinterpret_cast<const void*>(k_row_lanes<P, +1, RW, TPR>);
-    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
-    const long long tiles = (a.nrows + RW - 1) / RW;
-    long long grid = tiles;
-    const long long cap = (long long)ctas_per_sm(fn, RW * TPR, smem) * sm_count();
-    if (grid > cap) grid = cap;
-    if (a.sign < 0) k_row_lanes<P, -1, RW, TPR><<<(unsigned)grid, RW * TPR, smem, st>>>(a, tw, rt, nrt);
-    else k_row_lanes<P, +1, RW, TPR><<<(unsigned)grid, RW * TPR, smem, st>>>(a, tw, rt, nrt);
-    return cudaGetLastError();
-}
-
-// Row lanes forms (variant 3-5): (rows, threads per row) (8, 16) (16, 16)
-// (8, 32) for 368 (16 threads per row: one per radix-23 butterfly), (8, 32)
-// (16, 32) (8, 64) for the other lengths.
-template <class P>
-static cudaError_t row_lanes(const RowXformArgs& a, int variant, cudaStream_t st) {
-    if constexpr (big_odd_plan<P>()) {
-        if (variant == 4) return row_lanes_k<P, 16, 16>(a, st);
-        if (variant == 5) return row_lanes_k<P, 8, 32>(a, st);
-        return row_lanes_k<P, 8, 16>(a, st);
-    } else {
-        if (variant == 4) return row_lanes_k<P, 16, 32>(a, st);
-        if (variant == 5) return row_lanes_k<P, 8, 64>(a, st);
-        return row_lanes_k<P, 8, 32>(a, st);
-    }
 }
 
 template <class P, int G>
@@ -1230,7 +1119,9 @@ static cudaError_t col2d_p368_k(const Fista2dArgs& a, cudaStream_t st) {
     if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
     const long long tiles = a.nprob * ((a.nx + CW - 1) / CW);
     long long grid = tiles;
-    const long long cap = (long long)ctas_per_sm(fn, CW * TPC, smem) * sm_count();
+    int per = ctas_per_sm(fn, CW * TPC, smem);
+    if (a.col_ctas > 0 && a.col_ctas < per) per = a.col_ctas;
+    const long long cap = (long long)per * sm_count();
     if (grid > cap) grid = cap;
     k2d_col_p368<CW, TPC, SW><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw);
     return cudaGetLastError();
@@ -1289,18 +1180,6 @@ cudaError_t launch_row_xform_reg(const RowXformArgs& a, int n, cudaStream_t st) 
         if (n == 320) return reg::row_p<reg::V320>(a, st);    // 8·5·8 on 80 of 96 threads
     }
     if (a.variant == 2 && !a.tables && n == 192) return reg::row_p<reg::R192>(a, st);   // 4·12·4 on 96 threads
-    if (a.variant >= 3 && a.variant <= 5 && !a.tables) {   // the lanes forms
-        switch (n) {
-            case 192: return reg::row_lanes<reg::P192>(a, a.variant, st);
-            case 256: return reg::row_lanes<reg::S256>(a, a.variant, st);
-            case 320: return reg::row_lanes<reg::S320>(a, a.variant, st);
-            case 368: return reg::row_lanes<reg::S368>(a, a.variant, st);
-            case 384: return reg::row_lanes<reg::S384>(a, a.variant, st);
-            case 512: return reg::row_lanes<reg::S512>(a, a.variant, st);
-            case 640: return reg::row_lanes<reg::P640>(a, a.variant, st);
-            default: break;
-        }
-    }
     switch (n) {
         case 128: return reg::row_p<reg::S128>(a, st);
         case 192: return reg::row_p<reg::P192>(a, st);

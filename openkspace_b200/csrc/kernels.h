@@ -189,6 +189,9 @@ struct Fista2dArgs {
                               // pass (separable masks), bit 1 row pass; bit 2 row pass with
                               // bulk-copy (cp.async.bulk) staging of S, Z~, X~
     int* err;                 // bounded-wait error word (bulk-copy row pass), may be null
+    int row_ctas;             // > 0: the persistent row pass takes at most this many CTAs per SM
+    int col_ctas;             // > 0: the pruned 368 column pass takes at most this many CTAs per SM
+                              // (room for the other stream's pass on the same SM)
     int col_lanes;            // column pass in the lanes form: 0 off, else the form (1-8); 9-12
                               // the pruned 368 forms (separable masks, iteration passes)
 };

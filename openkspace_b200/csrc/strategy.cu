@@ -376,6 +376,7 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
         DevBuf raw(ctx);
         OKS_CUDA(raw.alloc(sizeof(float2) * (size_t)ng * gnc * gns));
         // gather (contiguous runs are one copy)
+        ProfScope ps_copy(ctx, A->data_on_device ? "copy_lines_d2d" : "copy_lines_h2d", nullptr, 0);   // no kernel
         for (long long i = 0; i < ng;) {
             long long j = i + 1;
             while (j < ng && H[ids[j]].data_offset == H[ids[j - 1]].data_offset + (long long)gnc * gns) ++j;
@@ -507,8 +508,11 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
     }
     // device-resident mode (data_on_device): h_out is a device buffer and the
     // call returns without waiting
-    OKS_CUDA(cudaMemcpyAsync(h_out, rss.p, sizeof(float) * (size_t)nout,
-                             A->data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    {
+        ProfScope ps(ctx, A->data_on_device ? "copy_out_d2d" : "copy_out_d2h", nullptr, 0);   // no kernel
+        OKS_CUDA(cudaMemcpyAsync(h_out, rss.p, sizeof(float) * (size_t)nout,
+                                 A->data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    }
     if (!A->data_on_device) OKS_CUDA(cudaStreamSynchronize(ctx->stream));
     return OKS_OK;
 }

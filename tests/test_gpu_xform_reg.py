@@ -167,43 +167,6 @@ def test_row_plan_variants(ctx, rng, n, variant):
     assert rel_l2(got_i, ref_rows(x.reshape(-1, n), 1, 1)) < TOL
 
 
-@pytest.mark.parametrize("variant", [3, 4, 5])
-@pytest.mark.parametrize("n", [192, 256, 320, 368, 384, 512, 640])
-def test_row_lanes_forms(ctx, rng, n, variant):
-    """The row transform with the lanes across rows (xform_row_variant 3-5):
-    row counts that leave a ragged last tile, both directions, the centred
-    2-D FFT and the plain inverse row DFT."""
-    x = crandn(rng, (3, 21, n))
-    ctx.set_option("xform_row_variant", variant)
-    try:
-        got = ctx.centred_fft2(x, False)
-        got_inv = ctx.centred_fft2(x, True)
-        got_i = ctx.dft_rows(x.reshape(-1, n)[:61], inverse=True, centred=True, engine=0)
-    finally:
-        ctx.set_option("xform_row_variant", 0)
-    assert rel_l2(got, o64.centred_fft2(x)) < TOL
-    assert rel_l2(got_inv, o64.centred_ifft2(x)) < TOL
-    assert rel_l2(got_i, ref_rows(x.reshape(-1, n)[:61], 1, 1)) < TOL
-
-
-@pytest.mark.parametrize("variant", [3, 4])
-def test_row_lanes_in_the_column_engine(ctx, rng, variant):
-    """The column engine's readout pass (rows outside the ky mask kept at
-    zero, per-problem row signs) through the row lanes forms: FISTA with a
-    ky-only mask against FP64."""
-    ny, nx, iters = 256, 368, 6
-    m = np.zeros((ny, nx), bool)
-    m[rng.random(ny) < 0.3] = True
-    m[ny // 2 - 4:ny // 2 + 4] = True
-    k = np.where(m[None], crandn(rng, (3, ny, nx)), 0).astype(np.complex64)
-    ctx.set_option("xform_row_variant", variant)
-    try:
-        got = ctx.fista_cs(k, m, iters, 0.02)
-    finally:
-        ctx.set_option("xform_row_variant", 0)
-    assert rel_l2(got, o64.fista_cs_single_coil(k, m, iters, 0.02)) < 1e-4
-
-
 @pytest.mark.parametrize("pf", [0, 1])
 @pytest.mark.parametrize("lanes", [5, 6, 7, 8])
 def test_column_lanes_368(ctx, rng, lanes, pf):
