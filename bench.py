@@ -916,7 +916,18 @@ def main():
         # the side workloads' synthetic inputs are generated in a separate
         # process (spawned before the first GPU call) while this one measures
         import multiprocessing as mp
+        # two math-library threads in the generator (the spawned process reads
+        # these at its numpy import), so that it does not compete with the
+        # host side of the timed end-to-end calls for every core
+        saved = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
+        for k in saved:
+            os.environ[k] = "2"
         side_pool = mp.get_context("spawn").Pool(1)
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
         side_dir = tempfile.mkdtemp()
         side_inputs = side_pool.apply_async(_side_inputs, (side_dir,))
 

@@ -363,33 +363,45 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     const int cw = (nx + 31) / 32, rw = (ny + 31) / 32;
     const size_t mbytes = (size_t)nmask * N, cb_off = (mbytes + 15) & ~size_t(15);
     const size_t rb_off = cb_off + sizeof(uint32_t) * (size_t)nmask * cw;
-    std::vector<uint8_t> up(rb_off + sizeof(uint32_t) * (size_t)nmask * rw, 0);
-    std::memcpy(up.data(), h_mask, mbytes);
-    uint32_t* colbits = reinterpret_cast<uint32_t*>(up.data() + cb_off);
-    uint32_t* rowbits = reinterpret_cast<uint32_t*>(up.data() + rb_off);
-    for (int k = 0; k < nmask; ++k)
-        for (int r = 0; r < ny; ++r) {
-            const uint8_t* row = h_mask + (size_t)k * N + (size_t)r * nx;
-            for (int x = 0; x < nx; ++x)
-                if (row[x]) {
-                    colbits[(size_t)k * cw + (x >> 5)] |= 1u << (x & 31);
-                    rowbits[(size_t)k * rw + (r >> 5)] |= 1u << (r & 31);
-                }
-        }
-    // separable: every sampled row holds exactly the mask's sampled columns
+    const size_t up_bytes = rb_off + sizeof(uint32_t) * (size_t)nmask * rw;
+    if (ctx->h_mask_up.size() < up_bytes) ctx->h_mask_up.resize(up_bytes);   // kept across calls
+    uint8_t* up = ctx->h_mask_up.data();
+    std::memcpy(up, h_mask, mbytes);
+    std::memset(up + mbytes, 0, up_bytes - mbytes);
+    uint32_t* colbits = reinterpret_cast<uint32_t*>(up + cb_off);
+    uint32_t* rowbits = reinterpret_cast<uint32_t*>(up + rb_off);
+    // per mask: the rows with any sample, the OR of those rows (the columns
+    // with any sample), and whether every sampled row holds exactly those
+    // columns (separable).  Whole-row loops the compiler vectorises; the
+    // byte-exact test runs only for a row whose bytes differ from the OR.
     bool separable = true;
-    for (int k = 0; k < nmask && separable; ++k)
+    std::vector<uint8_t> any_row((size_t)nx);
+    for (int k = 0; k < nmask; ++k) {
+        const uint8_t* mk = h_mask + (size_t)k * N;
+        std::fill(any_row.begin(), any_row.end(), uint8_t(0));
+        for (int r = 0; r < ny; ++r) {
+            const uint8_t* row = mk + (size_t)r * nx;
+            uint8_t acc = 0;
+            for (int x = 0; x < nx; ++x) acc |= row[x];
+            if (!acc) continue;
+            rowbits[(size_t)k * rw + (r >> 5)] |= 1u << (r & 31);
+            for (int x = 0; x < nx; ++x) any_row[x] |= row[x];
+        }
+        for (int x = 0; x < nx; ++x)
+            if (any_row[x]) colbits[(size_t)k * cw + (x >> 5)] |= 1u << (x & 31);
         for (int r = 0; r < ny && separable; ++r) {
             if (!((rowbits[(size_t)k * rw + (r >> 5)] >> (r & 31)) & 1u)) continue;
-            const uint8_t* row = h_mask + (size_t)k * N + (size_t)r * nx;
+            const uint8_t* row = mk + (size_t)r * nx;
+            if (std::memcmp(row, any_row.data(), (size_t)nx) == 0) continue;
             for (int x = 0; x < nx; ++x)
-                if ((row[x] != 0) != (((colbits[(size_t)k * cw + (x >> 5)] >> (x & 31)) & 1u) != 0)) {
+                if ((row[x] != 0) != (any_row[x] != 0)) {
                     separable = false;
                     break;
                 }
         }
+    }
     oks::Staging::Slot* slot = nullptr;
-    rc = stage_upload(ctx, up.data(), up.size(), &slot);
+    rc = stage_upload(ctx, up, up_bytes, &slot);
     if (rc) return rc;
     const TuneParams tp = tune_params(ctx, 1, ny, nx);
     long long chunk = tp.fista2d_chunk > 0 ? tp.fista2d_chunk
@@ -585,7 +597,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
         char kb[320];
         std::snprintf(kb, sizeof kb, "%d/%d/%lld/%d/%d/%08x/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%zu/%d/%d/%d/%d", ny, nx, nprob, nmask,
                       iters, [&] { uint32_t u; std::memcpy(&u, &lambda, 4); return u; }(), chunk, ns, (int)col_reg,
-                      (int)row_reg, tp.persist2d, tp.occ2d, tp.prefetch2d, (int)separable, ctx->mask_bits, up.size(),
+                      (int)row_reg, tp.persist2d, tp.occ2d, tp.prefetch2d, (int)separable, ctx->mask_bits, up_bytes,
                       ctx->device, ctx->col2d_lanes, ctx->row2d_ctas, ctx->col2d_ctas);
         const std::string key(kb);
         auto it = ctx->g2d.find(key);
@@ -609,7 +621,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
                 }
                 cudaError_t ge = cudaMalloc(&g.y, data_bytes);
                 if (ge == cudaSuccess) ge = cudaMalloc(&g.out, data_bytes);
-                if (ge == cudaSuccess) ge = cudaMalloc(&g.masks, up.size());
+                if (ge == cudaSuccess) ge = cudaMalloc(&g.masks, up_bytes);
                 if (ge == cudaSuccess) ge = cudaMalloc(&g.scratch, stream_bytes * ns);
                 if (ge == cudaSuccess) ge = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
                 if (ge == cudaSuccess) {
@@ -650,7 +662,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             if (g.exec) {
                 cudaError_t ge = cudaStreamWaitEvent(ctx->stream, g.done, 0);   // the previous replay is done
                 if (ge == cudaSuccess)
-                    ge = cudaMemcpyAsync(g.masks, slot->dev, up.size(), cudaMemcpyDeviceToDevice, ctx->stream);
+                    ge = cudaMemcpyAsync(g.masks, slot->dev, up_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
                 if (ge == cudaSuccess)
                     ge = cudaMemcpyAsync(g.y, d_kspace, data_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
                 if (ge == cudaSuccess) {

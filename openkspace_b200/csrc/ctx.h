@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <tuple>
 #include <string>
 #include <vector>
@@ -89,6 +90,9 @@ struct okscuda_ctx {
     int prewhiten_bulk = -1;              // prewhitening: -1 by channel count, 1 bulk-copy staged kernel, 0 plain loads
     struct Aux { cudaStream_t stream = nullptr; cudaEvent_t done = nullptr; };
     std::vector<Aux> aux;                 // fork/join streams (okscuda_cs_batch)
+    // host scratch kept across calls (no page faults on every call): the 2-D
+    // engine's mask upload image and the placement's filled mask
+    std::vector<uint8_t> h_mask_up, h_filled;
     cudaEvent_t fork_ev = nullptr;
     // per-launch CUDA-event profiling (okscuda_profile_*)
     bool prof_on = false;
@@ -201,8 +205,14 @@ inline int get_plan(okscuda_ctx* ctx, int n, const DevPlan** out) {
 // the copy is enqueued on the context stream, and a slot is reused only after
 // the event recorded behind the kernels that read it has completed.
 inline int stage_upload(okscuda_ctx* ctx, const void* src, size_t bytes, oks::Staging::Slot** out) {
-    oks::Staging::Slot* s = &ctx->staging.slots[ctx->staging.next];
-    ctx->staging.next = (ctx->staging.next + 1) % oks::Staging::kSlots;
+    oks::Staging::Slot* s;
+    if (bytes >= oks::Staging::kBig) {
+        s = &ctx->staging.big[ctx->staging.next_big];
+        ctx->staging.next_big ^= 1;
+    } else {
+        s = &ctx->staging.slots[ctx->staging.next];
+        ctx->staging.next = (ctx->staging.next + 1) % oks::Staging::kSlots;
+    }
     if (s->ev) OKS_CUDA(cudaEventSynchronize(s->ev));
     else OKS_CUDA(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming));
     if (bytes > s->cap) {

@@ -260,7 +260,19 @@ struct Staging {
     static constexpr int kSlots = 64;   // >= requests in flight on the request server
     Slot slots[kSlots];
     int next = 0;
+    // uploads of 1 MiB and more (2-D masks, large tables) take one of two
+    // slots of their own, so their pinned and device buffers are allocated
+    // once instead of once per ring slot
+    static constexpr size_t kBig = size_t(1) << 20;
+    Slot big[2];
+    int next_big = 0;
     void release() {
+        for (auto& s : big) {
+            if (s.ev) cudaEventSynchronize(s.ev), cudaEventDestroy(s.ev);
+            if (s.host) cudaFreeHost(s.host);
+            if (s.dev) cudaFree(s.dev);
+            s = Slot{};
+        }
         for (auto& s : slots) {
             if (s.ev) cudaEventSynchronize(s.ev), cudaEventDestroy(s.ev);
             if (s.host) cudaFreeHost(s.host);

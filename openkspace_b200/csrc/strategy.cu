@@ -360,7 +360,8 @@ int okscuda_csrss_reconstruct(okscuda_ctx* ctx, const okscuda_csrss_cfg* cfg, co
     // --- 3. second pass: preprocess + placement (reader.rs:332-457) ---------
     const int ky_off = ny / 2 - A->ky_center;
     const int kz_off = use_slice_axis ? 0 : nz / 2 - A->kz_center;
-    std::vector<uint8_t> filled((size_t)nz * N, 0);
+    std::vector<uint8_t>& filled = ctx->h_filled;   // kept across calls
+    filled.assign((size_t)nz * N, 0);
     DevBuf dk(ctx);
     OKS_CUDA(dk.alloc(sizeof(float2) * (size_t)nc * nz * N));
     OKS_CUDA(cudaMemsetAsync(dk.p, 0, sizeof(float2) * (size_t)nc * nz * N, ctx->stream));
