@@ -97,6 +97,10 @@ const char* okscuda_version(void);
  *                   only unsampled rows reach are left out), (columns,
  *                   threads per column) (8,16) (8,32) (16,16) (16,32); 13 =
  *                   (8,16) with the row slots swizzled against bank conflicts
+ *   "pdl2d"         2-D register passes launched as programmatic dependent
+ *                   launches: a pass's CTAs load their tables while the
+ *                   previous pass ends, then wait for it (griddepcontrol);
+ *                   0 (default) plain stream order, 1 on
  *   "row2d_ctas", "col2d_ctas" 2-D engine: at most this many CTAs per SM for
  *                   the persistent row pass / the pruned 368 column pass, so
  *                   the other stream's pass finds room on every SM; 0

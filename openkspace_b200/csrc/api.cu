@@ -144,6 +144,9 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
     } else if (!std::strcmp(name, "xform_row_variant")) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");
         ctx->xform_row_variant = (int)value;
+    } else if (!std::strcmp(name, "pdl2d")) {
+        if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "pdl2d: 0 or 1");
+        ctx->pdl2d = (int)value;
     } else if (!std::strcmp(name, "row2d_ctas")) {
         if (value < 0 || value > 16) return set_err(ctx, OKS_EINVAL, "row2d_ctas: 0 to 16");
         ctx->row2d_ctas = (int)value;
@@ -511,6 +514,7 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             // the column-pair pass), the column-pair pass elsewhere
             a.col_lanes = ctx->col2d_lanes > 0 ? ctx->col2d_lanes : (ctx->col2d_lanes == 0 && ny == 368 ? 9 : 0);
             a.row_ctas = ctx->row2d_ctas;
+            a.pdl = ctx->pdl2d;
             a.col_ctas = ctx->col2d_ctas;
             auto col = [&](int mode) {
                 if (col_reg) {
@@ -595,10 +599,10 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
     const size_t data_bytes = sizeof(float2) * (size_t)nprob * N;
     if (ctx->graph2d && !use_tc) {
         char kb[320];
-        std::snprintf(kb, sizeof kb, "%d/%d/%lld/%d/%d/%08x/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%zu/%d/%d/%d/%d", ny, nx, nprob, nmask,
+        std::snprintf(kb, sizeof kb, "%d/%d/%lld/%d/%d/%08x/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%zu/%d/%d/%d/%d/%d", ny, nx, nprob, nmask,
                       iters, [&] { uint32_t u; std::memcpy(&u, &lambda, 4); return u; }(), chunk, ns, (int)col_reg,
                       (int)row_reg, tp.persist2d, tp.occ2d, tp.prefetch2d, (int)separable, ctx->mask_bits, up_bytes,
-                      ctx->device, ctx->col2d_lanes, ctx->row2d_ctas, ctx->col2d_ctas);
+                      ctx->device, ctx->col2d_lanes, ctx->row2d_ctas, ctx->col2d_ctas, ctx->pdl2d);
         const std::string key(kb);
         auto it = ctx->g2d.find(key);
         if (it == ctx->g2d.end()) {

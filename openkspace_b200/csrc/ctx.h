@@ -85,6 +85,7 @@ struct okscuda_ctx {
     int xform_lanes_pf = 1;               // lanes form: 1 = next tile staged in shared memory while transforming
     int xform_row_variant = 0;            // register row transform: alternative plans for 192 and 320
     int col2d_lanes = 0;                  // 2-D engine column pass: 0 by length, -1 column pairs, 1-12 a lanes form
+    int pdl2d = 0;                        // 2-D register passes: programmatic dependent launches
     int row2d_ctas = 0;                   // 2-D row pass: CTAs per SM cap (0: every resident slot)
     int col2d_ctas = 0;                   // pruned 368 column pass: CTAs per SM cap (0: every resident slot)
     int prewhiten_bulk = -1;              // prewhitening: -1 by channel count, 1 bulk-copy staged kernel, 0 plain loads

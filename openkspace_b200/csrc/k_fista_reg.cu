@@ -165,6 +165,8 @@ k2d_col_reg(Fista2dArgs a, int mode, const float2* __restrict__ gtw, const float
     float2* B = A + P::SMEM_X;
     for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    pdl_wait();                                       // the previous pass's S is complete
+    pdl_trigger();
     __syncthreads();
     const int nx = a.nx, npairs = nx / 2;
     const bool live = t < TA;
@@ -310,6 +312,8 @@ k2d_row_reg(Fista2dArgs a, int mode, int it, const float2* __restrict__ gtw, con
     float2* B = A + P::SMEM_X;
     for (int q = threadIdx.x; q < NTW; q += blockDim.x) TW[q] = gtw[q];
     for (int q = threadIdx.x; q < roots_total; q += blockDim.x) RT[q] = groots[q];
+    pdl_wait();                                       // the previous pass's S, X~, Z~ are complete
+    pdl_trigger();
     __syncthreads();
     const int nrp = a.ny / 2;
     const bool live = t < TA;
@@ -794,10 +798,9 @@ static cudaError_t launch_2d_k(const Fista2dArgs& a, long long units, cudaStream
         if (grid > (long long)per * nsm) grid = (long long)per * nsm;
     }
     if (row)
-        k2d_row_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(b, mode, it, tw, rt, nrt);
-    else
-        k2d_col_reg<P, MINB><<<(unsigned)grid, P::T * G, smem, st>>>(b, mode, tw, rt, nrt);
-    return cudaGetLastError();
+        return launch_pass(k2d_row_reg<P, MINB>, (unsigned)grid, P::T * G, smem, st, b.pdl != 0, b, mode, it, tw, rt,
+                           nrt);
+    return launch_pass(k2d_col_reg<P, MINB>, (unsigned)grid, P::T * G, smem, st, b.pdl != 0, b, mode, tw, rt, nrt);
 }
 
 // The 15-warp form (a.occ = 3): between the two above (the 368 column pass

@@ -865,6 +865,8 @@ k2d_col_p368(Fista2dArgs a, const float2* __restrict__ gtw) {
     uint32_t* NEED = reinterpret_cast<uint32_t*>(TWs + Tw<P>::total());   // 3 words: need[0..92)
     uint32_t* ROWS = NEED + 4;                                // 12 words: the tile's sampled rows
     for (int q = threadIdx.x; q < Tw<P>::total(); q += blockDim.x) TWs[q] = gtw[q];
+    pdl_wait();                                       // the previous pass's S is complete
+    pdl_trigger();
     const int tid = threadIdx.x, c = tid % CW, tc = tid / CW, lane = tid & 31;
     const int cls = (tc >> 2) & 3;                            // this thread's radix-23 class (tc < 16)
     const int nx = a.nx;
@@ -1123,8 +1125,7 @@ static cudaError_t col2d_p368_k(const Fista2dArgs& a, cudaStream_t st) {
     if (a.col_ctas > 0 && a.col_ctas < per) per = a.col_ctas;
     const long long cap = (long long)per * sm_count();
     if (grid > cap) grid = cap;
-    k2d_col_p368<CW, TPC, SW><<<(unsigned)grid, CW * TPC, smem, st>>>(a, tw);
-    return cudaGetLastError();
+    return launch_pass(k2d_col_p368<CW, TPC, SW>, (unsigned)grid, CW * TPC, smem, st, a.pdl != 0, a, tw);
 }
 }  // namespace reg
 

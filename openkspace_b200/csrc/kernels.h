@@ -159,6 +159,28 @@ cudaError_t launch_fista_col_reg(const FistaColArgs& a, RegTables& tabs, cudaStr
 int fista_col_reg_variants(int ny);   // number of register plans for this column length
 
 // FISTA for arbitrary 2-D masks (k_fista2d.cu): state X~, Z~, S per problem.
+// Launch of a 2-D pass: with pdl, as a programmatic dependent launch (the
+// kernel calls pdl_wait() before it touches what the previous grid wrote).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pass(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                               bool pdl, Args... args) {
+    if (!pdl) {
+        kern<<<grid, block, smem, st>>>(args...);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 struct Fista2dArgs {
     const float2* y;          // k-space [ny][nx] per problem
     long long y_stride;
@@ -189,6 +211,8 @@ struct Fista2dArgs {
                               // pass (separable masks), bit 1 row pass; bit 2 row pass with
                               // bulk-copy (cp.async.bulk) staging of S, Z~, X~
     int* err;                 // bounded-wait error word (bulk-copy row pass), may be null
+    int pdl;                  // register passes: programmatic dependent launches (prologue overlaps the
+                              // previous pass's tail)
     int row_ctas;             // > 0: the persistent row pass takes at most this many CTAs per SM
     int col_ctas;             // > 0: the pruned 368 column pass takes at most this many CTAs per SM
                               // (room for the other stream's pass on the same SM)

@@ -571,6 +571,14 @@ __device__ __forceinline__ void inverse(float2* w, float2* A, float2* B, const f
     }
 }
 
+// Programmatic dependent launch: pdl_wait() returns once the grid this one
+// depends on in its stream has completed and its writes are visible (at once
+// for a grid launched without the attribute); pdl_trigger() lets the next
+// grid of the stream be scheduled (its CTAs take SM slots as this grid's CTAs
+// leave, and run their prologue up to their own pdl_wait).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
     return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
 }

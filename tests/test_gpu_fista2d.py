@@ -140,9 +140,11 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=1, fista2d_chunk=2, col2d_lanes=11),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=12),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, row2d_ctas=1, col2d_ctas=1),
-             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=3, row2d_ctas=2, col2d_ctas=2)]
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=3, row2d_ctas=2, col2d_ctas=2),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, pdl2d=1),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=1, fista2d_chunk=3, pdl2d=1, col2d_lanes=-1)]
     default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0, prefetch2d=1, col2d_lanes=0,
-                   row2d_ctas=0, col2d_ctas=0)
+                   row2d_ctas=0, col2d_ctas=0, pdl2d=0)
     results = []
     try:
         for form in forms:
