@@ -96,7 +96,9 @@ const char* okscuda_version(void);
  *                   sampled rows (radix-23 output pairs and input pairs that
  *                   only unsampled rows reach are left out), (columns,
  *                   threads per column) (8,16) (8,32) (16,16) (16,32); 13 =
- *                   (8,16) with the row slots swizzled against bank conflicts
+ *                   (8,16) with the row slots swizzled against bank conflicts;
+ *                   14 = the two-stage plan 16 · 23 with the residual fused
+ *                   between the directions in registers
  *   "pdl2d"         2-D register passes launched as programmatic dependent
  *                   launches: a pass's CTAs load their tables while the
  *                   previous pass ends, then wait for it (griddepcontrol);

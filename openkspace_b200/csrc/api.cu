@@ -137,9 +137,9 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
             return set_err(ctx, OKS_EINVAL, "xform_tile: 0 (by length), 2, 4 or 8 column pairs");
         ctx->xform_tile = (int)value;
     } else if (!std::strcmp(name, "col2d_lanes")) {
-        if (value < -1 || value > 13)
+        if (value < -1 || value > 14)
             return set_err(ctx, OKS_EINVAL,
-                           "col2d_lanes: -1 column pairs, 0 by length, 1 to 8 a lanes form, 9 to 13 the pruned 368 forms");
+                           "col2d_lanes: -1 column pairs, 0 by length, 1 to 8 a lanes form, 9 to 14 the pruned 368 forms");
         ctx->col2d_lanes = (int)value;
     } else if (!std::strcmp(name, "xform_row_variant")) {
         if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");

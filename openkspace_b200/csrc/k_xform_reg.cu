@@ -1127,6 +1127,273 @@ static cudaError_t col2d_p368_k(const Fista2dArgs& a, cudaStream_t st) {
     if (grid > cap) grid = cap;
     return launch_pass(k2d_col_p368<CW, TPC, SW>, (unsigned)grid, CW * TPC, smem, st, a.pdl != 0, a, tw);
 }
+
+// 2-D-mask engine, column pass at ny = 368 in two stages, 16 · 23, pruned to
+// the sampled rows with the residual fused between the two directions (form
+// 14).  Forward: radix 16 (p = 1), then radix 23 (p = 16), whose butterfly b
+// produces exactly rows b + 16 j; the inverse, in reversed order, starts with
+// radix 23 (p = 1) reading the same rows b + 16 j.  So one thread per radix-23
+// butterfly folds the forward's inputs, forms only the output pairs (j,
+// 23 - j) with a sampled row, takes the residual m' (F S - y') on them in
+// registers and folds it straight into the inverse's radix-23 butterfly,
+// where the pairs whose rows are both unsampled are zero and left out; it
+// writes the inverse's 23 outputs.  The last stage is the inverse radix 16
+// (p = 23), stored to S.  y' is copied by each thread for its own rows and
+// column (8-byte cp.async into the staging tile once the first stage has read
+// it), so no barrier guards it.  The pair masks depend on the butterfly's
+// rows; forward butterfly 4 (tc mod 4) + tc / 4 puts the four butterflies of
+// one class b mod 4 in each warp, so for masks sampled every 2nd or 4th row
+// the branches are nearly uniform per warp.
+// Twiddles (gtw, forward sign): [16][22] w_368^(j b) of the forward radix-23
+// stage, then [23][15] w_368^(j b) of the inverse radix-16 stage (conjugated).
+// Forward output pairs Q.. of radix-23 butterfly (fa, fb, x0) with a sampled
+// row, their residual, and the inverse's folds ra = r_Q + r_(23-Q),
+// rb = r_Q - r_(23-Q) (zero for a pair left out).  res(row, v) is the residual.
+template <int Q, class Res>
+__device__ __forceinline__ void q368_fwd_pairs(const float2* fa, const float2* fb, float2 x0, int b, uint32_t pm,
+                                               const Res& res, float2* ra, float2* rb) {
+    if constexpr (Q <= 11) {
+        if ((pm >> Q) & 1u) {
+            float2 re = x0, im = make_float2(0.f, 0.f);
+            odd_acc<23, Q, 1>(fa, fb, re, im);
+            const float2 si = mul_si<-1>(im);
+            const float2 r1 = res(b + 16 * Q, re + si), r2 = res(b + 16 * (23 - Q), re - si);
+            ra[Q - 1] = r1 + r2;
+            rb[Q - 1] = r1 - r2;
+        } else {
+            ra[Q - 1] = make_float2(0.f, 0.f);
+            rb[Q - 1] = make_float2(0.f, 0.f);
+        }
+        q368_fwd_pairs<Q + 1>(fa, fb, x0, b, pm, res, ra, rb);
+    }
+}
+// Inverse output pairs Q.. of radix-23 butterfly (ra, rb, r0), p = 1: outputs
+// 23 b + Q and 23 b + 23 - Q of the tile D.
+template <int CW, int Q>
+__device__ __forceinline__ void q368_inv_pairs(const float2* ra, const float2* rb, float2 r0, float2* D, int b, int c,
+                                               uint32_t pm) {
+    if constexpr (Q <= 11) {
+        float2 re = r0, im = make_float2(0.f, 0.f);
+        p368_acc_masked<Q, 1>(ra, rb, re, im, pm);
+        const float2 si = mul_si<+1>(im);
+        D[(23 * b + Q) * CW + c] = re + si;
+        D[(23 * b + 23 - Q) * CW + c] = re - si;
+        q368_inv_pairs<CW, Q + 1>(ra, rb, r0, D, b, c, pm);
+    }
+}
+
+template <int CW, int TPC>
+__global__ void __launch_bounds__(CW * TPC, 512 / (CW * TPC) > 0 ? 512 / (CW * TPC) : 1)   // 128 registers
+k2d_col_q368(Fista2dArgs a, const float2* __restrict__ gtw) {
+    constexpr int N = 368, NB16 = 23, H = 11;
+    constexpr int BPT = (NB16 + TPC - 1) / TPC;   // radix-16 butterflies per thread
+    constexpr int TWF = 16 * 22, TWN = TWF + 23 * 15;
+    static_assert(TPC >= 16 && CW == 8, "16 radix-23 butterflies; four of one class per warp");
+    extern __shared__ __align__(16) float2 sm[];
+    float2* D = sm;                                           // [N][CW] the stages, in place
+    float2* ST = sm + N * CW;                                 // [N][CW] S tile, then y' on the sampled rows
+    float2* TWs = ST + N * CW;
+    uint32_t* ROWS = reinterpret_cast<uint32_t*>(TWs + TWN);  // 12 words: the tile's sampled rows
+    for (int q = threadIdx.x; q < TWN; q += blockDim.x) TWs[q] = gtw[q];
+    pdl_wait();                                               // the previous pass's S is complete
+    pdl_trigger();
+    const int tid = threadIdx.x, c = tid % CW, tc = tid / CW;
+    const int nx = a.nx;
+    const int ntx = (nx + CW - 1) / CW;
+    const long long total = a.nprob * ntx;
+    const float minv = a.minv, ysc = a.ysc;
+    const bool act = tc < 16;                                 // owns a radix-23 butterfly
+    const int b23 = 4 * (tc & 3) + ((tc >> 2) & 3);
+    auto has_sample = [&](long long u) {
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const uint32_t* cb = a.colbits + ((p + a.mask_offset) % a.mask_mod) * a.col_wstride;
+        for (int cc = 0; cc < CW; ++cc) {
+            const int xx = x0 + cc;
+            if (xx < nx && ((__ldg(cb + (xx >> 5)) >> (xx & 31)) & 1u)) return true;
+        }
+        return false;
+    };
+    auto next_tile = [&](long long u) {
+        for (; u < total; u += gridDim.x)
+            if (has_sample(u)) break;
+        return u;
+    };
+    auto issue_s = [&](long long u) {
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const float2* S = a.S + p * a.st_stride;
+        for (int k = tid; k < N * (CW / 2); k += CW * TPC) {
+            const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+            const bool onj = x0 + j < nx;
+            if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                cp_async16(ST + r * CW + j, onj ? S + (long long)r * nx + x0 + j : S, onj ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    auto rowbit = [&](int r) { return (ROWS[r >> 5] >> (r & 31)) & 1u; };
+    long long u = next_tile(blockIdx.x);
+    if (u < total) issue_s(u);
+    while (u < total) {
+        const long long un = next_tile(u + gridDim.x);
+        const long long p = u / ntx;
+        const int x0 = (int)(u - p * ntx) * CW;
+        const long long mi = (p + a.mask_offset) % a.mask_mod;
+        const uint32_t* rb = a.rowbits + mi * a.row_wstride;
+        const int x = x0 + c;
+        const bool on = x < nx;
+        const bool colon = on && ((__ldg(a.colbits + mi * a.col_wstride + (x >> 5)) >> (x & 31)) & 1u);
+        cp_async_wait_all();
+        __syncthreads();                                      // ST holds this tile; the last tile is done with D, ROWS
+        if (tid < 12) ROWS[tid] = __ldg(rb + tid);
+        // forward stage 0 (radix 16, p = 1): inputs b + 23 j from ST, outputs 16 b + j
+#pragma unroll 1
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (b >= NB16) break;
+            float2 v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int r = b + NB16 * j;
+                v[j] = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? ST[r * CW + c] : make_float2(0.f, 0.f);
+            }
+            bfly16<-1>(v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                if (OKS_IN((16 * b + j) * CW + c, N * CW, OKS_B_TILE)) D[(16 * b + j) * CW + c] = v[j];
+        }
+        __syncthreads();                                      // D complete; ST read by every thread; ROWS set
+        // y' of this thread's own rows b23 + 16 j (sampled) and column into ST
+        const float2* y = a.y + p * a.y_stride;
+        if (act) {
+#pragma unroll
+            for (int j = 0; j < 23; ++j) {
+                const int r = b23 + 16 * j;
+                if (colon && rowbit(r) && OKS_IN(r * CW + c, N * CW, OKS_B_STAGE))
+                    cp_async8(ST + r * CW + c, y + (long long)r * nx + x, 8u);
+            }
+        }
+        cp_async_commit();
+        // pair mask of this thread's butterfly: bit q set when row b23 + 16 q
+        // or row b23 + 368 - 16 q is sampled (bit 0: row b23)
+        uint32_t pm = 0;
+        float2 x0v = make_float2(0.f, 0.f), fa[H], fb[H];
+        if (act) {
+            pm = rowbit(b23);
+#pragma unroll
+            for (int q = 1; q <= H; ++q) pm |= (rowbit(b23 + 16 * q) | rowbit(b23 + 368 - 16 * q)) << q;
+            // forward radix-23 folds (p = 16: inputs b23 + 16 j, twiddles w^(j b23))
+            x0v = D[b23 * CW + c];
+#pragma unroll
+            for (int j = 1; j <= H; ++j) {
+                const float2 uu = twmul<-1>(D[(b23 + 16 * j) * CW + c], TWs[b23 * 22 + j - 1]);
+                const float2 ww = twmul<-1>(D[(b23 + 16 * (23 - j)) * CW + c], TWs[b23 * 22 + 22 - j]);
+                fa[j - 1] = uu + ww;
+                fb[j - 1] = uu - ww;
+            }
+        }
+        __syncthreads();                                      // in place: every fold input read
+        if (act) {
+            cp_async_wait_all();                              // this thread's own y' copies
+            auto res = [&](int r, float2 v) {
+                const bool smp = colon && rowbit(r);
+                return smp ? (v - ST[r * CW + c] * (((r + x) & 1) ? -ysc : ysc)) * minv : make_float2(0.f, 0.f);
+            };
+            float2 r0 = make_float2(0.f, 0.f);
+            if (pm & 1u) {
+                float2 y0 = x0v;
+#pragma unroll
+                for (int j = 0; j < H; ++j) y0 = y0 + fa[j];
+                r0 = res(b23, y0);
+            }
+            float2 ra[H], rbv[H];
+            q368_fwd_pairs<1>(fa, fb, x0v, b23, pm, res, ra, rbv);
+            // inverse radix-23 (p = 1): outputs 23 b23 + j
+            float2 y0 = r0;
+#pragma unroll
+            for (int j = 1; j <= H; ++j)
+                if ((pm >> j) & 1u) y0 = y0 + ra[j - 1];
+            if (OKS_IN((23 * b23 + 22) * CW + c, N * CW, OKS_B_TILE)) {
+                D[(23 * b23) * CW + c] = y0;
+                q368_inv_pairs<CW, 1>(ra, rbv, r0, D, b23, c, pm);
+            }
+        }
+        __syncthreads();                                      // D complete; ST (y') read
+        if (un < total) issue_s(un);                          // the next S tile, in flight during the last stage
+        // inverse stage 1 (radix 16, p = 23): inputs b + 23 j, outputs rows b + 23 j of S
+        float2* Sc = a.S + p * a.st_stride + (on ? x : 0);
+#pragma unroll 1
+        for (int bb = 0; bb < BPT; ++bb) {
+            const int b = tc + TPC * bb;
+            if (b >= NB16) break;
+            float2 v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int r = b + NB16 * j;
+                float2 t = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? D[r * CW + c] : make_float2(0.f, 0.f);
+                if (j > 0) t = twmul<+1>(t, TWs[TWF + b * 15 + j - 1]);
+                v[j] = t;
+            }
+            bfly16<+1>(v);
+            if (on) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) Sc[(long long)(b + NB16 * j) * nx] = v[j];
+            }
+        }
+        u = un;
+    }
+    cp_async_wait_all();
+}
+
+// Twiddles of k2d_col_q368 on the current device, built on first use.
+static cudaError_t q368_tables(const float2** tw) {
+    static float2* d_tab[64] = {};
+    static std::mutex mu;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!d_tab[dev]) {
+        const double two_pi = 6.283185307179586476925286766559;
+        std::vector<float2> h;
+        for (int b = 0; b < 16; ++b)
+            for (int j = 1; j < 23; ++j) {
+                const double ang = -two_pi * j * b / 368.0;
+                h.push_back(make_float2((float)cos(ang), (float)sin(ang)));
+            }
+        for (int b = 0; b < 23; ++b)
+            for (int j = 1; j < 16; ++j) {
+                const double ang = -two_pi * j * b / 368.0;
+                h.push_back(make_float2((float)cos(ang), (float)sin(ang)));
+            }
+        float2* d = nullptr;
+        cudaError_t e = cudaMalloc(&d, sizeof(float2) * h.size());
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        d_tab[dev] = d;
+    }
+    *tw = d_tab[dev];
+    return cudaSuccess;
+}
+
+static cudaError_t col2d_q368(const Fista2dArgs& a, cudaStream_t st) {
+    constexpr int CW = 8, TPC = 16;
+    const float2* tw;
+    cudaError_t e = q368_tables(&tw);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)2 * 368 * CW + 16 * 22 + 23 * 15) + 16 * sizeof(uint32_t);
+    const void* fn = reinterpret_cast<const void*>(k2d_col_q368<CW, TPC>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = a.nprob * ((a.nx + CW - 1) / CW);
+    long long grid = tiles;
+    int per = ctas_per_sm(fn, CW * TPC, smem);
+    if (a.col_ctas > 0 && a.col_ctas < per) per = a.col_ctas;
+    const long long cap = (long long)per * sm_count();
+    if (grid > cap) grid = cap;
+    return launch_pass(k2d_col_q368<CW, TPC>, (unsigned)grid, CW * TPC, smem, st, a.pdl != 0, a, tw);
+}
+
 }  // namespace reg
 
 cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st) {
@@ -1140,6 +1407,7 @@ cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, c
             case 11: return reg::col2d_p368_k<16, 16>(a, st);
             case 12: return reg::col2d_p368_k<16, 32>(a, st);
             case 13: return reg::col2d_p368_k<8, 16, true>(a, st);
+            case 14: return reg::col2d_q368(a, st);
             default: return reg::col2d_p368_k<8, 16>(a, st);
         }
     }

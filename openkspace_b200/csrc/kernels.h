@@ -229,7 +229,8 @@ cudaError_t launch_fista2d_row_reg(const Fista2dArgs& a, RegTables& tabs, int mo
 // Column pass in the lanes form (k_xform_reg.cu): form 1-4 (16,32) (16,64)
 // (8,64) (8,32) columns x threads per column, 5-8 the 368 forms (16,16) (8,16)
 // (16,32) (8,32); 9-12 the 368 forms pruned to the sampled rows, (8,16) (8,32)
-// (16,16) (16,32), for separable masks and mode 1 only.
+// (16,16) (16,32) (13: (8,16) with swizzled row slots; 14: the two-stage
+// plan 16 · 23 with the residual fused), for separable masks and mode 1 only.
 cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st);
 cudaError_t launch_fista2d_demod(const float2* X, float2* out, long long nprob, int ny, int nx, long long in_stride,
                                  long long out_stride, cudaStream_t st);

@@ -68,7 +68,7 @@ with Context(0) as ctx:
              dict(occ2d=0, prefetch2d=4, persist2d=0), dict(col2d_lanes=5), dict(col2d_lanes=6), dict(col2d_lanes=7), dict(col2d_lanes=8), dict(col2d_lanes=1),
              dict(col2d_lanes=3), dict(col2d_lanes=-1), dict(col2d_lanes=9),
              dict(col2d_lanes=10), dict(col2d_lanes=11), dict(col2d_lanes=12),
-             dict(col2d_lanes=13)]
+             dict(col2d_lanes=13), dict(col2d_lanes=14)]
     default = dict(occ2d=1, prefetch2d=1, persist2d=1, col2d_lanes=0)
     for ny, nx in ((368, 640), (256, 192), (384, 320), (128, 512)):   # 2-D engine, partial rows
         m = np.zeros((ny, nx), bool)

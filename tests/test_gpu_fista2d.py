@@ -142,6 +142,7 @@ def test_mask_forms_and_launch_forms_agree(ctx, rng, ny, nx, iters):
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, row2d_ctas=1, col2d_ctas=1),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=3, row2d_ctas=2, col2d_ctas=2),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, pdl2d=1),
+             dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=2, col2d_lanes=14),
              dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=1, fista2d_chunk=3, pdl2d=1, col2d_lanes=-1)]
     default = dict(mask_bits=1, occ2d=1, persist2d=1, fista2d_streams=2, fista2d_chunk=0, prefetch2d=1, col2d_lanes=0,
                    row2d_ctas=0, col2d_ctas=0, pdl2d=0)
@@ -171,9 +172,9 @@ def row_set_mask(ny, nx, rows):
 
 
 @pytest.mark.parametrize("rows", ["r4_centre", "r4_offset", "r3", "random20", "one_row", "all", "class_edge"])
-@pytest.mark.parametrize("form", [9, 10, 11, 12, 13])
+@pytest.mark.parametrize("form", [9, 10, 11, 12, 13, 14])
 def test_pruned_368_column_pass(ctx, rng, rows, form):
-    """The 368 column pass pruned to the sampled rows (col2d_lanes 9-13)
+    """The 368 column pass pruned to the sampled rows (col2d_lanes 9-14)
     against the full register pass and FP64, for row sets that exercise
     every pruning case: R = 4 plus a centre block (the precision workload's
     pattern, dense class and sparse classes), R = 4 shifted by one row, R = 3
