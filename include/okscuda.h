@@ -87,7 +87,7 @@ const char* okscuda_version(void);
  *                   pass; bit 2 row pass with the next row pair of S, Z~ and
  *                   X~ staged in shared memory by cp.async.bulk (mbarrier
  *                   completion, bounded waits)
- *   "col2d_lanes"   2-D-mask engine column pass: 0 (default) by length (form 9
+ *   "col2d_lanes"   2-D-mask engine column pass: 0 (default) by length (form 14
  *                   at ny = 368, else -1); -1 one column pair
  *                   per thread group; 1-8 the lanes form (tiles of 8 or 16
  *                   columns in shared memory, lanes across the columns; the

@@ -509,10 +509,10 @@ static int fista2d_core(okscuda_ctx* ctx, const okscuda_c64* d_kspace, const uin
             a.occ = tp.occ2d;
             a.prefetch = tp.prefetch2d;
             a.err = ctx->tc_err;
-            // 0: by length -- the pruned lanes form (8, 16) at ny = 368 (it
+            // 0: by length -- the pruned two-stage form (14) at ny = 368 (it
             // takes the iteration passes of separable masks; the rest stay on
             // the column-pair pass), the column-pair pass elsewhere
-            a.col_lanes = ctx->col2d_lanes > 0 ? ctx->col2d_lanes : (ctx->col2d_lanes == 0 && ny == 368 ? 9 : 0);
+            a.col_lanes = ctx->col2d_lanes > 0 ? ctx->col2d_lanes : (ctx->col2d_lanes == 0 && ny == 368 ? 14 : 0);
             a.row_ctas = ctx->row2d_ctas;
             a.pdl = ctx->pdl2d;
             a.col_ctas = ctx->col2d_ctas;
