@@ -590,9 +590,13 @@ constexpr int lanes_default() {
 
 // Columns across the lanes: tile width CW and threads per column TPC
 // (lanes 1..4: (16, 32), (16, 64), (8, 64), (8, 32)).
+static cudaError_t col_q368(const ColXformArgs& a, cudaStream_t st);   // the two-stage 368 form (below)
+
 template <class P>
 static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) {
     if constexpr (big_odd_plan<P>()) {
+        if (lanes == 9 && P::N == 368 && (a.nx % 2) == 0 && (reinterpret_cast<uintptr_t>(a.data) & 15) == 0)
+            return col_q368(a, st);
         // 16 threads per column: one per radix-23 butterfly (368 / 23 = 16);
         // 32: half of them idle in that stage, fewer butterflies each in the others
         if (lanes == 6) return col_lanes_k<P, 8, 16>(a, st);
@@ -619,7 +623,7 @@ static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
         // 640; 368 takes the forms 5-8, the other lengths 1-4
         int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
         if (lanes > 0) {
-            if constexpr (big_odd_plan<P>()) lanes = lanes < 5 ? 5 : lanes;   // 5-8
+            if constexpr (big_odd_plan<P>()) lanes = lanes < 5 ? 5 : lanes;   // 5-9
             else lanes = lanes > 4 ? 1 : lanes;
         }
         if (a.tile == 0 && lanes > 0 && (long long)P::N * a.nx < (1ll << 31)) return col_lanes<P>(a, lanes, st);
@@ -1392,6 +1396,182 @@ static cudaError_t col2d_q368(const Fista2dArgs& a, cudaStream_t st) {
     const long long cap = (long long)per * sm_count();
     if (grid > cap) grid = cap;
     return launch_pass(k2d_col_q368<CW, TPC>, (unsigned)grid, CW * TPC, smem, st, a.pdl != 0, a, tw);
+}
+
+
+// Standalone 368-point column transform in two stages, 16 · 23, with the
+// lanes across 8 columns (xform_lanes 9).  Forward: radix 16 (p = 1) from the
+// staging tile into D, then radix 23 (p = 16), one thread per butterfly,
+// whose outputs are rows b + 16 j, stored straight to global memory (a warp
+// writes four rows of 8 columns per step).  Inverse: radix 23 (p = 1) from
+// the staging tile into D, then radix 16 (p = 23) storing rows b + 23 j.  One
+// shared-memory exchange in either direction (the 4 · 23 · 4 form has two).
+// Twiddles as k2d_col_q368.  Centring signs and scale as k_col_lanes.  The
+// next tile's columns are copied into the staging tile (16-byte cp.async)
+// once the first stage has read it: nx even and 16-byte aligned data.
+template <int SIGN>
+__device__ __forceinline__ void q368_out_pairs_store(const float2* fa, const float2* fb, float2 x0, float2* col,
+                                                     int b, int nx, bool on, bool centred, float sc) {
+    auto put = [&](int o, float2 v) {
+        if (on) col[(long long)o * nx] = v * ((centred && (o & 1)) ? -sc : sc);
+    };
+    float2 y0 = x0;
+#pragma unroll
+    for (int j = 0; j < 11; ++j) y0 = y0 + fa[j];
+    put(b, y0);
+#define OKS_Q368_PAIR(Q)                                                   \
+    {                                                                      \
+        float2 re = x0, im = make_float2(0.f, 0.f);                        \
+        odd_acc<23, Q, 1>(fa, fb, re, im);                                 \
+        const float2 si = mul_si<SIGN>(im);                                \
+        put(b + 16 * (Q), re + si);                                        \
+        put(b + 16 * (23 - (Q)), re - si);                                 \
+    }
+    OKS_Q368_PAIR(1) OKS_Q368_PAIR(2) OKS_Q368_PAIR(3) OKS_Q368_PAIR(4) OKS_Q368_PAIR(5) OKS_Q368_PAIR(6)
+    OKS_Q368_PAIR(7) OKS_Q368_PAIR(8) OKS_Q368_PAIR(9) OKS_Q368_PAIR(10) OKS_Q368_PAIR(11)
+#undef OKS_Q368_PAIR
+}
+
+template <int SIGN>
+__global__ void __launch_bounds__(128, 4)
+k_col_q368(ColXformArgs a, const float2* __restrict__ gtw) {
+    constexpr int N = 368, CW = 8, TPC = 16, H = 11, TWF = 16 * 22, TWN = TWF + 23 * 15;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* D = sm;                                  // [N][CW]
+    float2* ST = sm + N * CW;                        // [N][CW] staging
+    float2* TWs = ST + N * CW;
+    for (int q = threadIdx.x; q < TWN; q += blockDim.x) TWs[q] = gtw[q];
+    const int tid = threadIdx.x, c = tid % CW, tc = tid / CW;
+    const int ntx = (a.nx + CW - 1) / CW;
+    const long long total = a.nprob * ntx;
+    const bool centred = a.centred != 0;
+    const float sc = (centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    auto issue = [&](long long u) {
+        const long long pr = u / ntx;
+        const int x0 = (int)(u - pr * ntx) * CW;
+        const float2* base = a.data + pr * a.prob_stride + x0;
+        for (int k = tid; k < N * (CW / 2); k += CW * TPC) {
+            const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+            const bool on = x0 + j < a.nx;
+            if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                cp_async16(ST + r * CW + j, on ? base + (long long)r * a.nx + j : a.data, on ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    auto ld = [&](int r) {                           // staged input, centring sign on load
+        float2 x = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? ST[r * CW + c] : make_float2(0.f, 0.f);
+        if (centred && (r & 1)) x = make_float2(-x.x, -x.y);
+        return x;
+    };
+    long long u = blockIdx.x;
+    if (u < total) issue(u);
+    for (; u < total; u += gridDim.x) {
+        const long long pr = u / ntx;
+        const int x = (int)(u - pr * ntx) * CW + c;
+        const bool on = x < a.nx;
+        float2* col = a.data + pr * a.prob_stride + (on ? x : 0);
+        const long long un = u + gridDim.x;
+        cp_async_wait_all();
+        __syncthreads();                             // ST holds tile u; the last tile is done with D
+        if constexpr (SIGN < 0) {
+            // radix 16 (p = 1): inputs b + 23 j, outputs 16 b + j
+            float2 v[2][16];
+#pragma unroll
+            for (int bb = 0; bb < 2; ++bb) {
+                const int b = tc + TPC * bb;
+                if (b >= 23) break;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[bb][j] = ld(b + 23 * j);
+            }
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < total) issue(un);
+#pragma unroll
+            for (int bb = 0; bb < 2; ++bb) {
+                const int b = tc + TPC * bb;
+                if (b >= 23) break;
+                bfly16<-1>(v[bb]);
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (OKS_IN((16 * b + j) * CW + c, N * CW, OKS_B_TILE)) D[(16 * b + j) * CW + c] = v[bb][j];
+            }
+            __syncthreads();
+            // radix 23 (p = 16): butterfly tc, inputs tc + 16 j twiddled, outputs rows tc + 16 j
+            if (tc < 16) {
+                const int b = tc;
+                float2 fa[H], fb[H];
+                const float2 x0 = D[b * CW + c];
+#pragma unroll
+                for (int j = 1; j <= H; ++j) {
+                    const float2 uu = twmul<-1>(D[(b + 16 * j) * CW + c], TWs[b * 22 + j - 1]);
+                    const float2 ww = twmul<-1>(D[(b + 16 * (23 - j)) * CW + c], TWs[b * 22 + 22 - j]);
+                    fa[j - 1] = uu + ww;
+                    fb[j - 1] = uu - ww;
+                }
+                q368_out_pairs_store<-1>(fa, fb, x0, col, b, a.nx, on, centred, sc);
+            }
+        } else {
+            // radix 23 (p = 1): butterfly tc, inputs tc + 16 j, outputs 23 tc + j
+            float2 fa[H], fb[H], x0 = make_float2(0.f, 0.f);
+            if (tc < 16) {
+                x0 = ld(tc);
+#pragma unroll
+                for (int j = 1; j <= H; ++j) {
+                    const float2 uu = ld(tc + 16 * j), ww = ld(tc + 16 * (23 - j));
+                    fa[j - 1] = uu + ww;
+                    fb[j - 1] = uu - ww;
+                }
+            }
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < total) issue(un);
+            if (tc < 16 && OKS_IN((23 * tc + 22) * CW + c, N * CW, OKS_B_TILE)) {
+                float2 y0 = x0;
+#pragma unroll
+                for (int j = 0; j < H; ++j) y0 = y0 + fa[j];
+                D[(23 * tc) * CW + c] = y0;
+                q368_inv_pairs<CW, 1>(fa, fb, x0, D, tc, c, 0xFFFu);   // every pair
+            }
+            __syncthreads();
+            // radix 16 (p = 23): inputs b + 23 j twiddled, outputs rows b + 23 j
+#pragma unroll 1
+            for (int bb = 0; bb < 2; ++bb) {
+                const int b = tc + TPC * bb;
+                if (b >= 23) break;
+                float2 v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    float2 t = D[(b + 23 * j) * CW + c];
+                    if (j > 0) t = twmul<+1>(t, TWs[TWF + b * 15 + j - 1]);
+                    v[j] = t;
+                }
+                bfly16<+1>(v);
+                if (on) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int o = b + 23 * j;
+                        col[(long long)o * a.nx] = v[j] * ((centred && (o & 1)) ? -sc : sc);
+                    }
+                }
+            }
+        }
+    }
+    cp_async_wait_all();
+}
+
+static cudaError_t col_q368(const ColXformArgs& a, cudaStream_t st) {
+    const float2* tw;
+    cudaError_t e = q368_tables(&tw);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)2 * 368 * 8 + 16 * 22 + 23 * 15);
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_col_q368<-1>)
+                                : reinterpret_cast<const void*>(k_col_q368<+1>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = a.nprob * ((a.nx + 7) / 8);
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, 128, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    if (a.sign < 0) k_col_q368<-1><<<(unsigned)grid, 128, smem, st>>>(a, tw);
+    else k_col_q368<+1><<<(unsigned)grid, 128, smem, st>>>(a, tw);
+    return cudaGetLastError();
 }
 
 }  // namespace reg

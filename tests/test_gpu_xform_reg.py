@@ -168,11 +168,11 @@ def test_row_plan_variants(ctx, rng, n, variant):
 
 
 @pytest.mark.parametrize("pf", [0, 1])
-@pytest.mark.parametrize("lanes", [5, 6, 7, 8])
+@pytest.mark.parametrize("lanes", [5, 6, 7, 8, 9])
 def test_column_lanes_368(ctx, rng, lanes, pf):
     """The 368-point lanes forms (16 threads per column, one per radix-23
     butterfly), pipelined and direct, ragged and odd column counts."""
-    for ncols, inverse in ((38, True), (130, False), (7, True)):
+    for ncols, inverse in ((38, True), (130, False), (7, True), (40, False), (130, True)):
         x = crandn(rng, (2, 368, ncols))
         want = o64.centred_ifft2(x) if inverse else o64.centred_fft2(x)
         ctx.set_option("xform_lanes", lanes)
