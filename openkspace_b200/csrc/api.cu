@@ -142,7 +142,7 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
                            "col2d_lanes: -1 column pairs, 0 by length, 1 to 8 a lanes form, 9 to 14 the pruned 368 forms");
         ctx->col2d_lanes = (int)value;
     } else if (!std::strcmp(name, "xform_row_variant")) {
-        if (value < 0 || value > 2) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0, 1 or 2");
+        if (value < 0 || value > 3) return set_err(ctx, OKS_EINVAL, "xform_row_variant: 0 to 3");
         ctx->xform_row_variant = (int)value;
     } else if (!std::strcmp(name, "pdl2d")) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "pdl2d: 0 or 1");

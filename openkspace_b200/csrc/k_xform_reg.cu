@@ -584,7 +584,7 @@ constexpr int lanes_default() {
            : (P::N == 320 || P::N == 512) ? 1
            : P::N == 384 ? 3
            : P::N == 640 ? 2
-           : P::N == 368 ? 8
+           : P::N == 368 ? 9
                          : 0;
 }
 
@@ -1574,6 +1574,190 @@ static cudaError_t col_q368(const ColXformArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+
+// Standalone 368-point row transform in two stages, 16 · 23, 8 rows per CTA
+// (xform_row_variant 3).  The rows are staged row-major by 16-byte cp.async
+// (rows on 16-byte boundaries) while the previous tile is transformed.
+// Forward: radix 16 (p = 1), item (r, b), b < 23, reads elements b + 23 j of
+// row r from the staging tile and writes 16 b + j to D, whose rows are padded
+// (index k + k / 16) so the stride-16 writes spread over the banks; radix 23
+// (p = 16), thread (r, b) with b < 16, reads b + 16 j and stores elements
+// b + 16 j of the row to global memory (16 consecutive elements per
+// half-warp).  Inverse: radix 23 (p = 1) from the staging tile into D at
+// 23 b + j, then radix 16 (p = 23) storing elements b + 23 j.  Twiddles as
+// k2d_col_q368; kept rows, rowsign, centring and scale as k_row_xform_reg.
+__device__ __forceinline__ int q368_pad(int k) { return k + (k >> 4); }
+
+template <int SIGN>
+__global__ void __launch_bounds__(128, 4)
+k_row_q368(RowXformArgs a, const float2* __restrict__ gtw) {
+    constexpr int N = 368, RW = 8, NP = N + N / 16, H = 11, TWF = 16 * 22, TWN = TWF + 23 * 15;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* ST = sm;                                 // [RW][N] staged rows
+    float2* D = ST + RW * N;                         // [RW][NP] the exchange, padded rows
+    float2* TWs = D + RW * NP;
+    for (int q = threadIdx.x; q < TWN; q += blockDim.x) TWs[q] = gtw[q];
+    const int tid = threadIdx.x;
+    const long long ntiles = (a.nrows + RW - 1) / RW;
+    const bool centred = a.centred != 0;
+    const float sc_n2 = (centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    auto row_kept = [&](long long row) {
+        if (row >= a.nrows) return false;
+        return !a.use_keep || row_on(a.keep, row / a.rows_per_prob, (int)(row % a.rows_per_prob));
+    };
+    auto issue = [&](long long u) {
+        for (int k = tid; k < RW * (N / 2); k += 128) {
+            const int r = k / (N / 2), x = 2 * (k - r * (N / 2));
+            const long long row = u * RW + r;
+            const bool on = row_kept(row);
+            if (OKS_IN(r * N + x + 1, RW * N, OKS_B_STAGE))
+                cp_async16(ST + r * N + x, on ? a.in + row * a.ld_in + x : a.in, on ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    auto ld = [&](int r, int e) {                    // staged element e of row r, centring sign on load
+        float2 v = OKS_IN(r * N + e, RW * N, OKS_B_TILE) ? ST[r * N + e] : make_float2(0.f, 0.f);
+        if (centred && (e & 1)) v = make_float2(-v.x, -v.y);
+        return v;
+    };
+    auto dd = [&](int r, int k) -> float2& { return D[r * NP + q368_pad(k)]; };
+    long long u = blockIdx.x;
+    if (u < ntiles) issue(u);
+    for (; u < ntiles; u += gridDim.x) {
+        const long long un = u + gridDim.x;
+        // the output row of the radix-23 / radix-16 items is set per item below
+        auto store = [&](int r, int e, float2 v) {
+            const long long row = u * RW + r;
+            if (row >= a.nrows) return;
+            float s = sc_n2;
+            if (a.rowsign && ((row % a.rows_per_prob) & 1)) s = -s;
+            a.out[row * a.ld_out + e] = v * ((centred && (e & 1)) ? -s : s);
+        };
+        cp_async_wait_all();
+        __syncthreads();                             // ST holds tile u; the last tile is done with D
+        if constexpr (SIGN < 0) {
+            // radix 16 (p = 1): items f = tid, tid + 128 < 184: (r, b) = (f / 23, f % 23)
+            float2 v[2][16];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int f = tid + 128 * k;
+                if (f >= RW * 23) break;
+                const int r = f / 23, b = f - r * 23;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[k][j] = ld(r, b + 23 * j);
+            }
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < ntiles) issue(un);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int f = tid + 128 * k;
+                if (f >= RW * 23) break;
+                const int r = f / 23, b = f - r * 23;
+                bfly16<-1>(v[k]);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) dd(r, 16 * b + j) = v[k][j];
+            }
+            __syncthreads();
+            // radix 23 (p = 16): thread (r, b) = (tid / 16, tid % 16)
+            {
+                const int r = tid >> 4, b = tid & 15;
+                float2 fa[H], fb[H];
+                const float2 x0 = dd(r, b);
+#pragma unroll
+                for (int j = 1; j <= H; ++j) {
+                    const float2 uu = twmul<-1>(dd(r, b + 16 * j), TWs[b * 22 + j - 1]);
+                    const float2 ww = twmul<-1>(dd(r, b + 16 * (23 - j)), TWs[b * 22 + 22 - j]);
+                    fa[j - 1] = uu + ww;
+                    fb[j - 1] = uu - ww;
+                }
+                float2 y0 = x0;
+#pragma unroll
+                for (int j = 0; j < H; ++j) y0 = y0 + fa[j];
+                store(r, b, y0);
+#define OKS_RQ368_PAIR(Q)                                                   \
+                {                                                           \
+                    float2 re = x0, im = make_float2(0.f, 0.f);             \
+                    odd_acc<23, Q, 1>(fa, fb, re, im);                      \
+                    const float2 si = mul_si<-1>(im);                       \
+                    store(r, b + 16 * (Q), re + si);                        \
+                    store(r, b + 16 * (23 - (Q)), re - si);                 \
+                }
+                OKS_RQ368_PAIR(1) OKS_RQ368_PAIR(2) OKS_RQ368_PAIR(3) OKS_RQ368_PAIR(4) OKS_RQ368_PAIR(5)
+                OKS_RQ368_PAIR(6) OKS_RQ368_PAIR(7) OKS_RQ368_PAIR(8) OKS_RQ368_PAIR(9) OKS_RQ368_PAIR(10)
+                OKS_RQ368_PAIR(11)
+#undef OKS_RQ368_PAIR
+            }
+        } else {
+            // radix 23 (p = 1): thread (r, b) = (tid / 16, tid % 16), inputs b + 16 j
+            const int r = tid >> 4, b = tid & 15;
+            float2 fa[H], fb[H];
+            const float2 x0 = ld(r, b);
+#pragma unroll
+            for (int j = 1; j <= H; ++j) {
+                const float2 uu = ld(r, b + 16 * j), ww = ld(r, b + 16 * (23 - j));
+                fa[j - 1] = uu + ww;
+                fb[j - 1] = uu - ww;
+            }
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < ntiles) issue(un);
+            {
+                float2 y0 = x0;
+#pragma unroll
+                for (int j = 0; j < H; ++j) y0 = y0 + fa[j];
+                dd(r, 23 * b) = y0;
+#define OKS_RQ368_IPAIR(Q)                                                  \
+                {                                                           \
+                    float2 re = x0, im = make_float2(0.f, 0.f);             \
+                    odd_acc<23, Q, 1>(fa, fb, re, im);                      \
+                    const float2 si = mul_si<+1>(im);                       \
+                    dd(r, 23 * b + (Q)) = re + si;                          \
+                    dd(r, 23 * b + 23 - (Q)) = re - si;                     \
+                }
+                OKS_RQ368_IPAIR(1) OKS_RQ368_IPAIR(2) OKS_RQ368_IPAIR(3) OKS_RQ368_IPAIR(4) OKS_RQ368_IPAIR(5)
+                OKS_RQ368_IPAIR(6) OKS_RQ368_IPAIR(7) OKS_RQ368_IPAIR(8) OKS_RQ368_IPAIR(9) OKS_RQ368_IPAIR(10)
+                OKS_RQ368_IPAIR(11)
+#undef OKS_RQ368_IPAIR
+            }
+            __syncthreads();
+            // radix 16 (p = 23): items f < 184: (r, b) = (f / 23, f % 23), elements b + 23 j
+#pragma unroll 1
+            for (int k = 0; k < 2; ++k) {
+                const int f = tid + 128 * k;
+                if (f >= RW * 23) break;
+                const int rr = f / 23, bb = f - rr * 23;
+                float2 v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    float2 t = dd(rr, bb + 23 * j);
+                    if (j > 0) t = twmul<+1>(t, TWs[TWF + bb * 15 + j - 1]);
+                    v[j] = t;
+                }
+                bfly16<+1>(v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) store(rr, bb + 23 * j, v[j]);
+            }
+        }
+    }
+    cp_async_wait_all();
+}
+
+static cudaError_t row_q368(const RowXformArgs& a, cudaStream_t st) {
+    const float2* tw;
+    cudaError_t e = q368_tables(&tw);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)8 * 368 + 8 * (368 + 23) + 16 * 22 + 23 * 15);
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_row_q368<-1>)
+                                : reinterpret_cast<const void*>(k_row_q368<+1>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = (a.nrows + 7) / 8;
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, 128, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    if (a.sign < 0) k_row_q368<-1><<<(unsigned)grid, 128, smem, st>>>(a, tw);
+    else k_row_q368<+1><<<(unsigned)grid, 128, smem, st>>>(a, tw);
+    return cudaGetLastError();
+}
+
 }  // namespace reg
 
 cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st) {
@@ -1629,6 +1813,10 @@ cudaError_t launch_row_xform_reg(const RowXformArgs& a, int n, cudaStream_t st) 
         if (n == 320) return reg::row_p<reg::V320>(a, st);    // 8·5·8 on 80 of 96 threads
     }
     if (a.variant == 2 && !a.tables && n == 192) return reg::row_p<reg::R192>(a, st);   // 4·12·4 on 96 threads
+    // the two-stage 368 form: rows on 16-byte boundaries
+    if (a.variant == 3 && !a.tables && n == 368 && (reinterpret_cast<uintptr_t>(a.in) & 15) == 0 &&
+        (a.ld_in & 1) == 0)
+        return reg::row_q368(a, st);
     switch (n) {
         case 128: return reg::row_p<reg::S128>(a, st);
         case 192: return reg::row_p<reg::P192>(a, st);

@@ -153,7 +153,7 @@ def test_fista_prep_rows_same_on_both_engines(ctx, rng):
     assert o64.nrmse(reg, gen) < 1e-5
 
 
-@pytest.mark.parametrize("n,variant", [(192, 1), (192, 2), (320, 1)])
+@pytest.mark.parametrize("n,variant", [(192, 1), (192, 2), (320, 1), (368, 3)])
 def test_row_plan_variants(ctx, rng, n, variant):
     """The alternative register row plans (option xform_row_variant)."""
     x = crandn(rng, (3, 40, n))
@@ -165,6 +165,29 @@ def test_row_plan_variants(ctx, rng, n, variant):
         ctx.set_option("xform_row_variant", 0)
     assert rel_l2(got, o64.centred_fft2(x)) < TOL
     assert rel_l2(got_i, ref_rows(x.reshape(-1, n), 1, 1)) < TOL
+
+
+def test_row_q368_ragged_and_in_the_column_engine(ctx, rng):
+    """The two-stage 368 row transform (xform_row_variant 3): a row count that
+    leaves a ragged last tile, both directions, and the column engine's
+    readout pass (rows outside the ky mask kept at zero, per-problem row
+    signs) under FISTA with a ky-only mask, against FP64."""
+    x = crandn(rng, (61, 368))
+    ctx.set_option("xform_row_variant", 3)
+    try:
+        got_f = ctx.dft_rows(x, inverse=False, centred=True, engine=0)
+        got_i = ctx.dft_rows(x, inverse=True, centred=True, engine=0)
+        ny, nx, iters = 256, 368, 6
+        m = np.zeros((ny, nx), bool)
+        m[rng.random(ny) < 0.3] = True
+        m[ny // 2 - 4:ny // 2 + 4] = True
+        k = np.where(m[None], crandn(rng, (3, ny, nx)), 0).astype(np.complex64)
+        got_cs = ctx.fista_cs(k, m, iters, 0.02)
+    finally:
+        ctx.set_option("xform_row_variant", 0)
+    assert rel_l2(got_f, ref_rows(x, 0, 1)) < TOL
+    assert rel_l2(got_i, ref_rows(x, 1, 1)) < TOL
+    assert rel_l2(got_cs, o64.fista_cs_single_coil(k, m, iters, 0.02)) < 1e-4
 
 
 @pytest.mark.parametrize("pf", [0, 1])
