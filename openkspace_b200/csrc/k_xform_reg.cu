@@ -1758,6 +1758,207 @@ static cudaError_t row_q368(const RowXformArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+
+// Radix-20 butterfly in registers, 20 = 4 · 5: a 4-point DFT over j1 of
+// x[5 j1 + j2] for each j2, the twiddles w20^(j2 k1), a 5-point DFT over j2
+// for each k1, output k1 + 4 k2 (w = e^(SIGN 2 pi i / 20); the twiddles are
+// immediates).
+template <int SIGN, int J2, int K1>
+__device__ __forceinline__ float2 tw20(float2 a) {
+    if constexpr (J2 == 0 || K1 == 0) return a;
+    else return cmul(a, make_float2(RootRM<20, (J2 * K1) % 20>::c, SIGN * RootRM<20, (J2 * K1) % 20>::s));
+}
+template <int SIGN, int J2>
+__device__ __forceinline__ void bfly20_cols(const float2* v, float2 (*A)[4]) {
+    if constexpr (J2 < 5) {
+        float2 t[4] = {v[J2], v[5 + J2], v[10 + J2], v[15 + J2]};
+        bfly4<SIGN>(t);
+        A[J2][0] = t[0];
+        A[J2][1] = tw20<SIGN, J2, 1>(t[1]);
+        A[J2][2] = tw20<SIGN, J2, 2>(t[2]);
+        A[J2][3] = tw20<SIGN, J2, 3>(t[3]);
+        bfly20_cols<SIGN, J2 + 1>(v, A);
+    }
+}
+template <int SIGN>
+__device__ __forceinline__ void bfly20(float2* v) {
+    float2 A[5][4];
+    bfly20_cols<SIGN, 0>(v, A);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        float2 u[5] = {A[0][k1], A[1][k1], A[2][k1], A[3][k1], A[4][k1]};
+        bfly5<SIGN>(u);
+#pragma unroll
+        for (int k2 = 0; k2 < 5; ++k2) v[k1 + 4 * k2] = u[k2];
+    }
+}
+
+// Standalone 320-point row transform in two stages, 16 · 20, 8 rows per CTA
+// (xform_row_variant 3, and the default at 320): the structure of k_row_q368
+// with a radix-20 second stage (one butterfly of 20 points per thread, 16 per
+// row).  Twiddles (forward sign): [16][19] w_320^(j b) of the forward radix-20
+// stage, then [20][15] w_320^(j b) of the inverse radix-16 stage.
+template <int SIGN>
+__global__ void __launch_bounds__(128, 4)
+k_row_q320(RowXformArgs a, const float2* __restrict__ gtw) {
+    constexpr int N = 320, RW = 8, NP = N + N / 16, NB16 = 20, TWF = 16 * 19, TWN = TWF + 20 * 15;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* ST = sm;                                 // [RW][N] staged rows
+    float2* D = ST + RW * N;                         // [RW][NP] the exchange, padded rows
+    float2* TWs = D + RW * NP;
+    for (int q = threadIdx.x; q < TWN; q += blockDim.x) TWs[q] = gtw[q];
+    const int tid = threadIdx.x;
+    const long long ntiles = (a.nrows + RW - 1) / RW;
+    const bool centred = a.centred != 0;
+    const float sc_n2 = (centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    auto row_kept = [&](long long row) {
+        if (row >= a.nrows) return false;
+        return !a.use_keep || row_on(a.keep, row / a.rows_per_prob, (int)(row % a.rows_per_prob));
+    };
+    auto issue = [&](long long u) {
+        for (int k = tid; k < RW * (N / 2); k += 128) {
+            const int r = k / (N / 2), x = 2 * (k - r * (N / 2));
+            const long long row = u * RW + r;
+            const bool on = row_kept(row);
+            if (OKS_IN(r * N + x + 1, RW * N, OKS_B_STAGE))
+                cp_async16(ST + r * N + x, on ? a.in + row * a.ld_in + x : a.in, on ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    auto ld = [&](int r, int e) {
+        float2 v = OKS_IN(r * N + e, RW * N, OKS_B_TILE) ? ST[r * N + e] : make_float2(0.f, 0.f);
+        if (centred && (e & 1)) v = make_float2(-v.x, -v.y);
+        return v;
+    };
+    auto dd = [&](int r, int k) -> float2& { return D[r * NP + q368_pad(k)]; };
+    long long u = blockIdx.x;
+    if (u < ntiles) issue(u);
+    for (; u < ntiles; u += gridDim.x) {
+        const long long un = u + gridDim.x;
+        auto store = [&](int r, int e, float2 v) {
+            const long long row = u * RW + r;
+            if (row >= a.nrows) return;
+            float s = sc_n2;
+            if (a.rowsign && ((row % a.rows_per_prob) & 1)) s = -s;
+            a.out[row * a.ld_out + e] = v * ((centred && (e & 1)) ? -s : s);
+        };
+        cp_async_wait_all();
+        __syncthreads();                             // ST holds tile u; the last tile is done with D
+        const int r20 = tid >> 4, b20 = tid & 15;    // this thread's radix-20 butterfly
+        if constexpr (SIGN < 0) {
+            float2 v[2][16];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int f = tid + 128 * k;
+                if (f >= RW * NB16) break;
+                const int r = f / NB16, b = f - r * NB16;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[k][j] = ld(r, b + NB16 * j);
+            }
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < ntiles) issue(un);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int f = tid + 128 * k;
+                if (f >= RW * NB16) break;
+                const int r = f / NB16, b = f - r * NB16;
+                bfly16<-1>(v[k]);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) dd(r, 16 * b + j) = v[k][j];
+            }
+            __syncthreads();
+            // radix 20 (p = 16): inputs b + 16 j twiddled, outputs b + 16 j
+            float2 w[20];
+#pragma unroll
+            for (int j = 0; j < 20; ++j) {
+                float2 t = dd(r20, b20 + 16 * j);
+                if (j > 0) t = twmul<-1>(t, TWs[b20 * 19 + j - 1]);
+                w[j] = t;
+            }
+            bfly20<-1>(w);
+#pragma unroll
+            for (int j = 0; j < 20; ++j) store(r20, b20 + 16 * j, w[j]);
+        } else {
+            // radix 20 (p = 1): inputs b + 16 j from ST, outputs 20 b + j
+            float2 w[20];
+#pragma unroll
+            for (int j = 0; j < 20; ++j) w[j] = ld(r20, b20 + 16 * j);
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < ntiles) issue(un);
+            bfly20<+1>(w);
+#pragma unroll
+            for (int j = 0; j < 20; ++j) dd(r20, 20 * b20 + j) = w[j];
+            __syncthreads();
+            // radix 16 (p = 20): inputs b + 20 j twiddled, outputs b + 20 j
+#pragma unroll 1
+            for (int k = 0; k < 2; ++k) {
+                const int f = tid + 128 * k;
+                if (f >= RW * NB16) break;
+                const int rr = f / NB16, bb = f - rr * NB16;
+                float2 v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    float2 t = dd(rr, bb + NB16 * j);
+                    if (j > 0) t = twmul<+1>(t, TWs[TWF + bb * 15 + j - 1]);
+                    v[j] = t;
+                }
+                bfly16<+1>(v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) store(rr, bb + NB16 * j, v[j]);
+            }
+        }
+    }
+    cp_async_wait_all();
+}
+
+static cudaError_t q320_tables(const float2** tw) {
+    static float2* d_tab[64] = {};
+    static std::mutex mu;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!d_tab[dev]) {
+        const double two_pi = 6.283185307179586476925286766559;
+        std::vector<float2> h;
+        for (int b = 0; b < 16; ++b)
+            for (int j = 1; j < 20; ++j) {
+                const double ang = -two_pi * j * b / 320.0;
+                h.push_back(make_float2((float)cos(ang), (float)sin(ang)));
+            }
+        for (int b = 0; b < 20; ++b)
+            for (int j = 1; j < 16; ++j) {
+                const double ang = -two_pi * j * b / 320.0;
+                h.push_back(make_float2((float)cos(ang), (float)sin(ang)));
+            }
+        float2* d = nullptr;
+        cudaError_t e = cudaMalloc(&d, sizeof(float2) * h.size());
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        d_tab[dev] = d;
+    }
+    *tw = d_tab[dev];
+    return cudaSuccess;
+}
+
+static cudaError_t row_q320(const RowXformArgs& a, cudaStream_t st) {
+    const float2* tw;
+    cudaError_t e = q320_tables(&tw);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)8 * 320 + 8 * (320 + 20) + 16 * 19 + 20 * 15);
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_row_q320<-1>)
+                                : reinterpret_cast<const void*>(k_row_q320<+1>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = (a.nrows + 7) / 8;
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, 128, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    if (a.sign < 0) k_row_q320<-1><<<(unsigned)grid, 128, smem, st>>>(a, tw);
+    else k_row_q320<+1><<<(unsigned)grid, 128, smem, st>>>(a, tw);
+    return cudaGetLastError();
+}
+
 }  // namespace reg
 
 cudaError_t launch_fista2d_col_lanes(const Fista2dArgs& a, int form, int mode, cudaStream_t st) {
@@ -1818,6 +2019,10 @@ cudaError_t launch_row_xform_reg(const RowXformArgs& a, int n, cudaStream_t st) 
     if ((a.variant == 3 || a.variant == 0) && !a.tables && n == 368 &&
         (reinterpret_cast<uintptr_t>(a.in) & 15) == 0 && (a.ld_in & 1) == 0)
         return reg::row_q368(a, st);
+    // the two-stage 320 form (16 · 20), option only until measured
+    if (a.variant == 3 && !a.tables && n == 320 && (reinterpret_cast<uintptr_t>(a.in) & 15) == 0 &&
+        (a.ld_in & 1) == 0)
+        return reg::row_q320(a, st);
     switch (n) {
         case 128: return reg::row_p<reg::S128>(a, st);
         case 192: return reg::row_p<reg::P192>(a, st);

@@ -153,7 +153,7 @@ def test_fista_prep_rows_same_on_both_engines(ctx, rng):
     assert o64.nrmse(reg, gen) < 1e-5
 
 
-@pytest.mark.parametrize("n,variant", [(192, 1), (192, 2), (320, 1), (368, 3)])
+@pytest.mark.parametrize("n,variant", [(192, 1), (192, 2), (320, 1), (368, 3), (320, 3)])
 def test_row_plan_variants(ctx, rng, n, variant):
     """The alternative register row plans (option xform_row_variant)."""
     x = crandn(rng, (3, 40, n))
