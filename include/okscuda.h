@@ -134,9 +134,9 @@ const char* okscuda_version(void);
  *   "xform_row_variant" register row transform: 0 (default) the fastest plan
  *                   per length; 1 the E = 8 plans for 192 (8·3·8) and 320
  *                   (8·5·8); 2 the 96-thread plan 4·12·4 for 192 (measurement);
- *                   3 the two-stage forms at 368 (16 · 23, also the default
- *                   there) and 320 (16 · 20), 8 rows per CTA, rows on 16-byte
- *                   boundaries
+ *                   3 the two-stage forms at 368 (16 · 23) and 320 (16 · 20),
+ *                   8 rows per CTA, rows on 16-byte boundaries (also the
+ *                   default at those lengths)
  *   "xform_lanes_pf" lanes form: 1 (default) = software-pipelined (the next
  *                   tile is copied into shared memory with cp.async while the
  *                   current one is transformed; even nx and 16-byte aligned
