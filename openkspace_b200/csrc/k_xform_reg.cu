@@ -591,6 +591,7 @@ constexpr int lanes_default() {
 // Columns across the lanes: tile width CW and threads per column TPC
 // (lanes 1..4: (16, 32), (16, 64), (8, 64), (8, 32)).
 static cudaError_t col_q368(const ColXformArgs& a, cudaStream_t st);   // the two-stage 368 form (below)
+static cudaError_t col_q640(const ColXformArgs& a, cudaStream_t st);   // the two-stage 640 form (below)
 
 template <class P>
 static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) {
@@ -604,6 +605,8 @@ static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) 
         if (lanes == 8) return col_lanes_k<P, 8, 32>(a, st);
         return col_lanes_k<P, 16, 16>(a, st);
     } else {
+        if (lanes == 10 && P::N == 640 && (a.nx % 2) == 0 && (reinterpret_cast<uintptr_t>(a.data) & 15) == 0)
+            return col_q640(a, st);
         switch (lanes) {
             case 2: return col_lanes_k<P, 16, 64>(a, st);
             case 3: return col_lanes_k<P, 8, 64>(a, st);
@@ -624,7 +627,7 @@ static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
         int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
         if (lanes > 0) {
             if constexpr (big_odd_plan<P>()) lanes = lanes < 5 ? 5 : lanes;   // 5-9
-            else lanes = lanes > 4 ? 1 : lanes;
+            else lanes = (lanes > 4 && !(lanes == 10 && P::N == 640)) ? 1 : lanes;
         }
         if (a.tile == 0 && lanes > 0 && (long long)P::N * a.nx < (1ll << 31)) return col_lanes<P>(a, lanes, st);
     }
@@ -1956,6 +1959,185 @@ static cudaError_t row_q320(const RowXformArgs& a, cudaStream_t st) {
     if (grid > cap) grid = cap;
     if (a.sign < 0) k_row_q320<-1><<<(unsigned)grid, 128, smem, st>>>(a, tw);
     else k_row_q320<+1><<<(unsigned)grid, 128, smem, st>>>(a, tw);
+    return cudaGetLastError();
+}
+
+
+// Radix-32 butterfly in registers: two 16-point DFTs of the even and the odd
+// inputs, then X[k] = E[k] + w32^k O[k], X[k + 16] = E[k] - w32^k O[k]
+// (immediate twiddles).
+template <int SIGN, int K>
+__device__ __forceinline__ void bfly32_join(const float2* e, const float2* o, float2* v) {
+    if constexpr (K < 16) {
+        const float2 t = K == 0 ? o[K] : cmul(o[K], make_float2(RootRM<32, K>::c, SIGN * RootRM<32, K>::s));
+        v[K] = e[K] + t;
+        v[K + 16] = e[K] - t;
+        bfly32_join<SIGN, K + 1>(e, o, v);
+    }
+}
+template <int SIGN>
+__device__ __forceinline__ void bfly32(float2* v) {
+    float2 e[16], o[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        e[k] = v[2 * k];
+        o[k] = v[2 * k + 1];
+    }
+    bfly16<SIGN>(e);
+    bfly16<SIGN>(o);
+    bfly32_join<SIGN, 0>(e, o, v);
+}
+
+// Standalone 640-point column transform in two stages, 20 · 32, with the
+// lanes across 8 columns and 32 threads per column (xform_lanes 10).
+// Forward: radix 20 (p = 1), thread tc owns butterfly tc (inputs tc + 32 j,
+// outputs 20 tc + j) from the staging tile into D; radix 32 (p = 20), threads
+// tc < 20, inputs tc + 20 j twiddled w_640^(j tc), outputs rows tc + 20 j
+// straight to global memory.  Inverse: radix 32 (p = 1) from the staging
+// tile (outputs 32 b + j), then radix 20 (p = 32), outputs rows b + 32 j.
+// Twiddles (forward sign): [20][31] w_640^(j b), then [32][19] w_640^(j b).
+template <int SIGN>
+__global__ void __launch_bounds__(256, 2)
+k_col_q640(ColXformArgs a, const float2* __restrict__ gtw) {
+    constexpr int N = 640, CW = 8, TPC = 32, TWF = 20 * 31, TWN = TWF + 32 * 19;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* D = sm;                                  // [N][CW]
+    float2* ST = sm + N * CW;                        // [N][CW] staging
+    float2* TWs = ST + N * CW;
+    for (int q = threadIdx.x; q < TWN; q += blockDim.x) TWs[q] = gtw[q];
+    const int tid = threadIdx.x, c = tid % CW, tc = tid / CW;
+    const int ntx = (a.nx + CW - 1) / CW;
+    const long long total = a.nprob * ntx;
+    const bool centred = a.centred != 0;
+    const float sc = (centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    auto issue = [&](long long u) {
+        const long long pr = u / ntx;
+        const int x0 = (int)(u - pr * ntx) * CW;
+        const float2* base = a.data + pr * a.prob_stride + x0;
+        for (int k = tid; k < N * (CW / 2); k += CW * TPC) {
+            const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+            const bool on = x0 + j < a.nx;
+            if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                cp_async16(ST + r * CW + j, on ? base + (long long)r * a.nx + j : a.data, on ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    auto ld = [&](int r) {
+        float2 x = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? ST[r * CW + c] : make_float2(0.f, 0.f);
+        if (centred && (r & 1)) x = make_float2(-x.x, -x.y);
+        return x;
+    };
+    long long u = blockIdx.x;
+    if (u < total) issue(u);
+    for (; u < total; u += gridDim.x) {
+        const long long pr = u / ntx;
+        const int x = (int)(u - pr * ntx) * CW + c;
+        const bool on = x < a.nx;
+        float2* col = a.data + pr * a.prob_stride + (on ? x : 0);
+        const long long un = u + gridDim.x;
+        auto put = [&](int o, float2 v) {
+            if (on) col[(long long)o * a.nx] = v * ((centred && (o & 1)) ? -sc : sc);
+        };
+        cp_async_wait_all();
+        __syncthreads();                             // ST holds tile u; the last tile is done with D
+        if constexpr (SIGN < 0) {
+            float2 w[20];
+#pragma unroll
+            for (int j = 0; j < 20; ++j) w[j] = ld(tc + 32 * j);
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < total) issue(un);
+            bfly20<-1>(w);
+#pragma unroll
+            for (int j = 0; j < 20; ++j)
+                if (OKS_IN((20 * tc + j) * CW + c, N * CW, OKS_B_TILE)) D[(20 * tc + j) * CW + c] = w[j];
+            __syncthreads();
+            if (tc < 20) {
+                float2 v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    float2 t = D[(tc + 20 * j) * CW + c];
+                    if (j > 0) t = twmul<-1>(t, TWs[tc * 31 + j - 1]);
+                    v[j] = t;
+                }
+                bfly32<-1>(v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) put(tc + 20 * j, v[j]);
+            }
+        } else {
+            float2 v[32];
+            if (tc < 20) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = ld(tc + 20 * j);
+            }
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < total) issue(un);
+            if (tc < 20) {
+                bfly32<+1>(v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    if (OKS_IN((32 * tc + j) * CW + c, N * CW, OKS_B_TILE)) D[(32 * tc + j) * CW + c] = v[j];
+            }
+            __syncthreads();
+            float2 w[20];
+#pragma unroll
+            for (int j = 0; j < 20; ++j) {
+                float2 t = D[(tc + 32 * j) * CW + c];
+                if (j > 0) t = twmul<+1>(t, TWs[TWF + tc * 19 + j - 1]);
+                w[j] = t;
+            }
+            bfly20<+1>(w);
+#pragma unroll
+            for (int j = 0; j < 20; ++j) put(tc + 32 * j, w[j]);
+        }
+    }
+    cp_async_wait_all();
+}
+
+static cudaError_t q640_tables(const float2** tw) {
+    static float2* d_tab[64] = {};
+    static std::mutex mu;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!d_tab[dev]) {
+        const double two_pi = 6.283185307179586476925286766559;
+        std::vector<float2> h;
+        for (int b = 0; b < 20; ++b)
+            for (int j = 1; j < 32; ++j) {
+                const double ang = -two_pi * j * b / 640.0;
+                h.push_back(make_float2((float)cos(ang), (float)sin(ang)));
+            }
+        for (int b = 0; b < 32; ++b)
+            for (int j = 1; j < 20; ++j) {
+                const double ang = -two_pi * j * b / 640.0;
+                h.push_back(make_float2((float)cos(ang), (float)sin(ang)));
+            }
+        float2* d = nullptr;
+        cudaError_t e = cudaMalloc(&d, sizeof(float2) * h.size());
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        d_tab[dev] = d;
+    }
+    *tw = d_tab[dev];
+    return cudaSuccess;
+}
+
+static cudaError_t col_q640(const ColXformArgs& a, cudaStream_t st) {
+    const float2* tw;
+    cudaError_t e = q640_tables(&tw);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)2 * 640 * 8 + 20 * 31 + 32 * 19);
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_col_q640<-1>)
+                                : reinterpret_cast<const void*>(k_col_q640<+1>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = a.nprob * ((a.nx + 7) / 8);
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, 256, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    if (a.sign < 0) k_col_q640<-1><<<(unsigned)grid, 256, smem, st>>>(a, tw);
+    else k_col_q640<+1><<<(unsigned)grid, 256, smem, st>>>(a, tw);
     return cudaGetLastError();
 }
 

@@ -190,6 +190,21 @@ def test_row_q368_ragged_and_in_the_column_engine(ctx, rng):
     assert rel_l2(got_cs, o64.fista_cs_single_coil(k, m, iters, 0.02)) < 1e-4
 
 
+def test_column_q640(ctx, rng):
+    """The two-stage 640-point column transform (xform_lanes 10): both
+    directions, ragged tiles and an odd column count (which takes the
+    default form)."""
+    for ncols, inverse in ((38, True), (130, False), (7, True), (40, False), (24, True)):
+        x = crandn(rng, (2, 640, ncols))
+        want = o64.centred_ifft2(x) if inverse else o64.centred_fft2(x)
+        ctx.set_option("xform_lanes", 10)
+        try:
+            got = ctx.centred_fft2(x, inverse)
+        finally:
+            ctx.set_option("xform_lanes", 0)
+        assert rel_l2(got, want) < TOL
+
+
 @pytest.mark.parametrize("pf", [0, 1])
 @pytest.mark.parametrize("lanes", [5, 6, 7, 8, 9])
 def test_column_lanes_368(ctx, rng, lanes, pf):
