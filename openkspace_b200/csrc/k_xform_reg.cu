@@ -577,13 +577,15 @@ static cudaError_t col_lanes_k(const ColXformArgs& a, cudaStream_t st) {
 // 4581 / 3782 / 4063 (form 3), 512 4805 / 4154 / 4144 (form 1), 640 4078 /
 // 2784 / 3689 (form 2), 368 4158 / 2750 / 2624 (form 8, (8, 32): 32 threads
 // per column, the radix-23 stage on 16 of them, one butterfly each).  The
-// tiles stay at 128 (5043 / 3907 against the direct lanes form).
+// tiles stay at 128 (5043 / 3907 against the direct lanes form).  At 368 and
+// 640 the two-stage forms replace them: 368 = 16 · 23 (form 9) 5244, 640 =
+// 20 · 32 (form 10) 4575.
 template <class P>
 constexpr int lanes_default() {
     return (P::N == 192 || P::N == 256) ? 4
            : (P::N == 320 || P::N == 512) ? 1
            : P::N == 384 ? 3
-           : P::N == 640 ? 2
+           : P::N == 640 ? 10
            : P::N == 368 ? 9
                          : 0;
 }
