@@ -131,6 +131,7 @@ const char* okscuda_version(void);
  *                   threads per column being one per radix-23 butterfly,
  *                   9 the two-stage 368 form (16 · 23, 8 columns, the default),
  *                   10 the two-stage 640 form (20 · 32, 8 columns, the default),
+ *                   11 the two-stage 320 form (16 · 20, 8 columns, the default),
  *                   -1 never
  *   "xform_row_variant" register row transform: 0 (default) the fastest plan
  *                   per length; 1 the E = 8 plans for 192 (8·3·8) and 320

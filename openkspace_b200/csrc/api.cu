@@ -160,7 +160,7 @@ int okscuda_set_option(okscuda_ctx* ctx, const char* name, long long value) {
         if (value < 0 || value > 1) return set_err(ctx, OKS_EINVAL, "xform_lanes_pf: 0 or 1");
         ctx->xform_lanes_pf = (int)value;
     } else if (!std::strcmp(name, "xform_lanes")) {
-        if (value < -1 || value > 10) return set_err(ctx, OKS_EINVAL, "xform_lanes: -1 off, 0 by length, 1 to 10");
+        if (value < -1 || value > 11) return set_err(ctx, OKS_EINVAL, "xform_lanes: -1 off, 0 by length, 1 to 11");
         ctx->xform_lanes = (int)value;
     } else if (!std::strcmp(name, "fista2d_streams")) {
         if (value < 1 || value > 8) return set_err(ctx, OKS_EINVAL, "fista2d_streams: 1 to 8");

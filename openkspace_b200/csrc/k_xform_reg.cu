@@ -579,11 +579,12 @@ static cudaError_t col_lanes_k(const ColXformArgs& a, cudaStream_t st) {
 // per column, the radix-23 stage on 16 of them, one butterfly each).  The
 // tiles stay at 128 (5043 / 3907 against the direct lanes form).  At 368 and
 // 640 the two-stage forms replace them: 368 = 16 · 23 (form 9) 5244, 640 =
-// 20 · 32 (form 10) 4575.
+// 20 · 32 (form 10) 4575, and at 320: 16 · 20 (form 11) 5690.
 template <class P>
 constexpr int lanes_default() {
     return (P::N == 192 || P::N == 256) ? 4
-           : (P::N == 320 || P::N == 512) ? 1
+           : P::N == 320 ? 11
+           : P::N == 512 ? 1
            : P::N == 384 ? 3
            : P::N == 640 ? 10
            : P::N == 368 ? 9
@@ -594,6 +595,7 @@ constexpr int lanes_default() {
 // (lanes 1..4: (16, 32), (16, 64), (8, 64), (8, 32)).
 static cudaError_t col_q368(const ColXformArgs& a, cudaStream_t st);   // the two-stage 368 form (below)
 static cudaError_t col_q640(const ColXformArgs& a, cudaStream_t st);   // the two-stage 640 form (below)
+static cudaError_t col_q320(const ColXformArgs& a, cudaStream_t st);   // the two-stage 320 form (below)
 
 template <class P>
 static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) {
@@ -609,6 +611,8 @@ static cudaError_t col_lanes(const ColXformArgs& a, int lanes, cudaStream_t st) 
     } else {
         if (lanes == 10 && P::N == 640 && (a.nx % 2) == 0 && (reinterpret_cast<uintptr_t>(a.data) & 15) == 0)
             return col_q640(a, st);
+        if (lanes == 11 && P::N == 320 && (a.nx % 2) == 0 && (reinterpret_cast<uintptr_t>(a.data) & 15) == 0)
+            return col_q320(a, st);
         switch (lanes) {
             case 2: return col_lanes_k<P, 16, 64>(a, st);
             case 3: return col_lanes_k<P, 8, 64>(a, st);
@@ -629,7 +633,7 @@ static cudaError_t col_p(const ColXformArgs& a, cudaStream_t st) {
         int lanes = a.lanes != 0 ? a.lanes : lanes_default<P>();
         if (lanes > 0) {
             if constexpr (big_odd_plan<P>()) lanes = lanes < 5 ? 5 : lanes;   // 5-9
-            else lanes = (lanes > 4 && !(lanes == 10 && P::N == 640)) ? 1 : lanes;
+            else lanes = (lanes > 4 && !(lanes == 10 && P::N == 640) && !(lanes == 11 && P::N == 320)) ? 1 : lanes;
         }
         if (a.tile == 0 && lanes > 0 && (long long)P::N * a.nx < (1ll << 31)) return col_lanes<P>(a, lanes, st);
     }
@@ -2140,6 +2144,128 @@ static cudaError_t col_q640(const ColXformArgs& a, cudaStream_t st) {
     if (grid > cap) grid = cap;
     if (a.sign < 0) k_col_q640<-1><<<(unsigned)grid, 256, smem, st>>>(a, tw);
     else k_col_q640<+1><<<(unsigned)grid, 256, smem, st>>>(a, tw);
+    return cudaGetLastError();
+}
+
+
+// Standalone 320-point column transform in two stages, 16 · 20, with the
+// lanes across 8 columns and 20 threads per column (xform_lanes 11).
+// Forward: radix 16 (p = 1), thread tc owns butterfly tc (inputs tc + 20 j,
+// outputs 16 tc + j); radix 20 (p = 16), threads tc < 16, inputs tc + 16 j
+// twiddled w_320^(j tc), outputs rows tc + 16 j straight to global memory.
+// Inverse: radix 20 (p = 1) on threads tc < 16 (outputs 20 tc + j), then
+// radix 16 (p = 20), outputs rows tc + 20 j.  Twiddles as k_row_q320.
+template <int SIGN>
+__global__ void __launch_bounds__(160, 3)
+k_col_q320(ColXformArgs a, const float2* __restrict__ gtw) {
+    constexpr int N = 320, CW = 8, TPC = 20, TWF = 16 * 19, TWN = TWF + 20 * 15;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* D = sm;                                  // [N][CW]
+    float2* ST = sm + N * CW;                        // [N][CW] staging
+    float2* TWs = ST + N * CW;
+    for (int q = threadIdx.x; q < TWN; q += blockDim.x) TWs[q] = gtw[q];
+    const int tid = threadIdx.x, c = tid % CW, tc = tid / CW;
+    const int ntx = (a.nx + CW - 1) / CW;
+    const long long total = a.nprob * ntx;
+    const bool centred = a.centred != 0;
+    const float sc = (centred && ((N / 2) & 1)) ? -a.scale : a.scale;
+    auto issue = [&](long long u) {
+        const long long pr = u / ntx;
+        const int x0 = (int)(u - pr * ntx) * CW;
+        const float2* base = a.data + pr * a.prob_stride + x0;
+        for (int k = tid; k < N * (CW / 2); k += CW * TPC) {
+            const int r = k / (CW / 2), j = 2 * (k % (CW / 2));
+            const bool on = x0 + j < a.nx;
+            if (OKS_IN(r * CW + j + 1, N * CW, OKS_B_STAGE))
+                cp_async16(ST + r * CW + j, on ? base + (long long)r * a.nx + j : a.data, on ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    auto ld = [&](int r) {
+        float2 x = OKS_IN(r * CW + c, N * CW, OKS_B_TILE) ? ST[r * CW + c] : make_float2(0.f, 0.f);
+        if (centred && (r & 1)) x = make_float2(-x.x, -x.y);
+        return x;
+    };
+    long long u = blockIdx.x;
+    if (u < total) issue(u);
+    for (; u < total; u += gridDim.x) {
+        const long long pr = u / ntx;
+        const int x = (int)(u - pr * ntx) * CW + c;
+        const bool on = x < a.nx;
+        float2* col = a.data + pr * a.prob_stride + (on ? x : 0);
+        const long long un = u + gridDim.x;
+        auto put = [&](int o, float2 v) {
+            if (on) col[(long long)o * a.nx] = v * ((centred && (o & 1)) ? -sc : sc);
+        };
+        cp_async_wait_all();
+        __syncthreads();                             // ST holds tile u; the last tile is done with D
+        if constexpr (SIGN < 0) {
+            float2 v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = ld(tc + 20 * j);
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < total) issue(un);
+            bfly16<-1>(v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                if (OKS_IN((16 * tc + j) * CW + c, N * CW, OKS_B_TILE)) D[(16 * tc + j) * CW + c] = v[j];
+            __syncthreads();
+            if (tc < 16) {
+                float2 w[20];
+#pragma unroll
+                for (int j = 0; j < 20; ++j) {
+                    float2 t = D[(tc + 16 * j) * CW + c];
+                    if (j > 0) t = twmul<-1>(t, TWs[tc * 19 + j - 1]);
+                    w[j] = t;
+                }
+                bfly20<-1>(w);
+#pragma unroll
+                for (int j = 0; j < 20; ++j) put(tc + 16 * j, w[j]);
+            }
+        } else {
+            float2 w[20];
+            if (tc < 16) {
+#pragma unroll
+                for (int j = 0; j < 20; ++j) w[j] = ld(tc + 16 * j);
+            }
+            __syncthreads();                         // ST read by every thread: refill it
+            if (un < total) issue(un);
+            if (tc < 16) {
+                bfly20<+1>(w);
+#pragma unroll
+                for (int j = 0; j < 20; ++j)
+                    if (OKS_IN((20 * tc + j) * CW + c, N * CW, OKS_B_TILE)) D[(20 * tc + j) * CW + c] = w[j];
+            }
+            __syncthreads();
+            float2 v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                float2 t = D[(tc + 20 * j) * CW + c];
+                if (j > 0) t = twmul<+1>(t, TWs[TWF + tc * 15 + j - 1]);
+                v[j] = t;
+            }
+            bfly16<+1>(v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) put(tc + 20 * j, v[j]);
+        }
+    }
+    cp_async_wait_all();
+}
+
+static cudaError_t col_q320(const ColXformArgs& a, cudaStream_t st) {
+    const float2* tw;
+    cudaError_t e = q320_tables(&tw);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float2) * ((size_t)2 * 320 * 8 + 16 * 19 + 20 * 15);
+    const void* fn = a.sign < 0 ? reinterpret_cast<const void*>(k_col_q320<-1>)
+                                : reinterpret_cast<const void*>(k_col_q320<+1>);
+    if ((e = set_smem_attr(fn, smem)) != cudaSuccess) return e;
+    const long long tiles = a.nprob * ((a.nx + 7) / 8);
+    long long grid = tiles;
+    const long long cap = (long long)ctas_per_sm(fn, 160, smem) * sm_count();
+    if (grid > cap) grid = cap;
+    if (a.sign < 0) k_col_q320<-1><<<(unsigned)grid, 160, smem, st>>>(a, tw);
+    else k_col_q320<+1><<<(unsigned)grid, 160, smem, st>>>(a, tw);
     return cudaGetLastError();
 }
 

@@ -41,7 +41,7 @@ with Context(0) as ctx:
             want = o64.centred_ifft2(x) if inv else o64.centred_fft2(x)
             if rel(got, want) > 1e-5:
                 out["errors"].append(f"fft2 {n} inv={inv}")
-        lanes_forms = (5, 6, 7, 8, 9) if n == 368 else ((1, 2, 3, 4, 10) if n == 640 else (1, 2, 3, 4))
+        lanes_forms = {368: (5, 6, 7, 8, 9), 640: (1, 2, 3, 4, 10), 320: (1, 2, 3, 4, 11)}.get(n, (1, 2, 3, 4))
         for opt, vals in (("xform_tile", (2, 4, 8)), ("xform_lanes", lanes_forms)):
             for v in vals:
                 for pf in ((0, 1) if opt == "xform_lanes" else (0,)):

@@ -190,14 +190,15 @@ def test_row_q368_ragged_and_in_the_column_engine(ctx, rng):
     assert rel_l2(got_cs, o64.fista_cs_single_coil(k, m, iters, 0.02)) < 1e-4
 
 
-def test_column_q640(ctx, rng):
-    """The two-stage 640-point column transform (xform_lanes 10): both
-    directions, ragged tiles and an odd column count (which takes the
-    default form)."""
+@pytest.mark.parametrize("n,form", [(640, 10), (320, 11)])
+def test_column_two_stage(ctx, rng, n, form):
+    """The two-stage column transforms (xform_lanes 10: 640 = 20 · 32; 11:
+    320 = 16 · 20): both directions, ragged tiles and an odd column count
+    (which takes the default form)."""
     for ncols, inverse in ((38, True), (130, False), (7, True), (40, False), (24, True)):
-        x = crandn(rng, (2, 640, ncols))
+        x = crandn(rng, (2, n, ncols))
         want = o64.centred_ifft2(x) if inverse else o64.centred_fft2(x)
-        ctx.set_option("xform_lanes", 10)
+        ctx.set_option("xform_lanes", form)
         try:
             got = ctx.centred_fft2(x, inverse)
         finally:
